@@ -1,0 +1,295 @@
+"""Benchmark of the sparse-voxel rasterizer hot path on synthetic scenes.
+
+Default workload (N=1): 8M voxels (levels 8-14, surfaces + background shell),
+8 views at 1920x1080, SH degree 3.  One step = every view rendered forward and
+back-propagated (projection, binning, compositing, SH, recompute backward).
+
+  metric  fwd+bwd ms/view   (lower is better; `value` = device time per view,
+                             all ranks' views / max-over-ranks time)
+  e2e     the same metric through the public Python API with host buffers:
+          targets and cameras copied host->device every step, loss read back.
+
+Modes: --mode batched (one launch per stage over all views, bf16 storage of
+densities / SH) or --mode plain (one view per call, fp32, the reference's
+call pattern).  --impl reference times the CPU restatement of the same path
+(oracle/, all host threads) on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): views are sharded, each rank renders its own views of
+the shared scene; no collective in the timed data path (weak scaling).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--voxels", type=int, default=None, help="override the voxel count (smaller profiles)")
+    ap.add_argument("--views", type=int, default=None, help="use only the first N views")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def scene_for(args, rank, world):
+    from sv_raster_b200 import synthetic
+    sc = synthetic.config_scene(args.config, n_voxels=args.voxels)
+    cams = sc.cameras[: args.views] if args.views else sc.cameras
+    if world > 1:
+        # weak scaling: every rank renders its own set of views of the same size
+        extra = synthetic.orbit_cameras(len(cams) * world, 1000 + 7, radius=(1.5, 2.0),
+                                        fixed_size=(cams[0].width, cams[0].height)) if args.config == "c4" else None
+        if extra is not None and rank > 0:
+            cams = extra[rank * len(cams):(rank + 1) * len(cams)]
+    sc.cameras = cams
+    trng = np.random.default_rng(1234 + rank)
+    sc.targets = [trng.uniform(0, 1, size=(3, c.height, c.width)).astype(np.float32) for c in cams]
+    return sc
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+
+    from sv_raster_b200 import workload
+    sc = scene_for(args, rank, world)
+    wl = workload.PlainWorkload(sc, dev) if args.mode == "plain" else workload.BatchedWorkload(sc, dev)
+    n_views = len(sc.cameras)
+
+    for _ in range(args.warmup):
+        wl.step()
+    torch.cuda.synchronize()
+
+    # timed region: K steps bracketed by barrier + sync; events on the launch stream
+    stream = torch.cuda.current_stream(dev)
+    sampler = ClockSampler(dev.index if dev.index is not None else 0)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    wl.reset_kernel_timers()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        wl.step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms_total = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_per_step = ms_total / args.steps
+    ms_per_view = ms_per_step / n_views  # per-rank views; all ranks in parallel
+    views_all = n_views * world
+    value = ms_total / (args.steps * views_all)  # device ms per view over the whole job
+    kstats = wl.kernel_stats()
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = wl.e2e(args.steps, args.warmup)
+        if world > 1:
+            t = torch.tensor([e2e["ms_total"]], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e["ms_total"] = float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_baseline(sc, budget_s=15.0)
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        dom = kstats["dominant"]
+        achieved = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9 if dom["ms"] > 0 else 0.0
+        line = {
+            "metric": "fwd+bwd ms/view", "value": round(value, 4), "unit": "ms/view", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.mode == "plain" else "bf16-storage/f32-compute", "data": "synthetic",
+            "config": {"workload": f"{args.config}: {sc.n_voxels} voxels, {n_views} views/rank "
+                                   f"{sc.cameras[0].width}x{sc.cameras[0].height}, SH3, fwd+recompute bwd",
+                       "mode": args.mode, "l2": "inputs larger than L2 (scene arrays > 126 MB)",
+                       "instances_per_view": wl.instances_per_view()},
+            "render_fps": round(1000.0 / kstats["fwd_ms_per_view"], 2) if kstats.get("fwd_ms_per_view") else None,
+            "rays_per_s": round(sum(c.width * c.height for c in sc.cameras) * world / (ms_total / args.steps * 1e-3),
+                                1),
+            "gpu_launches": wl.launches_per_step() * args.steps,
+            "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": round(achieved, 2),
+                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_kind": peak_kind, "traffic": dom.get("traffic"),
+                         "algorithmic_bytes_per_launch": dom["bytes_per_launch"],
+                         "ms_per_launch": round(dom["ms_per_launch"], 4)},
+            "kernels": kstats["table"],
+            "clocks": clocks,
+        }
+        if e2e is not None:
+            line["e2e"] = {"value": round(e2e["ms_total"] / (args.steps * views_all), 4), "unit": "ms/view",
+                           "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(sc, budget_s=15.0):
+    """The CPU oracle (fp32 mimic, all host threads) on a bounded sample: the
+    first view's full projection + binning, then forward + backward on a run of
+    tiles in the middle of the image; reported as ms/view extrapolated by tiles."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cam = sc.cameras[0]
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    t0 = time.perf_counter()
+    idx = np.arange(sc.n_voxels)
+    rgbs = O.sh_fwd(3, idx, sc.centers, cam.position, sc.sh0, sc.shs)
+    ndup, bbox, quad = O.preprocess(cam, sc.centers, sc.lengths)
+    keys, vals, ranges = O.binning(cam, sc.octpath, ndup, bbox, quad)
+    t_setup = time.perf_counter() - t0
+    gx, gy = (cam.width + 15) // 16, (cam.height + 15) // 16
+    T = gx * gy
+    mid = T // 2
+    n_tiles = 8
+    spent = 0.0
+    done_tiles = 0
+    while spent < budget_s and done_tiles < T:
+        t1 = time.perf_counter()
+        lo, hi = max(0, mid - n_tiles // 2), min(T, mid - n_tiles // 2 + n_tiles)
+        out = O.render_fwd(cam, ranges, vals, bbox, sc.centers, sc.lengths, sc.geos, rgbs, tiles=(lo, hi))
+        dC = np.zeros_like(out["color"])
+        dC[:] = 1e-3
+        O.render_bwd(cam, ranges, out["tile_last"], vals, bbox, sc.centers, sc.lengths, sc.geos, rgbs,
+                     out["n_contrib"], out["T"], dC, np.zeros_like(out["T"], dtype=np.float32), tiles=(lo, hi))
+        dt = time.perf_counter() - t1
+        spent += dt
+        done_tiles = hi - lo
+        per_tile = dt / max(1, hi - lo)
+        if spent + per_tile * n_tiles * 2 > budget_s:
+            break
+        n_tiles *= 2
+    ms_view = (per_tile * T + t_setup) * 1e3
+    return {"value": round(ms_view, 2), "unit": "ms/view", "cores": cores, "kind": "port",
+            "sample": f"view 0: full projection+binning ({len(vals)} instances) + fwd/bwd of {done_tiles} of {T} "
+                      f"central tiles, extrapolated by tile count"}
+
+
+def run_reference(args):
+    """Reference arm: the CPU restatement of the reference path (oracle port,
+    all host threads) on a bounded sample of the same workload."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sc = scene_for(args, 0, 1)
+    vals = []
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        pass
+    for _ in range(max(1, args.steps)):
+        vals.append(cpu_baseline(sc, budget_s=max(5.0, 60.0 / max(1, args.steps))))
+    v = float(np.median([x["value"] for x in vals]))
+    line = {"metric": "fwd+bwd ms/view", "value": round(v, 2), "unit": "ms/view", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"{args.config}: {sc.n_voxels} voxels, {len(sc.cameras)} views "
+                                   f"{sc.cameras[0].width}x{sc.cameras[0].height}", "mode": "cpu"},
+            "cpu_baseline": {"value": round(v, 2), "unit": "ms/view", "cores": vals[0]["cores"], "kind": "port",
+                             "sample": vals[0]["sample"]},
+            "e2e": {"value": round(v, 2), "unit": "ms/view", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

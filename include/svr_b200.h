@@ -1,0 +1,170 @@
+/*
+ * svr_b200.h -- C ABI of the sm_100a sparse-voxel rasterizer (libsvr_b200.so).
+ *
+ * Drop-in replacement, at the native boundary, for the pybind11 module `_C`
+ * of the SVRaster CUDA backend (panicPaul/sv_raster, backends/cuda/binding.cpp:24-55).
+ * Each entry point below names the reference function it replaces.  The
+ * differences of convention are:
+ *   - the caller owns all memory: outputs and opaque state buffers are
+ *     allocated by the caller (sizes from the *_bytes queries) and passed as
+ *     raw device pointers; every output a reference op returns zero-filled
+ *     must be zero-filled by the caller (the Python layer does this);
+ *   - every call takes a cudaStream_t (as void*) and enqueues on it; no call
+ *     synchronises the device unless `debug` is set;
+ *   - every call returns an int status (SVR_OK ...); device-side consistency
+ *     failures (the reference __trap()s) set bits of a device error word that
+ *     svr_read_error reads.
+ * No torch types appear in any signature.
+ */
+#ifndef SVR_B200_H_
+#define SVR_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SVR_OK 0
+#define SVR_ERR_SHAPE 1
+#define SVR_ERR_CAPACITY 2
+#define SVR_ERR_KEYBITS 3
+#define SVR_ERR_CUDA 4
+#define SVR_ERR_DEVICE 5
+#define SVR_ERR_ALIGN 6
+
+/* Compile-time constants (config.h:16,21,23; exported at binding.cpp:51-53). */
+int svr_max_num_levels(void);     /* 16 */
+float svr_step_sz_scale(void);    /* 100 */
+int svr_max_n_samp(void);         /* 3 */
+const char* svr_status_string(int status);
+int svr_version(void);
+
+/* One pinhole camera.  w2c / c2w are DEVICE pointers to row-major 4x4 float
+ * matrices (the reference reads the first 12 entries in-kernel too:
+ * preprocess.cu:57-60, forward.cu:103-109). */
+typedef struct svr_camera {
+  int width, height;
+  float tanfovx, tanfovy;
+  float cx, cy;
+  const float* w2c;
+  const float* c2w;
+  float near_plane;
+  float bg_color;
+} svr_camera;
+
+/* ---- opaque state buffer sizes (raster_state.cu:54-117) ---------------- */
+size_t svr_geom_buffer_bytes(int64_t P);
+size_t svr_image_buffer_bytes(int width, int height);
+size_t svr_binning_buffer_bytes(int64_t num_rendered, int width, int height);
+
+/* Replaces PREPROCESS::rasterize_preprocess (preprocess.cu:136-199, binding
+ * "rasterize_preprocess").  Writes out_n_duplicates[P] (int32) and fills the
+ * caller's geom buffer.  It also scans the duplicate counts on the device and
+ * stores the instance count (uint32) at svr_geom_count_ptr(geom). */
+int svr_rasterize_preprocess(const svr_camera* cam, int64_t P, const int64_t* octree_paths,
+                             const float* vox_centers, const float* vox_lengths, int32_t* out_n_duplicates,
+                             void* geom_buffer, size_t geom_bytes, int debug, void* stream);
+
+/* Device address of the uint32 instance count ("num_rendered", read back by
+ * the reference at forward.cu:652-658) inside a geom buffer. */
+const uint32_t* svr_geom_count_ptr(const void* geom_buffer);
+/* Device address of the uint32 device error word inside a geom buffer. */
+uint32_t* svr_geom_error_ptr(void* geom_buffer);
+
+/* Replaces FORWARD::rasterize_voxels (forward.cu:739-825, binding
+ * "rasterize_voxels") after its count read-back: duplication, sort, tile
+ * ranges and compositing.  `num_rendered` is the value at
+ * svr_geom_count_ptr(geom).  Outputs (caller-zeroed): out_color [3,H,W],
+ * out_depth [3,H,W] (if need_depth || need_distortion, else NULL),
+ * out_normal [3,H,W] (if need_normal), out_T [1,H,W], max_w [P] (if
+ * track_max_w).  geos and rgbs are fp32 [P,8] and [P,3]. */
+int svr_rasterize_forward(const svr_camera* cam, int n_samp_per_vox, int need_depth, int need_distortion,
+                          int need_normal, int track_max_w, int64_t P, int64_t num_rendered,
+                          const int64_t* octree_paths, const float* vox_centers, const float* vox_lengths,
+                          const float* geos, const float* rgbs, void* geom_buffer, void* binning_buffer,
+                          size_t binning_bytes, void* image_buffer, size_t image_bytes, float* out_color,
+                          float* out_depth, float* out_normal, float* out_T, float* max_w, int debug, void* stream);
+
+/* The two stages of svr_rasterize_forward, callable separately (same
+ * arguments): duplication + sort + tile ranges (forward.cu:660-700), then the
+ * compositing kernel alone (forward.cu:702-731). */
+int svr_rasterize_binning(const svr_camera* cam, int64_t P, int64_t num_rendered, const int64_t* octree_paths,
+                          void* geom_buffer, void* binning_buffer, size_t binning_bytes, void* image_buffer,
+                          size_t image_bytes, int debug, void* stream);
+int svr_rasterize_render(const svr_camera* cam, int n_samp_per_vox, int need_depth, int need_distortion,
+                         int need_normal, int track_max_w, int64_t P, int64_t num_rendered, const float* vox_centers,
+                         const float* vox_lengths, const float* geos, const float* rgbs, void* geom_buffer,
+                         void* binning_buffer, size_t binning_bytes, void* image_buffer, size_t image_bytes,
+                         float* out_color, float* out_depth, float* out_normal, float* out_T, float* max_w, int debug,
+                         void* stream);
+
+/* Replaces BACKWARD::rasterize_voxels_backward (backward.cu:655-769, binding
+ * "rasterize_voxels_backward").  Outputs (caller-zeroed): dL_dgeos [P,8],
+ * dL_drgbs [P,3], subdiv_p_bw [P,1].  dL_ddepth / dL_dnormal / gt_color /
+ * out_depth / out_normal may be NULL when the matching feature is off. */
+int svr_rasterize_backward(const svr_camera* cam, int n_samp_per_vox, int64_t P, int64_t num_rendered,
+                           const float* vox_centers, const float* vox_lengths, const float* geos, const float* rgbs,
+                           const void* geom_buffer, const void* binning_buffer, const void* image_buffer,
+                           const float* out_T, const float* dL_dcolor, const float* dL_ddepth,
+                           const float* dL_dnormal, const float* dL_dT, float lambda_R_concen, const float* gt_color,
+                           float lambda_ascending, float lambda_dist, int need_depth, int need_normal,
+                           const float* out_depth, const float* out_normal, float* dL_dgeos, float* dL_drgbs,
+                           float* subdiv_p_bw, int debug, void* stream);
+
+/* Replaces RASTER_STATE::unpack_ImageState (raster_state.cu:155-175):
+ * copies ranges [T,2], tile_last [T], n_contrib [H*W] (int32, device) out of
+ * an image buffer. */
+int svr_unpack_image_state(int width, int height, const void* image_buffer, int32_t* ranges, int32_t* tile_last,
+                           int32_t* n_contrib, void* stream);
+/* Sorted instance keys/values of a binning buffer (device pointers), for
+ * parity checks of the sort (forward.cu:681-686 results). */
+int svr_binning_sorted(const void* binning_buffer, int64_t num_rendered, int width, int height,
+                       const uint64_t** keys, const uint32_t** vals);
+/* Per-voxel preprocess state of a geom buffer (device pointers). */
+int svr_geom_arrays(const void* geom_buffer, int64_t P, const uint32_t** n_dup, const uint32_t** scan,
+                    const uint64_t** bboxes, const uint32_t** quads);
+
+/* Replaces SH_COMPUTE::sh_compute (sh_compute.cu:244-270).  rgbs [P,3]
+ * caller-zeroed; idx may be NULL with n_idx = 0 (all voxels).  sh0 [P,3],
+ * shs [P,M-1,3]; coefficient storage fp32 or bf16 (sh_bf16 = 1). */
+int svr_sh_compute(int degree, int64_t n_idx, const int64_t* idx, int64_t P, int M, const float* vox_centers,
+                   const float* cam_pos, const void* sh0, const void* shs, int sh_bf16, float* rgbs, void* stream);
+/* Replaces SH_COMPUTE::sh_compute_bw (sh_compute.cu:272-299).  dL_dsh0 [P,3],
+ * dL_dshs [P,M-1,3] caller-zeroed. */
+int svr_sh_compute_bw(int degree, int M, int64_t n_idx, const int64_t* idx, int64_t P, const float* vox_centers,
+                      const float* cam_pos, const float* dL_drgbs, float* dL_dsh0, float* dL_dshs, void* stream);
+
+/* Replace ADAM_STEP::unbiased_adam_step / biased_adam_step
+ * (adam_step.cu:106-158); `step` is the 1-based step count. */
+int svr_unbiased_adam_step(int sparse, int64_t numel, float* param, const float* grad, float* exp_avg,
+                           float* exp_avg_sq, double step, double lr, double beta1, double beta2, float eps,
+                           void* stream);
+int svr_biased_adam_step(int sparse, int64_t numel, float* param, const float* grad, float* exp_avg,
+                         float* exp_avg_sq, float lr, float beta1, float beta2, float eps, void* stream);
+
+/* Fused multi-group unbiased Adam: one launch for up to 8 groups (no
+ * reference counterpart; same per-element arithmetic as
+ * unbiased_adam_step_cuda_kernel, adam_step.cu:28-64).  Arrays must be
+ * 16-byte aligned; params may be fp32 or bf16 (param_bf16[i] = 1). */
+int svr_fused_adam_step(int n_groups, int sparse, void* const* params, const int* param_bf16,
+                        const float* const* grads, float* const* exp_avgs, float* const* exp_avg_sqs,
+                        const int64_t* numels, const double* steps, const double* lrs, double beta1, double beta2,
+                        float eps, void* stream);
+
+/* Replace GEO_PARAMS_GATHER::gather_triinterp_geo_params(_bw) and the feat
+ * variants (geo_params_gather.cu:134-222).  dim = 1 (geo) or 3 (feat). */
+int svr_gather_grid_params(int dim, int64_t n_care, const int64_t* vox_key, const int64_t* care_idx,
+                           const float* grid_pts, float* out, void* stream);
+int svr_gather_grid_params_bw(int dim, int64_t n_care, const int64_t* vox_key, const int64_t* care_idx,
+                              const float* dL_dvox, float* dL_dgrid, void* stream);
+
+/* Read and clear a device error word (synchronises `stream`). */
+int svr_read_error(uint32_t* device_word, uint32_t* host_value, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SVR_B200_H_ */

@@ -1,0 +1,440 @@
+// Binning: inclusive scan of per-voxel duplicate counts, key/value
+// duplication, a stable LSD radix sort of (tile | Morton rank) keys and the
+// per-tile [start, end) ranges.
+//
+// Replaces, in forward.cu:601-700 of the reference backend, the CUB scan
+// (forward.cu:643-648), the blocking count read-back (forward.cu:653), the
+// duplicateWithKeys kernel (forward.cu:518-571), the CUB radix sort
+// (forward.cu:681-686) and identifyTileRanges (forward.cu:576-598).
+//
+// Design: every kernel reads the instance count from device memory and is
+// launched for a caller-given capacity, so the whole chain can be captured in
+// a CUDA graph without a host round trip.  The sort is a three-kernel-per-pass
+// LSD radix sort (upsweep histogram, per-digit row scan, stable downsweep)
+// with 8-bit digits and 4096-item CTA tiles; ranks within a CTA come from
+// warp __match_any_sync, which keeps it stable, so it reproduces the order of
+// any other stable sort of the same keys.
+#include "svr_common.cuh"
+#include "svr_views.cuh"
+#include "svr_kernels.h"
+
+namespace svr {
+
+// --------------------------------------------------------------------------
+// Block-wide helpers
+// --------------------------------------------------------------------------
+
+// Exclusive scan of one 32-bit value per thread over a CTA of NT threads.
+template <int NT, typename T>
+__device__ __forceinline__ T block_exclusive_scan(T x, T* s_warp /*[NT/32]*/, T& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    T w = (lane < NT / 32) ? s_warp[lane] : T(0);
+    T winc = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xffffffffu, winc, o);
+      if (lane >= o) winc += y;
+    }
+    if (lane < NT / 32) s_warp[lane] = winc - w;  // exclusive warp offsets
+    if (lane == NT / 32 - 1) s_warp[NT / 32] = winc;
+  }
+  __syncthreads();
+  T res = s_warp[warp] + inc - x;
+  total = s_warp[NT / 32];
+  __syncthreads();
+  return res;
+}
+
+// --------------------------------------------------------------------------
+// Inclusive scan of uint32 counts (three phases, no inter-CTA waiting)
+// --------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+size_t scan_temp_bytes(size_t n) {
+  const size_t nb = (n + kScanTile - 1) / kScanTile;
+  return (nb + 1) * sizeof(unsigned long long) + 256;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_reduce_kernel(const uint32_t* __restrict__ in, size_t n, unsigned long long* __restrict__ block_sums) {
+  __shared__ unsigned long long s_warp[kScanThreads / 32 + 1];
+  const size_t base = (size_t)blockIdx.x * kScanTile;
+  unsigned long long s = 0;
+#pragma unroll
+  for (int r = 0; r < kScanItems; ++r) {
+    const size_t i = base + (size_t)r * kScanThreads + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  unsigned long long tot;
+  block_exclusive_scan<kScanThreads>(s, s_warp, tot);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
+}
+
+// Single CTA: exclusive scan of the block sums (in place); writes the grand
+// total (clamped to 32 bits) and flags overflow of 32 bits or of `cap`.
+__global__ void __launch_bounds__(1024)
+scan_blocks_kernel(unsigned long long* __restrict__ block_sums, int nb, uint32_t* __restrict__ d_total,
+                   unsigned long long cap, uint32_t* __restrict__ err) {
+  __shared__ unsigned long long s_warp[1024 / 32 + 1];
+  unsigned long long running = 0;
+  for (int b0 = 0; b0 < nb; b0 += 1024) {
+    const int i = b0 + threadIdx.x;
+    const unsigned long long x = (i < nb) ? block_sums[i] : 0ull;
+    unsigned long long tot;
+    const unsigned long long ex = block_exclusive_scan<1024>(x, s_warp, tot);
+    if (i < nb) block_sums[i] = running + ex;
+    running += tot;
+  }
+  if (threadIdx.x == 0) {
+    if (running > 0xffffffffull) {
+      *d_total = 0xffffffffu;
+      if (err) atomicOr(err, SVR_DEVERR_CAPACITY);
+    } else {
+      *d_total = (uint32_t)running;
+      if (err && running > cap) atomicOr(err, SVR_DEVERR_CAPACITY);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_apply_kernel(const uint32_t* __restrict__ in, size_t n, const unsigned long long* __restrict__ block_off,
+                  uint32_t* __restrict__ out) {
+  __shared__ unsigned long long s_warp[kScanThreads / 32 + 1];
+  // Each thread owns kScanItems consecutive items: load through shared memory
+  // so global accesses stay coalesced.
+  __shared__ uint32_t s_val[kScanTile];
+  const size_t base = (size_t)blockIdx.x * kScanTile;
+#pragma unroll
+  for (int r = 0; r < kScanItems; ++r) {
+    const int li = r * kScanThreads + threadIdx.x;
+    const size_t i = base + li;
+    s_val[li] = (i < n) ? in[i] : 0u;
+  }
+  __syncthreads();
+  uint32_t v[kScanItems];
+  unsigned long long s = 0;
+#pragma unroll
+  for (int r = 0; r < kScanItems; ++r) {
+    v[r] = s_val[threadIdx.x * kScanItems + r];
+    s += v[r];
+  }
+  unsigned long long tot;
+  unsigned long long run = block_exclusive_scan<kScanThreads>(s, s_warp, tot) + block_off[blockIdx.x];
+#pragma unroll
+  for (int r = 0; r < kScanItems; ++r) {
+    run += v[r];
+    s_val[threadIdx.x * kScanItems + r] = (uint32_t)run;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kScanItems; ++r) {
+    const int li = r * kScanThreads + threadIdx.x;
+    const size_t i = base + li;
+    if (i < n) out[i] = s_val[li];
+  }
+}
+
+void launch_scan_inclusive(const uint32_t* in, uint32_t* out, size_t n, void* temp, uint32_t* d_total,
+                           unsigned long long cap, uint32_t* err, cudaStream_t stream) {
+  if (n == 0) {
+    cudaMemsetAsync(d_total, 0, sizeof(uint32_t), stream);
+    return;
+  }
+  const int nb = (int)((n + kScanTile - 1) / kScanTile);
+  unsigned long long* sums = reinterpret_cast<unsigned long long*>(temp);
+  scan_reduce_kernel<<<nb, kScanThreads, 0, stream>>>(in, n, sums);
+  scan_blocks_kernel<<<1, 1024, 0, stream>>>(sums, nb, d_total, cap, err);
+  scan_apply_kernel<<<nb, kScanThreads, 0, stream>>>(in, n, sums, out);
+}
+
+// --------------------------------------------------------------------------
+// Duplication: one (key, value) per (voxel, camera quadrant, touched tile),
+// emitted in quadrant-ascending, then row-major tile order at the voxel's
+// scan offset (forward.cu:518-563).
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+duplicate_kernel(const __grid_constant__ ViewTable views, int P,
+                 const int64_t* __restrict__ octpaths,
+                 const uint2* __restrict__ bboxes, const uint32_t* __restrict__ quads,
+                 const uint32_t* __restrict__ ndup, const uint32_t* __restrict__ scan,
+                 uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                 uint32_t cap, uint32_t* __restrict__ err) {
+  const int view = blockIdx.y;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= P) return;
+  const size_t o = (size_t)view * P + idx;
+  const uint32_t n = ndup[o];
+  if (n == 0) return;
+  const ViewParams& vp = views.v[view];
+  const uint32_t end = scan[o];
+  uint32_t off = end - n;
+  if (end > cap) {
+    atomicOr(err, SVR_DEVERR_CAPACITY);
+    return;
+  }
+  if ((uint32_t)idx >= (1u << kVoxIdBits)) {
+    atomicOr(err, SVR_DEVERR_VOXID);
+    return;
+  }
+  int tx0, ty0, tx1, ty1;
+  bbox_tile_rect(bboxes[o], vp.grid_x, vp.grid_y, tx0, ty0, tx1, ty1);
+  const uint64_t path = (uint64_t)octpaths[idx];
+  const uint32_t qb = quads[o];
+  for (uint32_t q = 0; q < 8; ++q) {
+    if (!(qb & (1u << q))) continue;
+    const uint64_t rank = order_rank(path, q);
+    const uint32_t val = make_sort_val((uint32_t)idx, q);
+    for (int y = ty0; y <= ty1; ++y) {
+      for (int x = tx0; x <= tx1; ++x) {
+        const uint64_t tile = (uint64_t)(y * vp.grid_x + x);
+        if (off < end) {
+          keys[off] = make_sort_key(tile, rank);
+          vals[off] = val;
+        }
+        ++off;
+      }
+    }
+  }
+  if (off != end) atomicOr(err, SVR_DEVERR_DUP_MISMATCH);
+}
+
+void launch_duplicate(const ViewTable& views, int P, const int64_t* octpaths, const uint2* bboxes,
+                      const uint32_t* quads, const uint32_t* ndup, const uint32_t* scan, uint64_t* keys,
+                      uint32_t* vals, uint32_t cap, uint32_t* err, cudaStream_t stream) {
+  if (P <= 0 || views.n <= 0) return;
+  dim3 grid((P + 255) / 256, views.n);
+  duplicate_kernel<<<grid, 256, 0, stream>>>(views, P, octpaths, bboxes, quads, ndup, scan, keys, vals, cap, err);
+}
+
+// --------------------------------------------------------------------------
+// LSD radix sort of (uint64 key, uint32 value) pairs
+// --------------------------------------------------------------------------
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortRounds = 16;                       // items per thread
+constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096
+constexpr int kWarpSpan = 32 * kSortRounds;            // 512 items per warp
+constexpr int kRadix = 256;
+
+static inline int sort_blocks(size_t cap) { return (int)((cap + kSortTile - 1) / kSortTile); }
+
+size_t sort_temp_bytes(size_t cap) {
+  const size_t nb = (size_t)std::max(1, sort_blocks(cap));
+  return (nb * kRadix + kRadix) * sizeof(uint32_t) + 256;
+}
+
+int sort_passes(int key_bits) { return (key_bits + 7) / 8; }
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+radix_upsweep_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ d_n, uint32_t cap,
+                     int shift, uint32_t* __restrict__ hist, int nblocks) {
+  __shared__ uint32_t s_hist[kSortWarps][kRadix];
+  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&s_hist[0][0])[i] = 0u;
+  __syncthreads();
+  const uint32_t n = min(*d_n, cap);
+  const size_t start = (size_t)blockIdx.x * kSortTile;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (start < n) {
+#pragma unroll 4
+    for (int r = 0; r < kSortRounds; ++r) {
+      const size_t i = start + (size_t)warp * kWarpSpan + r * 32 + lane;
+      if (i < n) {
+        const uint32_t d = (uint32_t)(keys[i] >> shift) & 0xFFu;
+        atomicAdd(&s_hist[warp][d], 1u);
+      }
+    }
+  }
+  __syncthreads();
+  uint32_t s = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w) s += s_hist[w][threadIdx.x];
+  hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = s;
+}
+
+// One CTA per digit: exclusive scan of that digit's per-block counts (in
+// place) and the digit total.
+__global__ void __launch_bounds__(1024)
+radix_scan_rows_kernel(uint32_t* __restrict__ hist, int nblocks, uint32_t* __restrict__ digit_total) {
+  __shared__ uint32_t s_warp[1024 / 32 + 1];
+  uint32_t* row = hist + (size_t)blockIdx.x * nblocks;
+  uint32_t running = 0;
+  for (int b0 = 0; b0 < nblocks; b0 += 1024 * 4) {
+    uint32_t v[4];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i = b0 + threadIdx.x * 4 + k;
+      v[k] = (i < nblocks) ? row[i] : 0u;
+      s += v[k];
+    }
+    uint32_t tot;
+    uint32_t ex = block_exclusive_scan<1024>(s, s_warp, tot) + running;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i = b0 + threadIdx.x * 4 + k;
+      if (i < nblocks) row[i] = ex;
+      ex += v[k];
+    }
+    running += tot;
+  }
+  if (threadIdx.x == 0) digit_total[blockIdx.x] = running;
+}
+
+struct DownsweepSmem {
+  uint64_t keys[kSortTile];
+  uint32_t vals[kSortTile];
+  uint32_t warp_cnt[kSortWarps][kRadix];
+  uint32_t local_start[kRadix];
+  uint32_t global_start[kRadix];
+  uint32_t scan_tmp[kSortThreads / 32 + 1];
+};
+
+__global__ void __launch_bounds__(kSortThreads)
+radix_downsweep_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                       uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                       const uint32_t* __restrict__ d_n, uint32_t cap, int shift,
+                       const uint32_t* __restrict__ hist, const uint32_t* __restrict__ digit_total,
+                       int nblocks) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  DownsweepSmem& sm = *reinterpret_cast<DownsweepSmem*>(smem_raw);
+  const uint32_t n = min(*d_n, cap);
+  const size_t start = (size_t)blockIdx.x * kSortTile;
+  if (start >= n) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  for (int i = tid; i < kSortWarps * kRadix; i += kSortThreads) (&sm.warp_cnt[0][0])[i] = 0u;
+  {
+    uint32_t tot;
+    const uint32_t gbase = block_exclusive_scan<kSortThreads>(digit_total[tid], sm.scan_tmp, tot);
+    sm.global_start[tid] = gbase + hist[(size_t)tid * nblocks + blockIdx.x];
+  }
+  __syncthreads();
+
+  uint64_t k[kSortRounds];
+  uint32_t v[kSortRounds];
+  uint32_t rk[kSortRounds];
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int r = 0; r < kSortRounds; ++r) {
+    const size_t i = start + (size_t)warp * kWarpSpan + r * 32 + lane;
+    const bool valid = i < n;
+    k[r] = valid ? kin[i] : 0ull;
+    v[r] = valid ? vin[i] : 0u;
+    const uint32_t d = valid ? ((uint32_t)(k[r] >> shift) & 0xFFu) : kRadix;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t before = __popc(peers & lt);
+    const uint32_t base = valid ? sm.warp_cnt[warp][d] : 0u;
+    __syncwarp();
+    if (valid && before == 0) sm.warp_cnt[warp][d] = base + __popc(peers);
+    __syncwarp();
+    rk[r] = base + before;
+  }
+  __syncthreads();
+  {
+    // Per digit: exclusive prefix over warps, then local start of the digit.
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t c = sm.warp_cnt[w][tid];
+      sm.warp_cnt[w][tid] = run;
+      run += c;
+    }
+    uint32_t tot;
+    sm.local_start[tid] = block_exclusive_scan<kSortThreads>(run, sm.scan_tmp, tot);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortRounds; ++r) {
+    const size_t i = start + (size_t)warp * kWarpSpan + r * 32 + lane;
+    if (i < n) {
+      const uint32_t d = (uint32_t)(k[r] >> shift) & 0xFFu;
+      const uint32_t pos = sm.local_start[d] + sm.warp_cnt[warp][d] + rk[r];
+      sm.keys[pos] = k[r];
+      sm.vals[pos] = v[r];
+    }
+  }
+  __syncthreads();
+  const uint32_t tile_n = (uint32_t)min((size_t)kSortTile, (size_t)n - start);
+  for (uint32_t p = tid; p < tile_n; p += kSortThreads) {
+    const uint64_t key = sm.keys[p];
+    const uint32_t d = (uint32_t)(key >> shift) & 0xFFu;
+    const uint32_t g = sm.global_start[d] + (p - sm.local_start[d]);
+    kout[g] = key;
+    vout[g] = sm.vals[p];
+  }
+}
+
+// Sorts `n` (read on the device) pairs held in (k0, v0) using (k1, v1) as the
+// ping-pong buffer.  Returns 0 if the result is in (k0, v0), 1 if in (k1, v1).
+int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, const uint32_t* d_n, uint32_t cap,
+                      int key_bits, void* temp, cudaStream_t stream) {
+  const int passes = sort_passes(key_bits);
+  if (cap == 0 || passes == 0) return 0;
+  const int nb = sort_blocks(cap);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(temp);
+  uint32_t* digit_total = hist + (size_t)nb * kRadix;
+  const size_t smem = sizeof(DownsweepSmem);
+  static bool attr_set = false;  // idempotent attribute, safe to repeat
+  if (!attr_set) {
+    cudaFuncSetAttribute(radix_downsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set = true;
+  }
+  uint64_t* kin = k0; uint32_t* vin = v0; uint64_t* kout = k1; uint32_t* vout = v1;
+  for (int p = 0; p < passes; ++p) {
+    const int shift = 8 * p;
+    radix_upsweep_kernel<<<nb, kSortThreads, 0, stream>>>(kin, d_n, cap, shift, hist, nb);
+    radix_scan_rows_kernel<<<kRadix, 1024, 0, stream>>>(hist, nb, digit_total);
+    radix_downsweep_kernel<<<nb, kSortThreads, smem, stream>>>(kin, vin, kout, vout, d_n, cap, shift, hist,
+                                                               digit_total, nb);
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  return passes & 1;
+}
+
+// --------------------------------------------------------------------------
+// Tile ranges from the sorted keys (forward.cu:576-598); `ranges` must be
+// zeroed beforehand.
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+tile_ranges_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ d_n, uint32_t cap,
+                   uint2* __restrict__ ranges) {
+  const uint32_t n = min(*d_n, cap);
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t cur = (uint32_t)(keys[i] >> kRankBits);
+  if (i == 0) {
+    ranges[cur].x = 0;
+  } else {
+    const uint32_t prev = (uint32_t)(keys[i - 1] >> kRankBits);
+    if (cur != prev) {
+      ranges[prev].y = i;
+      ranges[cur].x = i;
+    }
+  }
+  if (i == n - 1) ranges[cur].y = n;
+}
+
+void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_n, uint32_t cap, uint2* ranges, cudaStream_t stream) {
+  if (cap == 0) return;
+  tile_ranges_kernel<<<(cap + 255) / 256, 256, 0, stream>>>(keys, d_n, cap, ranges);
+}
+
+}  // namespace svr

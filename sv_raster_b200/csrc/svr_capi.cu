@@ -1,0 +1,478 @@
+// C ABI implementation: buffer layouts, argument checks and launch sequences
+// of the plain (one view per call) path.  See include/svr_b200.h.
+#include <cmath>
+#include <cstring>
+
+#include "../../include/svr_b200.h"
+#include "svr_common.cuh"
+#include "svr_kernels.h"
+#include "svr_render.cuh"
+#include "svr_render_bwd.cuh"
+#include "svr_render_fwd.cuh"
+
+using namespace svr;
+
+namespace {
+
+constexpr size_t kAlign = 256;
+
+inline size_t align_up(size_t x, size_t a = kAlign) { return (x + a - 1) / a * a; }
+
+// Sequential carve of a caller buffer into aligned sub-arrays, relative to
+// the buffer start (so sizes do not depend on the base address).
+struct Carver {
+  char* base;
+  size_t off = 0;
+  explicit Carver(void* b) : base(static_cast<char*>(b)) {}
+  template <typename T>
+  T* take(size_t count) {
+    off = align_up(off);
+    T* p = reinterpret_cast<T*>(base + off);
+    off += count * sizeof(T);
+    return p;
+  }
+  size_t size() const { return align_up(off) + kAlign; }
+};
+
+// ---- geom buffer: header | n_dup | scan | bbox | quad | scan temp -------------
+struct GeomLayout {
+  uint32_t* header;  // [0] instance count, [1] device error word
+  uint32_t* ndup;
+  uint32_t* scan;
+  uint2* bbox;
+  uint32_t* quad;
+  void* scan_temp;
+  size_t bytes;
+};
+
+GeomLayout geom_layout(void* buf, int64_t P) {
+  Carver c(buf);
+  GeomLayout g;
+  g.header = c.take<uint32_t>(16);
+  g.ndup = c.take<uint32_t>(P);
+  g.scan = c.take<uint32_t>(P);
+  g.bbox = c.take<uint2>(P);
+  g.quad = c.take<uint32_t>(P);
+  g.scan_temp = c.take<char>(scan_temp_bytes((size_t)P));
+  g.bytes = c.size();
+  return g;
+}
+
+// ---- image buffer: ranges | tile_last | n_contrib ----------------------------
+struct ImageLayout {
+  uint2* ranges;
+  uint32_t* tile_last;
+  uint32_t* n_contrib;
+  size_t bytes;
+};
+
+inline int tiles_x(int W) { return (W + kTileX - 1) / kTileX; }
+inline int tiles_y(int H) { return (H + kTileY - 1) / kTileY; }
+
+ImageLayout image_layout(void* buf, int W, int H) {
+  Carver c(buf);
+  ImageLayout im;
+  const size_t T = (size_t)tiles_x(W) * tiles_y(H);
+  im.ranges = c.take<uint2>(T);
+  im.tile_last = c.take<uint32_t>(T);
+  im.n_contrib = c.take<uint32_t>((size_t)W * H);
+  im.bytes = c.size();
+  return im;
+}
+
+// ---- binning buffer: keys a/b | vals a/b | sort temp ---------------------------
+struct BinningLayout {
+  uint64_t* keys_a;
+  uint64_t* keys_b;
+  uint32_t* vals_a;
+  uint32_t* vals_b;
+  void* sort_temp;
+  size_t bytes;
+};
+
+BinningLayout binning_layout(void* buf, size_t n) {
+  Carver c(buf);
+  BinningLayout b;
+  b.keys_a = c.take<uint64_t>(n);
+  b.keys_b = c.take<uint64_t>(n);
+  b.vals_a = c.take<uint32_t>(n);
+  b.vals_b = c.take<uint32_t>(n);
+  b.sort_temp = c.take<char>(sort_temp_bytes(n));
+  b.bytes = c.size();
+  return b;
+}
+
+// Bits needed to represent n (the tile-id width of the sort key).
+inline int bit_width_u32(uint32_t n) {
+  int b = 0;
+  while (b < 32 && (n >> b)) ++b;
+  return b;
+}
+
+inline int plain_key_bits(int W, int H) { return kRankBits + bit_width_u32((uint32_t)(tiles_x(W) * tiles_y(H))); }
+
+ViewParams make_view(const svr_camera& cam) {
+  ViewParams v;
+  memset(&v, 0, sizeof(v));
+  v.W = cam.width;
+  v.H = cam.height;
+  v.grid_x = tiles_x(cam.width);
+  v.grid_y = tiles_y(cam.height);
+  v.tanfovx = cam.tanfovx;
+  v.tanfovy = cam.tanfovy;
+  v.cx = cam.cx;
+  v.cy = cam.cy;
+  // Same float arithmetic as the reference host code (preprocess.cu:173-174).
+  v.focal_x = 0.5f * cam.width / cam.tanfovx;
+  v.focal_y = 0.5f * cam.height / cam.tanfovy;
+  v.near_plane = cam.near_plane;
+  v.bg = cam.bg_color;
+  v.w2c = cam.w2c;
+  v.c2w = cam.c2w;
+  return v;
+}
+
+inline bool valid_camera(const svr_camera* cam) {
+  return cam && cam->width > 0 && cam->height > 0 && cam->width < 65536 && cam->height < 65536 && cam->w2c &&
+         cam->c2w;
+}
+
+inline int check_launch(int debug, cudaStream_t stream) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return SVR_ERR_CUDA;
+  if (debug) {
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return SVR_ERR_CUDA;
+  }
+  return SVR_OK;
+}
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace
+
+extern "C" {
+
+int svr_max_num_levels(void) { return kMaxLevels; }
+float svr_step_sz_scale(void) { return kStepScale; }
+int svr_max_n_samp(void) { return kMaxSamples; }
+int svr_version(void) { return 1; }
+
+const char* svr_status_string(int s) {
+  switch (s) {
+    case SVR_OK: return "ok";
+    case SVR_ERR_SHAPE: return "invalid sizes or arguments";
+    case SVR_ERR_CAPACITY: return "buffer capacity exceeded";
+    case SVR_ERR_KEYBITS: return "sort key does not fit in 64 bits";
+    case SVR_ERR_CUDA: return "CUDA runtime error";
+    case SVR_ERR_DEVICE: return "device-side consistency check failed";
+    case SVR_ERR_ALIGN: return "pointer alignment requirement not met";
+    default: return "unknown status";
+  }
+}
+
+size_t svr_geom_buffer_bytes(int64_t P) { return P < 0 ? 0 : geom_layout(nullptr, P).bytes; }
+size_t svr_image_buffer_bytes(int width, int height) {
+  return (width <= 0 || height <= 0) ? 0 : image_layout(nullptr, width, height).bytes;
+}
+size_t svr_binning_buffer_bytes(int64_t n, int width, int height) {
+  (void)width;
+  (void)height;
+  return n < 0 ? 0 : binning_layout(nullptr, (size_t)n).bytes;
+}
+
+const uint32_t* svr_geom_count_ptr(const void* geom) { return static_cast<const uint32_t*>(geom); }
+uint32_t* svr_geom_error_ptr(void* geom) { return static_cast<uint32_t*>(geom) + 1; }
+
+int svr_rasterize_preprocess(const svr_camera* cam, int64_t P, const int64_t* octree_paths, const float* vox_centers,
+                             const float* vox_lengths, int32_t* out_n_duplicates, void* geom_buffer,
+                             size_t geom_bytes, int debug, void* stream_) {
+  (void)octree_paths;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (P < 0 || P >= (1ll << kVoxIdBits) || !valid_camera(cam)) return SVR_ERR_SHAPE;
+  if (P == 0) return SVR_OK;
+  GeomLayout g = geom_layout(geom_buffer, P);
+  if (!geom_buffer || geom_bytes < g.bytes || !vox_centers || !vox_lengths || !out_n_duplicates) return SVR_ERR_SHAPE;
+  ViewTable vt;
+  vt.n = 1;
+  vt.v[0] = make_view(*cam);
+  cudaMemsetAsync(g.header, 0, 16 * sizeof(uint32_t), stream);
+  launch_preprocess(vt, (int)P, vox_centers, vox_lengths, out_n_duplicates, g.ndup, g.bbox, g.quad, stream);
+  launch_scan_inclusive(g.ndup, g.scan, (size_t)P, g.scan_temp, g.header, 0xffffffffull, g.header + 1, stream);
+  return check_launch(debug, stream);
+}
+
+// Shared argument checks and layouts of the forward stages.
+struct FwdCtx {
+  ViewTable vt;
+  GeomLayout g;
+  ImageLayout im;
+  BinningLayout bl;
+  size_t n;
+  int key_bits;
+};
+
+static int fwd_prepare(const svr_camera* cam, int n_samp, int64_t P, int64_t num_rendered, void* geom_buffer,
+                       void* binning_buffer, size_t binning_bytes, void* image_buffer, size_t image_bytes,
+                       FwdCtx& c) {
+  if (!valid_camera(cam) || n_samp < 1 || n_samp > kMaxSamples || P < 0 || num_rendered < 0 ||
+      num_rendered > 0xffffffffll)
+    return SVR_ERR_SHAPE;
+  const int W = cam->width, H = cam->height;
+  c.im = image_layout(image_buffer, W, H);
+  if (!image_buffer || image_bytes < c.im.bytes) return SVR_ERR_CAPACITY;
+  c.n = (size_t)num_rendered;
+  c.bl = binning_layout(binning_buffer, c.n);
+  if (c.n > 0 && (!binning_buffer || binning_bytes < c.bl.bytes)) return SVR_ERR_CAPACITY;
+  c.key_bits = plain_key_bits(W, H);
+  if (c.key_bits > 64) return SVR_ERR_KEYBITS;
+  c.g = geom_layout(geom_buffer, P);
+  c.vt.n = 1;
+  c.vt.v[0] = make_view(*cam);
+  return SVR_OK;
+}
+
+int svr_rasterize_binning(const svr_camera* cam, int64_t P, int64_t num_rendered, const int64_t* octree_paths,
+                          void* geom_buffer, void* binning_buffer, size_t binning_bytes, void* image_buffer,
+                          size_t image_bytes, int debug, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  FwdCtx c;
+  int st = fwd_prepare(cam, 1, P, num_rendered, geom_buffer, binning_buffer, binning_bytes, image_buffer,
+                       image_bytes, c);
+  if (st != SVR_OK) return st;
+  if (P == 0) return SVR_OK;
+  if (c.n > 0 && !octree_paths) return SVR_ERR_SHAPE;
+  const ViewParams& vp = c.vt.v[0];
+  cudaMemsetAsync(c.im.ranges, 0, (size_t)vp.grid_x * vp.grid_y * sizeof(uint2), stream);
+  if (c.n > 0) {
+    // Duplicate into the buffer that leaves the sorted result in (keys_b, vals_b).
+    const bool odd = (sort_passes(c.key_bits) & 1) != 0;
+    uint64_t* k0 = odd ? c.bl.keys_a : c.bl.keys_b;
+    uint32_t* v0 = odd ? c.bl.vals_a : c.bl.vals_b;
+    uint64_t* k1 = odd ? c.bl.keys_b : c.bl.keys_a;
+    uint32_t* v1 = odd ? c.bl.vals_b : c.bl.vals_a;
+    launch_duplicate(c.vt, (int)P, octree_paths, c.g.bbox, c.g.quad, c.g.ndup, c.g.scan, k0, v0, (uint32_t)c.n,
+                     c.g.header + 1, stream);
+    launch_radix_sort(k0, v0, k1, v1, c.g.header, (uint32_t)c.n, c.key_bits, c.bl.sort_temp, stream);
+    launch_tile_ranges(c.bl.keys_b, c.g.header, (uint32_t)c.n, c.im.ranges, stream);
+  }
+  return check_launch(debug, stream);
+}
+
+int svr_rasterize_render(const svr_camera* cam, int n_samp, int need_depth, int need_distortion, int need_normal,
+                         int track_max_w, int64_t P, int64_t num_rendered, const float* vox_centers,
+                         const float* vox_lengths, const float* geos, const float* rgbs, void* geom_buffer,
+                         void* binning_buffer, size_t binning_bytes, void* image_buffer, size_t image_bytes,
+                         float* out_color, float* out_depth, float* out_normal, float* out_T, float* max_w, int debug,
+                         void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  FwdCtx c;
+  int st = fwd_prepare(cam, n_samp, P, num_rendered, geom_buffer, binning_buffer, binning_bytes, image_buffer,
+                       image_bytes, c);
+  if (st != SVR_OK) return st;
+  if (P == 0) return SVR_OK;
+  if (!out_color || !out_T || ((need_depth || need_distortion) && !out_depth) || (need_normal && !out_normal) ||
+      (track_max_w && !max_w) || !geos || !rgbs || !vox_centers || !vox_lengths)
+    return SVR_ERR_SHAPE;
+  if (!aligned16(geos)) return SVR_ERR_ALIGN;
+  VoxelArrays va{c.g.bbox, vox_centers, vox_lengths, geos, nullptr, rgbs};
+  FwdTileOut out{c.im.tile_last, c.im.n_contrib, out_color, out_depth, out_normal, out_T, max_w};
+  launch_render_fwd(c.vt.v[0], c.im.ranges, c.n > 0 ? c.bl.vals_b : nullptr, va, out, n_samp, need_depth != 0,
+                    need_distortion != 0, need_normal != 0, track_max_w != 0, stream);
+  return check_launch(debug, stream);
+}
+
+int svr_rasterize_forward(const svr_camera* cam, int n_samp, int need_depth, int need_distortion, int need_normal,
+                          int track_max_w, int64_t P, int64_t num_rendered, const int64_t* octree_paths,
+                          const float* vox_centers, const float* vox_lengths, const float* geos, const float* rgbs,
+                          void* geom_buffer, void* binning_buffer, size_t binning_bytes, void* image_buffer,
+                          size_t image_bytes, float* out_color, float* out_depth, float* out_normal, float* out_T,
+                          float* max_w, int debug, void* stream) {
+  int st = svr_rasterize_binning(cam, P, num_rendered, octree_paths, geom_buffer, binning_buffer, binning_bytes,
+                                 image_buffer, image_bytes, debug, stream);
+  if (st != SVR_OK) return st;
+  return svr_rasterize_render(cam, n_samp, need_depth, need_distortion, need_normal, track_max_w, P, num_rendered,
+                              vox_centers, vox_lengths, geos, rgbs, geom_buffer, binning_buffer, binning_bytes,
+                              image_buffer, image_bytes, out_color, out_depth, out_normal, out_T, max_w, debug,
+                              stream);
+}
+
+int svr_rasterize_backward(const svr_camera* cam, int n_samp, int64_t P, int64_t num_rendered,
+                           const float* vox_centers, const float* vox_lengths, const float* geos, const float* rgbs,
+                           const void* geom_buffer, const void* binning_buffer, const void* image_buffer,
+                           const float* out_T, const float* dL_dcolor, const float* dL_ddepth,
+                           const float* dL_dnormal, const float* dL_dT, float lambda_R_concen, const float* gt_color,
+                           float lambda_ascending, float lambda_dist, int need_depth, int need_normal,
+                           const float* out_depth, const float* out_normal, float* dL_dgeos, float* dL_drgbs,
+                           float* subdiv_p_bw, int debug, void* stream_) {
+  (void)out_normal;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (!valid_camera(cam) || n_samp < 1 || n_samp > kMaxSamples || P < 0 || num_rendered < 0) return SVR_ERR_SHAPE;
+  if (P == 0) return SVR_OK;
+  const bool need_dist = lambda_dist > 0;
+  if (!out_T || !dL_dcolor || !dL_dT || !dL_dgeos || !dL_drgbs || !subdiv_p_bw || (need_depth && !dL_ddepth) ||
+      (need_normal && !dL_dnormal) || (need_dist && !out_depth) || (lambda_R_concen > 0 && !gt_color))
+    return SVR_ERR_SHAPE;
+  if (!aligned16(geos)) return SVR_ERR_ALIGN;
+  const int W = cam->width, H = cam->height;
+  GeomLayout g = geom_layout(const_cast<void*>(geom_buffer), P);
+  ImageLayout im = image_layout(const_cast<void*>(image_buffer), W, H);
+  BinningLayout bl = binning_layout(const_cast<void*>(binning_buffer), (size_t)num_rendered);
+  const ViewParams vp = make_view(*cam);
+  VoxelArrays va{g.bbox, vox_centers, vox_lengths, geos, nullptr, rgbs};
+  BwdTileIn in{out_T, im.n_contrib, dL_dcolor, need_depth ? dL_ddepth : nullptr,
+               need_normal ? dL_dnormal : nullptr, dL_dT, lambda_R_concen > 0 ? gt_color : nullptr,
+               need_dist ? out_depth : nullptr, lambda_R_concen, lambda_ascending, lambda_dist};
+  BwdTileOut out{dL_dgeos, dL_drgbs, subdiv_p_bw, g.header + 1};
+  launch_render_bwd(vp, im.ranges, im.tile_last, num_rendered > 0 ? bl.vals_b : nullptr, va, in, out, n_samp,
+                    need_depth != 0, need_dist, need_normal != 0, stream);
+  return check_launch(debug, stream);
+}
+
+int svr_unpack_image_state(int width, int height, const void* image_buffer, int32_t* ranges, int32_t* tile_last,
+                           int32_t* n_contrib, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (width <= 0 || height <= 0 || !image_buffer) return SVR_ERR_SHAPE;
+  ImageLayout im = image_layout(const_cast<void*>(image_buffer), width, height);
+  const size_t T = (size_t)tiles_x(width) * tiles_y(height);
+  if (ranges) cudaMemcpyAsync(ranges, im.ranges, T * sizeof(uint2), cudaMemcpyDeviceToDevice, stream);
+  if (tile_last) cudaMemcpyAsync(tile_last, im.tile_last, T * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream);
+  if (n_contrib)
+    cudaMemcpyAsync(n_contrib, im.n_contrib, (size_t)width * height * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                    stream);
+  return check_launch(0, stream);
+}
+
+int svr_binning_sorted(const void* binning_buffer, int64_t num_rendered, int width, int height,
+                       const uint64_t** keys, const uint32_t** vals) {
+  (void)width;
+  (void)height;
+  if (!binning_buffer || num_rendered < 0) return SVR_ERR_SHAPE;
+  BinningLayout bl = binning_layout(const_cast<void*>(binning_buffer), (size_t)num_rendered);
+  if (keys) *keys = bl.keys_b;
+  if (vals) *vals = bl.vals_b;
+  return SVR_OK;
+}
+
+int svr_geom_arrays(const void* geom_buffer, int64_t P, const uint32_t** n_dup, const uint32_t** scan,
+                    const uint64_t** bboxes, const uint32_t** quads) {
+  if (!geom_buffer || P < 0) return SVR_ERR_SHAPE;
+  GeomLayout g = geom_layout(const_cast<void*>(geom_buffer), P);
+  if (n_dup) *n_dup = g.ndup;
+  if (scan) *scan = g.scan;
+  if (bboxes) *bboxes = reinterpret_cast<const uint64_t*>(g.bbox);
+  if (quads) *quads = g.quad;
+  return SVR_OK;
+}
+
+int svr_sh_compute(int degree, int64_t n_idx, const int64_t* idx, int64_t P, int M, const float* vox_centers,
+                   const float* cam_pos, const void* sh0, const void* shs, int sh_bf16, float* rgbs, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (degree < 0 || degree > 3 || P < 0 || n_idx < 0 || M < 1 || (M - 1) < (degree + 1) * (degree + 1) - 1 ||
+      (n_idx > 0 && !idx) || P >= (1ll << 31))
+    return SVR_ERR_SHAPE;
+  if (P == 0) return SVR_OK;
+  launch_sh_eval(degree, (int)n_idx, (int)P, M, idx, vox_centers, cam_pos, sh0, shs, sh_bf16 != 0, rgbs, stream);
+  return check_launch(0, stream);
+}
+
+int svr_sh_compute_bw(int degree, int M, int64_t n_idx, const int64_t* idx, int64_t P, const float* vox_centers,
+                      const float* cam_pos, const float* dL_drgbs, float* dL_dsh0, float* dL_dshs, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (degree < 0 || degree > 3 || P < 0 || n_idx < 0 || M < 1 || (M - 1) < (degree + 1) * (degree + 1) - 1 ||
+      (n_idx > 0 && !idx) || P >= (1ll << 31))
+    return SVR_ERR_SHAPE;
+  if (P == 0) return SVR_OK;
+  launch_sh_eval_bw(degree, (int)n_idx, (int)P, M, idx, vox_centers, cam_pos, dL_drgbs, dL_dsh0, dL_dshs, stream);
+  return check_launch(0, stream);
+}
+
+int svr_unbiased_adam_step(int sparse, int64_t numel, float* param, const float* grad, float* exp_avg,
+                           float* exp_avg_sq, double step, double lr, double beta1, double beta2, float eps,
+                           void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (numel < 0) return SVR_ERR_SHAPE;
+  if (numel == 0) return SVR_OK;
+  // Bias corrections in double on the host (adam_step.cu:117-122).
+  const double bc1 = 1.0 - pow(beta1, step);
+  const double bc2 = 1.0 - pow(beta2, step);
+  const double step_size = lr / bc1;
+  const double rsqrt_bc2 = 1.0 / sqrt(bc2);
+  launch_adam(false, sparse != 0, numel, param, grad, exp_avg, exp_avg_sq, (float)step_size, (float)beta1,
+              (float)beta2, (float)rsqrt_bc2, eps, stream);
+  return check_launch(0, stream);
+}
+
+int svr_biased_adam_step(int sparse, int64_t numel, float* param, const float* grad, float* exp_avg,
+                         float* exp_avg_sq, float lr, float beta1, float beta2, float eps, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (numel < 0) return SVR_ERR_SHAPE;
+  if (numel == 0) return SVR_OK;
+  launch_adam(true, sparse != 0, numel, param, grad, exp_avg, exp_avg_sq, lr, beta1, beta2, 0.f, eps, stream);
+  return check_launch(0, stream);
+}
+
+int svr_fused_adam_step(int n_groups, int sparse, void* const* params, const int* param_bf16,
+                        const float* const* grads, float* const* exp_avgs, float* const* exp_avg_sqs,
+                        const int64_t* numels, const double* steps, const double* lrs, double beta1, double beta2,
+                        float eps, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (n_groups < 0 || n_groups > kMaxAdamGroups) return SVR_ERR_SHAPE;
+  AdamGroupTable t;
+  memset(&t, 0, sizeof(t));
+  t.n = n_groups;
+  t.sparse = sparse != 0;
+  for (int i = 0; i < n_groups; ++i) {
+    if (numels[i] < 0) return SVR_ERR_SHAPE;
+    if (!aligned16(grads[i]) || !aligned16(exp_avgs[i]) || !aligned16(exp_avg_sqs[i]) ||
+        (reinterpret_cast<uintptr_t>(params[i]) & (param_bf16[i] ? 7u : 15u)))
+      return SVR_ERR_ALIGN;
+    const double bc1 = 1.0 - pow(beta1, steps[i]);
+    const double bc2 = 1.0 - pow(beta2, steps[i]);
+    AdamGroup& G = t.g[i];
+    G.param = params[i];
+    G.param_bf16 = param_bf16[i];
+    G.grad = grads[i];
+    G.exp_avg = exp_avgs[i];
+    G.exp_avg_sq = exp_avg_sqs[i];
+    G.numel = numels[i];
+    G.step_size = (float)(lrs[i] / bc1);
+    G.beta1 = (float)beta1;
+    G.beta2 = (float)beta2;
+    G.rsqrt_bc2 = (float)(1.0 / sqrt(bc2));
+    G.eps = eps;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  launch_adam_fused(t, sms, stream);
+  return check_launch(0, stream);
+}
+
+int svr_gather_grid_params(int dim, int64_t n_care, const int64_t* vox_key, const int64_t* care_idx,
+                           const float* grid_pts, float* out, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if ((dim != 1 && dim != 3) || n_care < 0 || n_care >= (1ll << 31)) return SVR_ERR_SHAPE;
+  launch_gather(dim, (int)n_care, vox_key, care_idx, grid_pts, out, stream);
+  return check_launch(0, stream);
+}
+
+int svr_gather_grid_params_bw(int dim, int64_t n_care, const int64_t* vox_key, const int64_t* care_idx,
+                              const float* dL_dvox, float* dL_dgrid, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if ((dim != 1 && dim != 3) || n_care < 0 || n_care >= (1ll << 31)) return SVR_ERR_SHAPE;
+  launch_gather_bw(dim, (int)n_care, vox_key, care_idx, dL_dvox, dL_dgrid, stream);
+  return check_launch(0, stream);
+}
+
+int svr_read_error(uint32_t* device_word, uint32_t* host_value, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  uint32_t v = 0;
+  if (cudaMemcpyAsync(&v, device_word, sizeof(v), cudaMemcpyDeviceToHost, stream) != cudaSuccess) return SVR_ERR_CUDA;
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return SVR_ERR_CUDA;
+  cudaMemsetAsync(device_word, 0, sizeof(uint32_t), stream);
+  if (host_value) *host_value = v;
+  return v ? SVR_ERR_DEVICE : SVR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,82 @@
+// Internal launcher declarations (host side of each kernel file).
+#pragma once
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "svr_views.cuh"
+
+namespace svr {
+
+struct VoxelArrays;
+struct FwdTileOut;
+struct BwdTileIn;
+struct BwdTileOut;
+
+// svr_preprocess.cu
+void launch_preprocess(const ViewTable& views, int P, const float* centers, const float* lengths, int32_t* out_ndup,
+                       uint32_t* ndup, uint2* bboxes, uint32_t* quads, cudaStream_t stream);
+
+// svr_binning.cu
+size_t scan_temp_bytes(size_t n);
+void launch_scan_inclusive(const uint32_t* in, uint32_t* out, size_t n, void* temp, uint32_t* d_total,
+                           unsigned long long cap, uint32_t* err, cudaStream_t stream);
+void launch_duplicate(const ViewTable& views, int P, const int64_t* octpaths, const uint2* bboxes,
+                      const uint32_t* quads, const uint32_t* ndup, const uint32_t* scan, uint64_t* keys,
+                      uint32_t* vals, uint32_t cap, uint32_t* err, cudaStream_t stream);
+size_t sort_temp_bytes(size_t cap);
+int sort_passes(int key_bits);
+int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, const uint32_t* d_n, uint32_t cap,
+                      int key_bits, void* temp, cudaStream_t stream);
+void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_n, uint32_t cap, uint2* ranges, cudaStream_t stream);
+
+// svr_render_fwd.cu / svr_render_bwd.cu
+void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t* vals, const VoxelArrays& va,
+                       const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
+                       cudaStream_t stream);
+void launch_render_fwd_batch(const ViewTable& views, int n_items, const int* item_view, const uint2* ranges,
+                             const uint32_t* vals, const VoxelArrays& va, int P, size_t rgb_view_stride,
+                             const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
+                             cudaStream_t stream);
+void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t* tile_last, const uint32_t* vals,
+                       const VoxelArrays& va, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
+                       bool dist, bool normal, cudaStream_t stream);
+void launch_render_bwd_batch(const ViewTable& views, int n_items, const int* item_view, const uint2* ranges,
+                             const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
+                             size_t rgb_view_stride, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
+                             bool dist, bool normal, cudaStream_t stream);
+
+// svr_sh_adam.cu
+void launch_sh_eval(int deg, int n_idx, int P, int M, const int64_t* idx, const float* centers, const float* cam_pos,
+                    const void* sh0, const void* shs, bool bf16, float* rgbs, cudaStream_t stream);
+void launch_sh_eval_bw(int deg, int n_idx, int P, int M, const int64_t* idx, const float* centers,
+                       const float* cam_pos, const float* dL_drgbs, float* dL_dsh0, float* dL_dshs,
+                       cudaStream_t stream);
+void launch_adam(bool biased, bool sparse, int64_t numel, float* param, const float* grad, float* m, float* v,
+                 float step_or_lr, float beta1, float beta2, float rsqrt_bc2, float eps, cudaStream_t stream);
+
+constexpr int kMaxAdamGroups = 8;
+struct AdamGroup {
+  void* param;         // fp32 or bf16
+  const float* grad;
+  float* exp_avg;
+  float* exp_avg_sq;
+  int64_t numel;
+  float step_size, beta1, beta2, rsqrt_bc2, eps;
+  int param_bf16;
+};
+struct AdamGroupTable {
+  int n;
+  int sparse;
+  AdamGroup g[kMaxAdamGroups];
+};
+void launch_adam_fused(const AdamGroupTable& t, int num_sms, cudaStream_t stream);
+
+void launch_gather(int dim, int n_care, const int64_t* vox_key, const int64_t* care_idx, const float* grid_pts,
+                   float* out, cudaStream_t stream);
+void launch_gather_bw(int dim, int n_care, const int64_t* vox_key, const int64_t* care_idx, const float* dL_dvox,
+                      float* dL_dgrid, cudaStream_t stream);
+
+}  // namespace svr

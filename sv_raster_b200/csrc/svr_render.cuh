@@ -1,0 +1,87 @@
+// Per-tile compositing shared by the forward and backward kernels.
+//
+// A CTA of 256 threads owns one 16x16 pixel tile; each warp owns an 8x4
+// micro-tile (forward.cu:77-92).  Voxel instances of the tile's sorted list
+// are staged into shared memory in batches of kBatch records (structure of
+// arrays, vector loads where the layout allows), then every warp builds a
+// ballot mask of the staged records whose packed bbox overlaps its 8x4
+// micro-tile and whose camera quadrant matches a ray quadrant present in the
+// warp.  Lanes walk only those records, in list order, so every pixel sees
+// exactly the records the reference's per-pixel loop would accept
+// (forward.cu:182-200), in the same order, with the same arithmetic.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "svr_common.cuh"
+#include "svr_views.cuh"
+
+namespace svr {
+
+constexpr int kBatch = 256;              // records staged per round (one per thread)
+constexpr int kGroups = kBatch / 32;     // 32-record ballot groups per round
+
+// Voxel attributes of one view as the kernels read them.
+struct VoxelArrays {
+  const uint2* bboxes;        // [P] packed pixel bbox (this view)
+  const float* centers;       // [P,3]
+  const float* lengths;       // [P]
+  const float* geos;          // [P,8] fp32, or nullptr when geos_bf16 is set
+  const __nv_bfloat16* geos_bf16;  // [P,8] bf16 storage
+  const float* rgbs;          // [P,3] (this view)
+};
+
+struct StageSmem {
+  uint2 bbox[kBatch];
+  float4 cl[kBatch];          // centre xyz, edge length
+  float4 geo[kBatch][2];      // 8 corner densities
+  float4 rgbv[kBatch];        // rgb, voxel id (as int bits)
+  uint32_t val[kBatch];       // sorted value (quadrant << 29 | voxel id)
+};
+
+__device__ __forceinline__ void stage_record(StageSmem& s, int slot, uint32_t val, const VoxelArrays& va) {
+  const uint32_t vid = val_vox_id(val);
+  s.val[slot] = val;
+  s.bbox[slot] = va.bboxes[vid];
+  const float* c = va.centers + 3 * (size_t)vid;
+  s.cl[slot] = make_float4(c[0], c[1], c[2], va.lengths[vid]);
+  if (va.geos_bf16) {
+    const uint4 raw = *reinterpret_cast<const uint4*>(va.geos_bf16 + 8 * (size_t)vid);
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&raw);
+    const float2 g0 = __bfloat1622float2(h[0]), g1 = __bfloat1622float2(h[1]);
+    const float2 g2 = __bfloat1622float2(h[2]), g3 = __bfloat1622float2(h[3]);
+    s.geo[slot][0] = make_float4(g0.x, g0.y, g1.x, g1.y);
+    s.geo[slot][1] = make_float4(g2.x, g2.y, g3.x, g3.y);
+  } else {
+    const float4* g = reinterpret_cast<const float4*>(va.geos + 8 * (size_t)vid);
+    s.geo[slot][0] = g[0];
+    s.geo[slot][1] = g[1];
+  }
+  const float* rgb = va.rgbs + 3 * (size_t)vid;
+  s.rgbv[slot] = make_float4(rgb[0], rgb[1], rgb[2], __int_as_float((int)vid));
+}
+
+// Does staged record `slot` possibly touch a pixel of this warp's 8x4
+// micro-tile with a matching ray quadrant?
+__device__ __forceinline__ bool record_hits_warp(const StageSmem& s, int slot, uint32_t wx0, uint32_t wy0,
+                                                 uint32_t quad_mask) {
+  const uint2 bb = s.bbox[slot];
+  const uint32_t q = val_quadrant(s.val[slot]);
+  return bb_xmin(bb) <= wx0 + 7u && bb_xmax(bb) >= wx0 && bb_ymin(bb) <= wy0 + 3u && bb_ymax(bb) >= wy0 &&
+         ((quad_mask >> q) & 1u);
+}
+
+__device__ __forceinline__ void load_geo(const StageSmem& s, int j, float g[8]) {
+  const float4 a = s.geo[j][0], b = s.geo[j][1];
+  g[0] = a.x; g[1] = a.y; g[2] = a.z; g[3] = a.w;
+  g[4] = b.x; g[5] = b.y; g[6] = b.z; g[7] = b.w;
+}
+
+// Linear-gradient "normal" of the trilinear field (forward.cu:301-310).
+__device__ __forceinline__ void field_normal(const float g[8], float& nx, float& ny, float& nz) {
+  nx = ((g[4] + g[5] + g[6] + g[7]) - (g[0] + g[1] + g[2] + g[3]));
+  ny = ((g[2] + g[3] + g[6] + g[7]) - (g[0] + g[1] + g[4] + g[5]));
+  nz = ((g[1] + g[3] + g[5] + g[7]) - (g[0] + g[2] + g[4] + g[6]));
+}
+
+}  // namespace svr

@@ -1,0 +1,332 @@
+// Backward compositing of one 16x16 tile: walks the tile's list back to
+// front from tile_last, recovers transmittance by division and accumulates
+// per-voxel gradients.
+//
+// Per-pixel arithmetic mirrors BACKWARD::renderCUDA (backward.cu:35-530):
+// contributor skip (:246-248), recomputed quadrature with dI/dgeo
+// (:295-323), T recovery (:333), colour / distortion / normal / depth /
+// ascending / colour-concentration terms (:344-510) and the 12-float
+// gradient pack (:515-522).  The reference issues 12 global atomics per
+// contributing (pixel, voxel); here each warp reduces its lanes' gradients
+// with shuffles into a shared-memory accumulator per staged record, and each
+// record is flushed once per tile with 12 global reductions.
+#pragma once
+
+#include "svr_render.cuh"
+
+namespace svr {
+
+struct BwdTileIn {
+  const float* T;          // [H*W] final transmittance from the forward
+  const uint32_t* n_contrib;
+  const float* dL_dcolor;  // [3,H,W]
+  const float* dL_ddepth;  // [3,H,W] or nullptr
+  const float* dL_dnormal; // [3,H,W] or nullptr
+  const float* dL_dT;      // [H*W]
+  const float* gt_color;   // [3,H,W] or nullptr
+  const float* out_depth;  // [3,H,W] or nullptr (distortion prefix sums)
+  float lambda_R_concen, lambda_ascending, lambda_dist;
+};
+
+struct BwdTileOut {
+  float* dL_dgeos;   // [P,8]
+  float* dL_drgbs;   // [P,3] (this view)
+  float* subdiv;     // [P]
+  uint32_t* err;     // device error word
+};
+
+constexpr int kGradStride = 13;  // 12 gradient floats + 1 pad (bank spread)
+
+__device__ __forceinline__ float warp_sum(float x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+template <int NS, bool DEPTH, bool DIST, bool NORMAL>
+__device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const float* __restrict__ c2w_s, int tile_x,
+                                                int tile_y, uint2 range_raw, uint32_t tile_last,
+                                                const uint32_t* __restrict__ vals, const VoxelArrays& va,
+                                                const BwdTileIn& in, const BwdTileOut& out, StageSmem& s,
+                                                float* s_grad /*[kBatch*kGradStride]*/) {
+  const int W = vp.W, H = vp.H;
+  const int tid = threadIdx.x, lane = tid & 31;
+  int lx, ly;
+  tile_pixel(tid, lx, ly);
+  const uint32_t px = tile_x * kTileX + lx, py = tile_y * kTileY + ly;
+  const uint32_t pix_id = (uint32_t)W * py + px;
+  const bool inside = px < (uint32_t)W && py < (uint32_t)H;
+  const PixelRay ray = make_pixel_ray((float)px, (float)py, W, H, vp.tanfovx, vp.tanfovy, vp.cx, vp.cy, c2w_s);
+  const int warp = tid >> 5;
+  const uint32_t wx0 = tile_x * kTileX + (warp & 1) * 8, wy0 = tile_y * kTileY + (warp >> 1) * 4;
+
+  // Range check (replaces the __trap at backward.cu:122-133).
+  if (tile_last > range_raw.y || range_raw.x > tile_last) {
+    if (tid == 0) atomicOr(out.err, SVR_DEVERR_RANGE);
+    return;
+  }
+  const uint2 range = make_uint2(range_raw.x, tile_last);
+  const size_t HW = (size_t)H * W;
+
+  const float T_final = inside ? in.T[pix_id] : 0.f;
+  float T = T_final;
+  const int todo_total = (int)(range.y - range.x);
+  const uint32_t last_contrib = inside ? in.n_contrib[pix_id] : 0u;
+
+  float gx = 0.f, gy = 0.f, gz = 0.f, last_dL_dT = 0.f, dL_dD = 0.f;
+  float dNx = 0.f, dNy = 0.f, dNz = 0.f;
+  if (inside) {
+    gx = in.dL_dcolor[0 * HW + pix_id];
+    gy = in.dL_dcolor[1 * HW + pix_id];
+    gz = in.dL_dcolor[2 * HW + pix_id];
+    const float dT = in.dL_dT[pix_id];
+    last_dL_dT = dT + vp.bg * (gx + gy + gz);
+    if (DEPTH) dL_dD = in.dL_ddepth[pix_id] * ray.rd_norm_inv;
+    if (NORMAL) {
+      dNx = in.dL_dnormal[0 * HW + pix_id];
+      dNy = in.dL_dnormal[1 * HW + pix_id];
+      dNz = in.dL_dnormal[2 * HW + pix_id];
+    }
+  }
+  const float WH_inv = 1.f / ((float)(W * H));
+  const float weight_R = in.lambda_R_concen * WH_inv;
+  const float weight_asc = in.lambda_ascending * WH_inv;
+  float gtx = 0.f, gty = 0.f, gtz = 0.f;
+  if (in.lambda_R_concen > 0 && inside) {
+    gtx = in.gt_color[0 * HW + pix_id];
+    gty = in.gt_color[1 * HW + pix_id];
+    gtz = in.gt_color[2 * HW + pix_id];
+  }
+  const float weight_dist = in.lambda_dist * WH_inv;
+  float prefix_wm = 0.f, suffix_wm = 0.f, prefix_w = 0.f, suffix_w = 0.f;
+  if (DIST && inside) {
+    prefix_wm = in.out_depth[HW + pix_id];
+    prefix_w = 1.f - T_final;
+  }
+
+  for (int i = tid; i < kBatch * kGradStride; i += kBatch) s_grad[i] = 0.f;
+  // Largest contributor count of this warp: records at or beyond it are skipped by every lane.
+  const uint32_t warp_lc = __reduce_max_sync(0xffffffffu, last_contrib);
+  const uint32_t quad_mask = __reduce_or_sync(0xffffffffu, inside ? (1u << ray.quad) : 0u);
+
+  const int rounds = (todo_total + kBatch - 1) / kBatch;
+  for (int r = 0; r < rounds; ++r) {
+    __syncthreads();
+    const int base = r * kBatch;                     // records [base, base+n_here) from the back
+    const int n_here = min(kBatch, todo_total - base);
+    if (tid < n_here) stage_record(s, tid, vals[range.y - base - tid - 1], va);
+    __syncthreads();
+
+    // Position (relative to range.x) of staged slot j is todo_total - base - j - 1.
+    for (int g = 0; g < kGroups && g * 32 < n_here; ++g) {
+      const int slot = g * 32 + lane;
+      const uint32_t pos = (uint32_t)(todo_total - base - slot - 1);
+      const bool hit = slot < n_here && pos < warp_lc && record_hits_warp(s, slot, wx0, wy0, quad_mask);
+      uint32_t m = __ballot_sync(0xffffffffu, hit);
+      while (m) {
+        const int j = g * 32 + __ffs(m) - 1;
+        m &= m - 1;
+        const uint32_t jpos = (uint32_t)(todo_total - base - j - 1);
+        bool contrib = false;
+        float gp[12];
+        if (inside && jpos < last_contrib) {
+          const uint32_t val = s.val[j];
+          if (pixel_in_bbox(px, py, s.bbox[j]) && ray.quad == val_quadrant(val)) {
+            const float4 cl = s.cl[j];
+            const float2 ab = ray_box(cl.x, cl.y, cl.z, cl.w, ray);
+            const float a = ab.x, b = ab.y;
+            if (!(a > b)) {
+              float geo[8];
+              load_geo(s, j, geo);
+              float dgeo[8];
+#pragma unroll
+              for (int c = 0; c < 8; ++c) dgeo[c] = 0.f;
+              float vol_int = 0.f;
+              float dI_dgeo[8];
+#pragma unroll
+              for (int c = 0; c < 8; ++c) dI_dgeo[c] = 0.f;
+              float each_dI[NS][8];
+              float w[8];
+              float local_alpha[NS];
+              const float vox_l_inv = 1.f / cl.w;
+              const float step_sz = (b - a) * (1.f / NS);
+              const float stx = step_sz * ray.dx, sty = step_sz * ray.dy, stz = step_sz * ray.dz;
+              const float t0 = a + 0.5f * step_sz;
+              const float ptx = ray.ox + t0 * ray.dx, pty = ray.oy + t0 * ray.dy, ptz = ray.oz + t0 * ray.dz;
+              float qx = (ptx - (cl.x - 0.5f * cl.w)) * vox_l_inv;
+              float qy = (pty - (cl.y - 0.5f * cl.w)) * vox_l_inv;
+              float qz = (ptz - (cl.z - 0.5f * cl.w)) * vox_l_inv;
+              const float qsx = stx * vox_l_inv, qsy = sty * vox_l_inv, qsz = stz * vox_l_inv;
+#pragma unroll
+              for (int k = 0; k < NS; ++k) {
+                trilinear_weights(qx, qy, qz, w);
+                float d = 0.f;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) d += geo[c] * w[c];
+                const float lvi = kStepScale * step_sz * density_act(d);
+                vol_int += lvi;
+                if (DEPTH && NS > 1) local_alpha[k] = fminf(kMaxAlpha, 1.f - expf(-lvi));
+                const float dd_dd = kStepScale * step_sz * density_act_grad(d);
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                  const float tmp = dd_dd * w[c];
+                  dI_dgeo[c] += tmp;
+                  if (DEPTH && NS > 1) each_dI[k][c] = tmp;
+                }
+                qx = qx + qsx; qy = qy + qsy; qz = qz + qsz;
+              }
+              const float exp_neg = expf(-vol_int);
+              const float alpha = fminf(kMaxAlpha, 1.f - exp_neg);
+              if (!(alpha < kMinAlpha)) {
+                contrib = true;
+                T = T / (1.f - alpha);
+                const float pt_w = alpha * T;
+                const float4 rgbv = s.rgbv[j];
+                float dL_dpt_w = gx * rgbv.x + gy * rgbv.y + gz * rgbv.z;
+                if (DIST) {
+                  const float adist = contract_depth(a), bdist = contract_depth(b);
+                  const float now_m = 0.5f * (adist + bdist);
+                  const float now_wm = now_m * pt_w;
+                  prefix_wm -= now_wm;
+                  prefix_w -= pt_w;
+                  const float uni = 0.6666666f * pt_w * (bdist - adist);
+                  const float bi = 2.f * (now_m * (prefix_w - suffix_w) - (prefix_wm - suffix_wm));
+                  dL_dpt_w += weight_dist * (uni + bi);
+                  suffix_wm += now_wm;
+                  suffix_w += pt_w;
+                }
+                if (NORMAL) {
+                  float nx, ny, nz;
+                  field_normal(geo, nx, ny, nz);
+                  const float rl = safe_rnorm3(nx, ny, nz);
+                  const float sx = rl * nx, sy = rl * ny, sz = rl * nz;
+                  dL_dpt_w += dNx * sx + dNy * sy + dNz * sz;
+                  const float dsx = pt_w * dNx, dsy = pt_w * dNy, dsz = pt_w * dNz;
+                  const float dot_ = dsx * nx + dsy * ny + dsz * nz;
+                  const float lnx = rl * (dsx - dot_ * rl * sx);
+                  const float lny = rl * (dsy - dot_ * rl * sy);
+                  const float lnz = rl * (dsz - dot_ * rl * sz);
+                  dgeo[0] += -lnx - lny - lnz;
+                  dgeo[1] += -lnx - lny + lnz;
+                  dgeo[2] += -lnx + lny - lnz;
+                  dgeo[3] += -lnx + lny + lnz;
+                  dgeo[4] += +lnx - lny - lnz;
+                  dgeo[5] += +lnx - lny + lnz;
+                  dgeo[6] += +lnx + lny - lnz;
+                  dgeo[7] += +lnx + lny + lnz;
+                }
+                const float dL_dalpha = T * (dL_dpt_w - last_dL_dT);
+                last_dL_dT += alpha * (dL_dpt_w - last_dL_dT);
+                const float dL_dI = dL_dalpha * exp_neg;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) dgeo[c] += dL_dI * dI_dgeo[c];
+                if (DEPTH) {
+                  float dval;
+                  float dI[NS];
+                  if (NS == 3) {
+                    const float ss = 0.3333333f * (b - a);
+                    const float a0 = local_alpha[0], a1 = local_alpha[NS > 1 ? 1 : 0], a2 = local_alpha[NS > 2 ? 2 : 0];
+                    const float t0_ = a + 0.5f * ss, t1_ = a + 1.5f * ss, t2_ = a + 2.5f * ss;
+                    dval = a0 * t0_ + (1.f - a0) * a1 * t1_ + (1.f - a0) * (1.f - a1) * a2 * t2_;
+                    dI[0] = dL_dD * T * (t0_ + a1 * a2 * t2_ - a1 * t1_ - a2 * t2_) * (1.f - a0);
+                    dI[NS > 1 ? 1 : 0] = dL_dD * T * (t1_ + a0 * a2 * t2_ - a0 * t1_ - a2 * t2_) * (1.f - a1);
+                    dI[NS > 2 ? 2 : 0] = dL_dD * T * (t2_ + a0 * a1 * t2_ - a0 * t2_ - a1 * t2_) * (1.f - a2);
+                  } else if (NS == 2) {
+                    const float ss = 0.5f * (b - a);
+                    const float a0 = local_alpha[0], a1 = local_alpha[NS > 1 ? 1 : 0];
+                    const float t0_ = a + 0.5f * ss, t1_ = a + 1.5f * ss;
+                    dval = a0 * t0_ + (1.f - a0) * a1 * t1_;
+                    dI[0] = dL_dD * T * (t0_ - a1 * t1_) * (1.f - a0);
+                    dI[NS > 1 ? 1 : 0] = dL_dD * T * (t1_ - a0 * t1_) * (1.f - a1);
+                  } else {
+                    const float t0_ = 0.5f * (a + b);
+                    dval = alpha * t0_;
+                    dI[0] = dL_dD * T * t0_ * (1.f - alpha);
+                  }
+                  last_dL_dT += dL_dD * dval;
+                  if (NS == 3) {
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                      dgeo[c] += dI[0] * each_dI[0][c] + dI[NS > 1 ? 1 : 0] * each_dI[NS > 1 ? 1 : 0][c] +
+                                 dI[NS > 2 ? 2 : 0] * each_dI[NS > 2 ? 2 : 0][c];
+                  } else if (NS == 2) {
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                      dgeo[c] += dI[0] * each_dI[0][c] + dI[NS > 1 ? 1 : 0] * each_dI[NS > 1 ? 1 : 0][c];
+                  } else {
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) dgeo[c] += dI[0] * dI_dgeo[c];
+                  }
+                }
+                if (in.lambda_ascending > 0) {
+                  const float lo_x = cl.x - 0.5f * cl.w, lo_y = cl.y - 0.5f * cl.w, lo_z = cl.z - 0.5f * cl.w;
+                  const float pax = ray.ox + a * ray.dx, pay = ray.oy + a * ray.dy, paz = ray.oz + a * ray.dz;
+                  const float pbx = ray.ox + b * ray.dx, pby = ray.oy + b * ray.dy, pbz = ray.oz + b * ray.dz;
+                  float wa[8], wb[8];
+                  trilinear_weights((pax - lo_x) * vox_l_inv, (pay - lo_y) * vox_l_inv, (paz - lo_z) * vox_l_inv, wa);
+                  trilinear_weights((pbx - lo_x) * vox_l_inv, (pby - lo_y) * vox_l_inv, (pbz - lo_z) * vox_l_inv, wb);
+                  float d_a = 0.f, d_b = 0.f;
+#pragma unroll
+                  for (int c = 0; c < 8; ++c) {
+                    d_a += geo[c] * wa[c];
+                    d_b += geo[c] * wb[c];
+                  }
+                  const float reg_w = weight_asc * pt_w * static_cast<float>(d_a > d_b);
+#pragma unroll
+                  for (int c = 0; c < 8; ++c) dgeo[c] += reg_w * (wa[c] - wb[c]);
+                }
+                float drx = pt_w * gx, dry = pt_w * gy, drz = pt_w * gz;
+                if (in.lambda_R_concen > 0) {
+                  const float sR = weight_R * pt_w * 2.0f;
+                  drx += sR * (rgbv.x - gtx);
+                  dry += sR * (rgbv.y - gty);
+                  drz += sR * (rgbv.z - gtz);
+                }
+#pragma unroll
+                for (int c = 0; c < 8; ++c) gp[c] = dgeo[c];
+                gp[8] = drx; gp[9] = dry; gp[10] = drz;
+                gp[11] = fabsf(dL_dalpha * alpha);
+              }
+            }
+          }
+        }
+        // Warp reduction of this record's gradients into its shared accumulator.
+        const uint32_t act = __ballot_sync(0xffffffffu, contrib);
+        if (act == 0u) continue;
+        float* acc = s_grad + j * kGradStride;
+        if (__popc(act) == 1) {
+          if (contrib) {
+#pragma unroll
+            for (int c = 0; c < 12; ++c) atomicAdd(acc + c, gp[c]);
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < 12; ++c) {
+            const float v = warp_sum(contrib ? gp[c] : 0.f);
+            if (lane == c) atomicAdd(acc + c, v);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // Flush this batch's accumulators: one set of reductions per (voxel, tile).
+    if (tid < n_here) {
+      float* acc = s_grad + tid * kGradStride;
+      float gsum = 0.f;
+#pragma unroll
+      for (int c = 0; c < 12; ++c) gsum += fabsf(acc[c]);
+      if (gsum != 0.f) {
+        const uint32_t vid = val_vox_id(s.val[tid]);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) atomicAdd(out.dL_dgeos + 8 * (size_t)vid + c, acc[c]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) atomicAdd(out.dL_drgbs + 3 * (size_t)vid + c, acc[8 + c]);
+        atomicAdd(out.subdiv + vid, acc[11]);
+      }
+#pragma unroll
+      for (int c = 0; c < 12; ++c) acc[c] = 0.f;
+    }
+  }
+}
+
+}  // namespace svr

@@ -1,0 +1,218 @@
+// Forward compositing of one 16x16 tile: front-to-back alpha blending of the
+// tile's sorted voxel instances with trilinear density quadrature.
+//
+// Per-pixel arithmetic mirrors FORWARD::renderCUDA (forward.cu:39-392):
+// ray setup (:100-111), slab test (:192), n_samp midpoint quadrature
+// (:228-248), alpha clamp and MIN_ALPHA skip (:251-253), colour / depth /
+// distortion / normal accumulation (:256-313), early stop at T < 1e-4
+// (:315-316), median-depth refinement (:328-364) and outputs (:368-391).
+// Differences are in scheduling only: SoA staging, warp-ballot culling of the
+// staged batch, a single pass per pixel instead of the collect-then-process
+// two-pass with a 256-entry local array, and a CTA reduction for tile_last.
+#pragma once
+
+#include "svr_render.cuh"
+
+namespace svr {
+
+struct FwdTileOut {
+  uint32_t* tile_last;   // [T] of this view
+  uint32_t* n_contrib;   // [H*W] of this view
+  float* color;          // [3,H,W]
+  float* depth;          // [3,H,W] or nullptr
+  float* normal;         // [3,H,W] or nullptr
+  float* T;              // [H*W]
+  float* max_w;          // [P] or nullptr
+};
+
+template <int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
+__device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const float* __restrict__ c2w_s, int tile_x,
+                                                int tile_y, uint2 range, const uint32_t* __restrict__ vals,
+                                                const VoxelArrays& va, const FwdTileOut& out, StageSmem& s,
+                                                uint32_t* s_red) {
+  const int W = vp.W, H = vp.H;
+  const int tid = threadIdx.x;
+  const int tile_id = tile_y * vp.grid_x + tile_x;
+  int lx, ly;
+  tile_pixel(tid, lx, ly);
+  const uint32_t px = tile_x * kTileX + lx, py = tile_y * kTileY + ly;
+  const uint32_t pix_id = (uint32_t)W * py + px;
+  const bool inside = px < (uint32_t)W && py < (uint32_t)H;
+  const PixelRay ray = make_pixel_ray((float)px, (float)py, W, H, vp.tanfovx, vp.tanfovy, vp.cx, vp.cy, c2w_s);
+  const int warp = tid >> 5;
+  const uint32_t wx0 = tile_x * kTileX + (warp & 1) * 8, wy0 = tile_y * kTileY + (warp >> 1) * 4;
+
+  bool done = !inside;
+  float T = 1.f;
+  float Cx = 0.f, Cy = 0.f, Cz = 0.f;
+  float Nx = 0.f, Ny = 0.f, Nz = 0.f;
+  float D = 0.f, Ddist = 0.f;
+  int dmed_vid = -1;
+  float dmed_T = 0.f;
+  uint32_t last_contrib = 0;
+
+  const int todo_total = (int)(range.y - range.x);
+  const int rounds = (todo_total + kBatch - 1) / kBatch;
+  for (int r = 0; r < rounds; ++r) {
+    // All pixels finished: stop (also the barrier that frees the staging buffer).
+    if (__syncthreads_count(done) == kBatch) break;
+    const int base = r * kBatch;
+    const int n_here = min(kBatch, todo_total - base);
+    if (tid < n_here) stage_record(s, tid, vals[range.x + base + tid], va);
+    __syncthreads();
+
+    const uint32_t quad_mask = __reduce_or_sync(0xffffffffu, done ? 0u : (1u << ray.quad));
+    if (quad_mask == 0u) continue;  // whole warp finished
+    for (int g = 0; g < kGroups && g * 32 < n_here; ++g) {
+      const int slot = g * 32 + (tid & 31);
+      const bool hit = slot < n_here && record_hits_warp(s, slot, wx0, wy0, quad_mask);
+      uint32_t m = __ballot_sync(0xffffffffu, hit);
+      while (m) {
+        const int j = g * 32 + __ffs(m) - 1;
+        m &= m - 1;
+        if (done) continue;
+        const uint32_t val = s.val[j];
+        if (!pixel_in_bbox(px, py, s.bbox[j]) || ray.quad != val_quadrant(val)) continue;
+        const float4 cl = s.cl[j];
+        const float2 ab = ray_box(cl.x, cl.y, cl.z, cl.w, ray);
+        const float a = ab.x, b = ab.y;
+        if (a > b) continue;
+
+        float geo[8];
+        load_geo(s, j, geo);
+        float vol_int = 0.f;
+        float w[8];
+        float local_alpha[NS];
+        const float vox_l_inv = 1.f / cl.w;
+        const float step_sz = (b - a) * (1.f / NS);
+        const float stx = step_sz * ray.dx, sty = step_sz * ray.dy, stz = step_sz * ray.dz;
+        const float t0 = a + 0.5f * step_sz;
+        const float ptx = ray.ox + t0 * ray.dx, pty = ray.oy + t0 * ray.dy, ptz = ray.oz + t0 * ray.dz;
+        float qx = (ptx - (cl.x - 0.5f * cl.w)) * vox_l_inv;
+        float qy = (pty - (cl.y - 0.5f * cl.w)) * vox_l_inv;
+        float qz = (ptz - (cl.z - 0.5f * cl.w)) * vox_l_inv;
+        const float qsx = stx * vox_l_inv, qsy = sty * vox_l_inv, qsz = stz * vox_l_inv;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          trilinear_weights(qx, qy, qz, w);
+          float d = 0.f;
+#pragma unroll
+          for (int c = 0; c < 8; ++c) d += geo[c] * w[c];
+          const float lvi = kStepScale * step_sz * density_act(d);
+          vol_int += lvi;
+          if (DEPTH && NS > 1) local_alpha[k] = fminf(kMaxAlpha, 1.f - expf(-lvi));
+          qx = qx + qsx; qy = qy + qsy; qz = qz + qsz;
+        }
+        const float alpha = fminf(kMaxAlpha, 1.f - expf(-vol_int));
+        if (alpha < kMinAlpha) continue;
+
+        const float pt_w = T * alpha;
+        const float4 rgbv = s.rgbv[j];
+        Cx = Cx + pt_w * rgbv.x;
+        Cy = Cy + pt_w * rgbv.y;
+        Cz = Cz + pt_w * rgbv.z;
+        if (DEPTH) {
+          float dval;
+          if (NS == 3) {
+            const float ss = 0.3333333f * (b - a);
+            const float a0 = local_alpha[0], a1 = local_alpha[NS > 1 ? 1 : 0], a2 = local_alpha[NS > 2 ? 2 : 0];
+            const float t0_ = a + 0.5f * ss, t1_ = a + 1.5f * ss, t2_ = a + 2.5f * ss;
+            dval = a0 * t0_ + (1.f - a0) * a1 * t1_ + (1.f - a0) * (1.f - a1) * a2 * t2_;
+          } else if (NS == 2) {
+            const float ss = 0.5f * (b - a);
+            const float a0 = local_alpha[0], a1 = local_alpha[NS > 1 ? 1 : 0];
+            const float t0_ = a + 0.5f * ss, t1_ = a + 1.5f * ss;
+            dval = a0 * t0_ + (1.f - a0) * a1 * t1_;
+          } else {
+            dval = alpha * 0.5f * (a + b);
+          }
+          D = D + T * dval;
+          if (T > 0.5f) {
+            dmed_vid = __float_as_int(rgbv.w);
+            dmed_T = T;
+          }
+        }
+        if (DIST) Ddist = Ddist + pt_w * 0.5f * (contract_depth(a) + contract_depth(b));
+        if (NORMAL) {
+          float nx, ny, nz;
+          field_normal(geo, nx, ny, nz);
+          const float rl = safe_rnorm3(nx, ny, nz);
+          Nx = Nx + pt_w * rl * nx;
+          Ny = Ny + pt_w * rl * ny;
+          Nz = Nz + pt_w * rl * nz;
+        }
+        T *= (1.f - alpha);
+        done |= (T < kEarlyStopT);
+        last_contrib = (uint32_t)(base + j + 1);
+        if (MAXW) atomicMax(reinterpret_cast<int*>(out.max_w) + __float_as_int(rgbv.w), __float_as_int(pt_w));
+      }
+    }
+  }
+
+  float Dmed = 0.f;
+  if (DEPTH && inside && dmed_vid != -1) {
+    // Median depth refined with 16 samples inside the voxel where T crosses 0.5.
+    constexpr int kMedSamples = 16;
+    const float* c = va.centers + 3 * (size_t)dmed_vid;
+    const float cxv = c[0], cyv = c[1], czv = c[2], lv = va.lengths[dmed_vid];
+    float geo[8];
+    if (va.geos_bf16) {
+      for (int k = 0; k < 8; ++k) geo[k] = __bfloat162float(va.geos_bf16[8 * (size_t)dmed_vid + k]);
+    } else {
+      for (int k = 0; k < 8; ++k) geo[k] = va.geos[8 * (size_t)dmed_vid + k];
+    }
+    const float2 ab = ray_box(cxv, cyv, czv, lv, ray);
+    const float a = ab.x, b = ab.y;
+    const float vox_l_inv = 1.f / lv;
+    const float step_sz = (b - a) * (1.f / kMedSamples);
+    const float stx = step_sz * ray.dx, sty = step_sz * ray.dy, stz = step_sz * ray.dz;
+    const float t0 = a + 0.5f * step_sz;
+    const float ptx = ray.ox + t0 * ray.dx, pty = ray.oy + t0 * ray.dy, ptz = ray.oz + t0 * ray.dz;
+    float qx = (ptx - (cxv - 0.5f * lv)) * vox_l_inv;
+    float qy = (pty - (cyv - 0.5f * lv)) * vox_l_inv;
+    float qz = (ptz - (czv - 0.5f * lv)) * vox_l_inv;
+    const float qsx = stx * vox_l_inv, qsy = sty * vox_l_inv, qsz = stz * vox_l_inv;
+    Dmed = a - 0.5f * step_sz;
+    for (int k = 0; k < kMedSamples && dmed_T > 0.5f; k++) {
+      Dmed += step_sz;
+      float w[8];
+      trilinear_weights(qx, qy, qz, w);
+      float d = 0.f;
+      for (int cc = 0; cc < 8; ++cc) d += geo[cc] * w[cc];
+      const float vol_int = kStepScale * step_sz * density_act(d);
+      dmed_T *= expf(-vol_int);
+      qx = qx + qsx; qy = qy + qsy; qz = qz + qsz;
+    }
+  }
+
+  const size_t HW = (size_t)H * W;
+  if (inside) {
+    out.n_contrib[pix_id] = last_contrib;
+    out.color[0 * HW + pix_id] = Cx + T * vp.bg;
+    out.color[1 * HW + pix_id] = Cy + T * vp.bg;
+    out.color[2 * HW + pix_id] = Cz + T * vp.bg;
+    out.T[pix_id] = T;
+    if (DEPTH) {
+      out.depth[pix_id] = D * ray.rd_norm_inv;
+      out.depth[2 * HW + pix_id] = Dmed * ray.rd_norm_inv;
+    }
+    if (DIST) out.depth[HW + pix_id] = Ddist;
+    if (NORMAL) {
+      out.normal[0 * HW + pix_id] = Nx;
+      out.normal[1 * HW + pix_id] = Ny;
+      out.normal[2 * HW + pix_id] = Nz;
+    }
+  }
+  // tile_last = range start + the largest contributor count of the tile.
+  const uint32_t lc = __reduce_max_sync(0xffffffffu, inside ? last_contrib : 0u);
+  if ((tid & 31) == 0) s_red[tid >> 5] = lc;
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int w = 0; w < kBatch / 32; ++w) m = max(m, s_red[w]);
+    out.tile_last[tile_id] = range.x + m;
+  }
+}
+
+}  // namespace svr

@@ -1,0 +1,359 @@
+// Spherical-harmonics colour, Adam updates and grid-point gathers.
+//
+// SH: follows computeColorFromSH / _bw (backends/cuda/src/sh_compute.cu:54-176)
+// expression for expression, so colours are bit-identical.  Degree is a
+// template parameter; fp32 and bf16 coefficient storage are supported.
+//
+// Adam: unbiased_adam_step_cuda_kernel / biased_... (adam_step.cu:28-102)
+// with the host-side double bias correction (adam_step.cu:117-122), plus a
+// fused multi-group form that updates several parameter groups in one launch.
+//
+// Gather: gather_triinterp_geo_params(_bw) / feat (geo_params_gather.cu:22-130).
+#include <cuda_bf16.h>
+
+#include "svr_common.cuh"
+#include "svr_kernels.h"
+
+namespace svr {
+
+// Real SH basis normalisation constants (degrees 0-3).
+__device__ constexpr float kC0 = 0.28209479177387814f;
+__device__ constexpr float kC1 = 0.4886025119029199f;
+__device__ constexpr float kC2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f,
+                                     -1.0925484305920792f, 0.5462742152960396f};
+__device__ constexpr float kC3[7] = {-0.5900435899266435f, 2.890611442640554f, -0.4570457994644658f,
+                                     0.3731763325901154f, -0.4570457994644658f, 1.445305721320277f,
+                                     -0.5900435899266435f};
+
+template <typename TS>
+__device__ __forceinline__ float ldf(const TS* p, size_t i) {
+  if constexpr (sizeof(TS) == 2) return __bfloat162float(p[i]);
+  else return p[i];
+}
+
+// rgb of one channel `c`; `sh` points at the voxel's (M-1) x 3 rest coefficients.
+template <int DEG, typename TS>
+__device__ __forceinline__ float sh_channel(float x, float y, float z, float base0, const TS* sh, int c) {
+  float r = kC0 * base0;
+  if (DEG > 0) {
+    r = r - kC1 * y * ldf(sh, 0 * 3 + c) + kC1 * z * ldf(sh, 1 * 3 + c) - kC1 * x * ldf(sh, 2 * 3 + c);
+    if (DEG > 1) {
+      const float xx = x * x, yy = y * y, zz = z * z;
+      const float xy = x * y, yz = y * z, xz = x * z;
+      r = r + kC2[0] * xy * ldf(sh, 3 * 3 + c) + kC2[1] * yz * ldf(sh, 4 * 3 + c) +
+          kC2[2] * (2.0f * zz - xx - yy) * ldf(sh, 5 * 3 + c) + kC2[3] * xz * ldf(sh, 6 * 3 + c) +
+          kC2[4] * (xx - yy) * ldf(sh, 7 * 3 + c);
+      if (DEG > 2) {
+        r = r + kC3[0] * y * (3.0f * xx - yy) * ldf(sh, 8 * 3 + c) + kC3[1] * xy * z * ldf(sh, 9 * 3 + c) +
+            kC3[2] * y * (4.0f * zz - xx - yy) * ldf(sh, 10 * 3 + c) +
+            kC3[3] * z * (2.0f * zz - 3.0f * xx - 3.0f * yy) * ldf(sh, 11 * 3 + c) +
+            kC3[4] * x * (4.0f * zz - xx - yy) * ldf(sh, 12 * 3 + c) + kC3[5] * z * (xx - yy) * ldf(sh, 13 * 3 + c) +
+            kC3[6] * x * (xx - 3.0f * yy) * ldf(sh, 14 * 3 + c);
+      }
+    }
+  }
+  r = r + 0.5f;
+  r *= (r > 0.0f);
+  return r;
+}
+
+template <int DEG, typename TS>
+__global__ void __launch_bounds__(256)
+sh_eval_kernel(int n_idx, int P, int M, const int64_t* __restrict__ idx, const float* __restrict__ centers,
+               const float* __restrict__ cam_pos, const TS* __restrict__ sh0, const TS* __restrict__ shs,
+               float* __restrict__ rgbs) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((n_idx == 0 && tid >= P) || (n_idx != 0 && tid >= n_idx)) return;
+  const int64_t i = (n_idx != 0) ? idx[tid] : tid;
+  float dx = centers[3 * i + 0] - cam_pos[0];
+  float dy = centers[3 * i + 1] - cam_pos[1];
+  float dz = centers[3 * i + 2] - cam_pos[2];
+  const float rn = rnorm3df(dx, dy, dz);
+  dx = dx * rn; dy = dy * rn; dz = dz * rn;
+  const TS* sh = shs + (size_t)i * (M - 1) * 3;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) rgbs[3 * i + c] = sh_channel<DEG>(dx, dy, dz, ldf(sh0, 3 * i + c), sh, c);
+}
+
+template <int DEG>
+__global__ void __launch_bounds__(256)
+sh_eval_bw_kernel(int n_idx, int P, int M, const int64_t* __restrict__ idx, const float* __restrict__ centers,
+                  const float* __restrict__ cam_pos, const float* __restrict__ dL_drgbs, float* __restrict__ dL_dsh0,
+                  float* __restrict__ dL_dshs) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((n_idx == 0 && tid >= P) || (n_idx != 0 && tid >= n_idx)) return;
+  const int64_t i = (n_idx != 0) ? idx[tid] : tid;
+  float x = centers[3 * i + 0] - cam_pos[0];
+  float y = centers[3 * i + 1] - cam_pos[1];
+  float z = centers[3 * i + 2] - cam_pos[2];
+  const float rn = rnorm3df(x, y, z);
+  x = x * rn; y = y * rn; z = z * rn;
+  const float g[3] = {dL_drgbs[3 * i + 0], dL_drgbs[3 * i + 1], dL_drgbs[3 * i + 2]};
+  float* d = dL_dshs + (size_t)i * (M - 1) * 3;
+  float basis[15];
+  int nb = 0;
+  if (DEG > 0) {
+    basis[0] = -kC1 * y;
+    basis[1] = kC1 * z;
+    basis[2] = -kC1 * x;
+    nb = 3;
+    if (DEG > 1) {
+      const float xx = x * x, yy = y * y, zz = z * z;
+      const float xy = x * y, yz = y * z, xz = x * z;
+      basis[3] = kC2[0] * xy;
+      basis[4] = kC2[1] * yz;
+      basis[5] = kC2[2] * (2.f * zz - xx - yy);
+      basis[6] = kC2[3] * xz;
+      basis[7] = kC2[4] * (xx - yy);
+      nb = 8;
+      if (DEG > 2) {
+        basis[8] = kC3[0] * y * (3.f * xx - yy);
+        basis[9] = kC3[1] * xy * z;
+        basis[10] = kC3[2] * y * (4.f * zz - xx - yy);
+        basis[11] = kC3[3] * z * (2.f * zz - 3.f * xx - 3.f * yy);
+        basis[12] = kC3[4] * x * (4.f * zz - xx - yy);
+        basis[13] = kC3[5] * z * (xx - yy);
+        basis[14] = kC3[6] * x * (xx - 3.f * yy);
+        nb = 15;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) dL_dsh0[3 * i + c] = kC0 * g[c];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) {
+    if (k >= nb) break;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) d[3 * k + c] = basis[k] * g[c];
+  }
+}
+
+void launch_sh_eval(int deg, int n_idx, int P, int M, const int64_t* idx, const float* centers, const float* cam_pos,
+                    const void* sh0, const void* shs, bool bf16, float* rgbs, cudaStream_t stream) {
+  const int n = n_idx != 0 ? n_idx : P;
+  if (n <= 0) return;
+  const int g = (n + 255) / 256;
+#define SVR_SH_L(D)                                                                                            \
+  if (bf16)                                                                                                    \
+    sh_eval_kernel<D, __nv_bfloat16><<<g, 256, 0, stream>>>(n_idx, P, M, idx, centers, cam_pos,                \
+                                                            (const __nv_bfloat16*)sh0, (const __nv_bfloat16*)shs, rgbs); \
+  else                                                                                                         \
+    sh_eval_kernel<D, float><<<g, 256, 0, stream>>>(n_idx, P, M, idx, centers, cam_pos, (const float*)sh0,     \
+                                                    (const float*)shs, rgbs);
+  switch (deg) {
+    case 0: SVR_SH_L(0) break;
+    case 1: SVR_SH_L(1) break;
+    case 2: SVR_SH_L(2) break;
+    default: SVR_SH_L(3) break;
+  }
+#undef SVR_SH_L
+}
+
+void launch_sh_eval_bw(int deg, int n_idx, int P, int M, const int64_t* idx, const float* centers,
+                       const float* cam_pos, const float* dL_drgbs, float* dL_dsh0, float* dL_dshs,
+                       cudaStream_t stream) {
+  const int n = n_idx != 0 ? n_idx : P;
+  if (n <= 0) return;
+  const int g = (n + 255) / 256;
+  switch (deg) {
+    case 0: sh_eval_bw_kernel<0><<<g, 256, 0, stream>>>(n_idx, P, M, idx, centers, cam_pos, dL_drgbs, dL_dsh0, dL_dshs); break;
+    case 1: sh_eval_bw_kernel<1><<<g, 256, 0, stream>>>(n_idx, P, M, idx, centers, cam_pos, dL_drgbs, dL_dsh0, dL_dshs); break;
+    case 2: sh_eval_bw_kernel<2><<<g, 256, 0, stream>>>(n_idx, P, M, idx, centers, cam_pos, dL_drgbs, dL_dsh0, dL_dshs); break;
+    default: sh_eval_bw_kernel<3><<<g, 256, 0, stream>>>(n_idx, P, M, idx, centers, cam_pos, dL_drgbs, dL_dsh0, dL_dshs); break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Adam
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float adam_lerp(float v0, float v1, float t) {
+  return fmaf(t, v1, fmaf(-t, v0, v0));  // (1-t)*v0 + t*v1, adam_step.cu:21-25
+}
+
+template <bool SPARSE>
+__global__ void __launch_bounds__(256)
+adam_unbiased_kernel(int64_t numel, float* __restrict__ param, const float* __restrict__ grad,
+                     float* __restrict__ exp_avg, float* __restrict__ exp_avg_sq, float step_size, float beta1,
+                     float beta2, float rsqrt_bc2, float eps) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= numel) return;
+  const float g = grad[i];
+  if (SPARSE && g == 0.0f) return;
+  float m = exp_avg[i];
+  float v = exp_avg_sq[i];
+  m = adam_lerp(g, m, beta1);
+  v = adam_lerp(g * g, v, beta2);
+  const float denom = fmaf(sqrtf(v), rsqrt_bc2, eps);
+  const float step = step_size * (m / denom);
+  param[i] -= step;
+  exp_avg[i] = m;
+  exp_avg_sq[i] = v;
+}
+
+template <bool SPARSE>
+__global__ void __launch_bounds__(256)
+adam_biased_kernel(int64_t numel, float* __restrict__ param, const float* __restrict__ grad,
+                   float* __restrict__ exp_avg, float* __restrict__ exp_avg_sq, float lr, float beta1, float beta2,
+                   float eps) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= numel) return;
+  const float g = grad[i];
+  if (SPARSE && g == 0.0f) return;
+  float m = exp_avg[i];
+  float v = exp_avg_sq[i];
+  m = adam_lerp(g, m, beta1);
+  v = adam_lerp(g * g, v, beta2);
+  const float denom = sqrtf(v) + eps;
+  const float step = lr * (m / denom);
+  param[i] -= step;
+  exp_avg[i] = m;
+  exp_avg_sq[i] = v;
+}
+
+void launch_adam(bool biased, bool sparse, int64_t numel, float* param, const float* grad, float* m, float* v,
+                 float step_or_lr, float beta1, float beta2, float rsqrt_bc2, float eps, cudaStream_t stream) {
+  if (numel <= 0) return;
+  const unsigned g = (unsigned)((numel + 255) / 256);
+  if (biased) {
+    if (sparse) adam_biased_kernel<true><<<g, 256, 0, stream>>>(numel, param, grad, m, v, step_or_lr, beta1, beta2, eps);
+    else adam_biased_kernel<false><<<g, 256, 0, stream>>>(numel, param, grad, m, v, step_or_lr, beta1, beta2, eps);
+  } else {
+    if (sparse)
+      adam_unbiased_kernel<true><<<g, 256, 0, stream>>>(numel, param, grad, m, v, step_or_lr, beta1, beta2, rsqrt_bc2, eps);
+    else
+      adam_unbiased_kernel<false><<<g, 256, 0, stream>>>(numel, param, grad, m, v, step_or_lr, beta1, beta2, rsqrt_bc2, eps);
+  }
+}
+
+// Fused multi-group Adam: one launch walks every group's elements with
+// 4-wide vector access.  Parameters may be fp32 or bf16 (fp32 moments and
+// gradients); the per-element arithmetic is the unbiased kernel's.
+__global__ void __launch_bounds__(256)
+adam_fused_kernel(const __grid_constant__ AdamGroupTable t) {
+  const int grp = blockIdx.y;
+  if (grp >= t.n) return;
+  const AdamGroup& G = t.g[grp];
+  const int64_t n4 = G.numel / 4;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < (G.numel + 3) / 4; q += stride) {
+    const bool full = q < n4;
+    float g4[4], m4[4], v4[4], p4[4];
+    if (full) {
+      *reinterpret_cast<float4*>(g4) = reinterpret_cast<const float4*>(G.grad)[q];
+      *reinterpret_cast<float4*>(m4) = reinterpret_cast<const float4*>(G.exp_avg)[q];
+      *reinterpret_cast<float4*>(v4) = reinterpret_cast<const float4*>(G.exp_avg_sq)[q];
+      if (G.param_bf16) {
+        const uint2 raw = reinterpret_cast<const uint2*>(G.param)[q];
+        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&raw);
+        const float2 a = __bfloat1622float2(h[0]), b = __bfloat1622float2(h[1]);
+        p4[0] = a.x; p4[1] = a.y; p4[2] = b.x; p4[3] = b.y;
+      } else {
+        *reinterpret_cast<float4*>(p4) = reinterpret_cast<const float4*>(G.param)[q];
+      }
+    } else {
+      for (int k = 0; k < 4; ++k) {
+        const int64_t i = 4 * q + k;
+        const bool ok = i < G.numel;
+        g4[k] = ok ? G.grad[i] : 0.f;
+        m4[k] = ok ? G.exp_avg[i] : 0.f;
+        v4[k] = ok ? G.exp_avg_sq[i] : 0.f;
+        p4[k] = ok ? (G.param_bf16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(G.param)[i])
+                                   : reinterpret_cast<const float*>(G.param)[i])
+                   : 0.f;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float g = g4[k];
+      if (t.sparse && g == 0.0f) continue;
+      float m = adam_lerp(g, m4[k], G.beta1);
+      float v = adam_lerp(g * g, v4[k], G.beta2);
+      const float denom = fmaf(sqrtf(v), G.rsqrt_bc2, G.eps);
+      const float step = G.step_size * (m / denom);
+      p4[k] -= step;
+      m4[k] = m;
+      v4[k] = v;
+    }
+    if (full) {
+      reinterpret_cast<float4*>(G.exp_avg)[q] = *reinterpret_cast<float4*>(m4);
+      reinterpret_cast<float4*>(G.exp_avg_sq)[q] = *reinterpret_cast<float4*>(v4);
+      if (G.param_bf16) {
+        __nv_bfloat162 h[2] = {__floats2bfloat162_rn(p4[0], p4[1]), __floats2bfloat162_rn(p4[2], p4[3])};
+        reinterpret_cast<uint2*>(G.param)[q] = *reinterpret_cast<uint2*>(h);
+      } else {
+        reinterpret_cast<float4*>(G.param)[q] = *reinterpret_cast<float4*>(p4);
+      }
+    } else {
+      for (int k = 0; k < 4; ++k) {
+        const int64_t i = 4 * q + k;
+        if (i >= G.numel) break;
+        G.exp_avg[i] = m4[k];
+        G.exp_avg_sq[i] = v4[k];
+        if (G.param_bf16) reinterpret_cast<__nv_bfloat16*>(G.param)[i] = __float2bfloat16_rn(p4[k]);
+        else reinterpret_cast<float*>(G.param)[i] = p4[k];
+      }
+    }
+  }
+}
+
+void launch_adam_fused(const AdamGroupTable& t, int num_sms, cudaStream_t stream) {
+  if (t.n <= 0) return;
+  int64_t maxq = 0;
+  for (int i = 0; i < t.n; ++i) maxq = std::max<int64_t>(maxq, (t.g[i].numel + 3) / 4);
+  if (maxq == 0) return;
+  const int64_t want = (maxq + 255) / 256;
+  const int cap = std::max(1, num_sms * 8);
+  dim3 grid((unsigned)std::min<int64_t>(want, cap), t.n);
+  adam_fused_kernel<<<grid, 256, 0, stream>>>(t);
+}
+
+// ---------------------------------------------------------------------------
+// Grid-point gathers
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(256)
+gather_kernel(int n_care, const int64_t* __restrict__ vox_key, const int64_t* __restrict__ care_idx,
+              const float* __restrict__ grid_pts, float* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_care) return;
+  const int64_t i = care_idx[t];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int64_t k = vox_key[8 * i + c];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) out[(8 * i + c) * DIM + d] = grid_pts[k * DIM + d];
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256)
+gather_bw_kernel(int n_care, const int64_t* __restrict__ vox_key, const int64_t* __restrict__ care_idx,
+                 const float* __restrict__ dL_dvox, float* __restrict__ dL_dgrid) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_care) return;
+  const int64_t i = care_idx[t];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int64_t k = vox_key[8 * i + c];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) atomicAdd(dL_dgrid + k * DIM + d, dL_dvox[(8 * i + c) * DIM + d]);
+  }
+}
+
+void launch_gather(int dim, int n_care, const int64_t* vox_key, const int64_t* care_idx, const float* grid_pts,
+                   float* out, cudaStream_t stream) {
+  if (n_care <= 0) return;
+  const int g = (n_care + 255) / 256;
+  if (dim == 1) gather_kernel<1><<<g, 256, 0, stream>>>(n_care, vox_key, care_idx, grid_pts, out);
+  else gather_kernel<3><<<g, 256, 0, stream>>>(n_care, vox_key, care_idx, grid_pts, out);
+}
+
+void launch_gather_bw(int dim, int n_care, const int64_t* vox_key, const int64_t* care_idx, const float* dL_dvox,
+                      float* dL_dgrid, cudaStream_t stream) {
+  if (n_care <= 0) return;
+  const int g = (n_care + 255) / 256;
+  if (dim == 1) gather_bw_kernel<1><<<g, 256, 0, stream>>>(n_care, vox_key, care_idx, dL_dvox, dL_dgrid);
+  else gather_bw_kernel<3><<<g, 256, 0, stream>>>(n_care, vox_key, care_idx, dL_dvox, dL_dgrid);
+}
+
+}  // namespace svr

@@ -1,0 +1,29 @@
+// Per-view camera description passed to every kernel by value.
+#pragma once
+
+#include <cstdint>
+
+namespace svr {
+
+constexpr int kMaxViews = 64;
+
+struct ViewParams {
+  int W, H;              // image size in pixels
+  int grid_x, grid_y;    // tile grid (ceil(W/16), ceil(H/16))
+  float tanfovx, tanfovy;
+  float cx, cy;          // principal point in pixels
+  float focal_x, focal_y;  // 0.5*W/tanfovx, computed in float on the host (preprocess.cu:173-174)
+  float near_plane;
+  float bg;              // background intensity
+  const float* w2c;      // device, row-major 4x4 (first 12 read)
+  const float* c2w;      // device, row-major 4x4 (first 12 read)
+  uint32_t tile_base;    // first global tile id of this view (batched path)
+  uint32_t pix_base;     // first global pixel of this view (batched path)
+};
+
+struct ViewTable {
+  int n;
+  ViewParams v[kMaxViews];
+};
+
+}  // namespace svr

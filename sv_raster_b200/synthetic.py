@@ -1,0 +1,345 @@
+"""Seeded synthetic sparse-voxel scenes and cameras.
+
+Stands in for the reference's datasets (none are available here): sparse
+octree voxels inside the scene cube [-0.5, 0.5]^3 (scene centre 0, extent 1,
+so a level-l voxel has edge 2^-l), with the reference's octree encoding:
+
+* ``octpath``: 3 bits per level, level-1 octant in bits 45-47, deeper levels
+  below, then zero-padded to 16 levels (``ijk_2_octpath``, utils.cu:129-158);
+* voxel centre ``-0.5 + (ijk + 0.5) * 2^-l`` and size ``2^-l``
+  (``octpath_decoding``, utils/octree_utils.py:99-126);
+* no voxel overlaps another (no ancestor/descendant pairs), as in a valid
+  SVRaster model.
+
+Cameras are OpenCV pinholes (x right, y down, z forward) with row-major 4x4
+``w2c`` and ``c2w = inverse(w2c)`` (cameras.py:119-155), principal point at the
+image centre.  All randomness comes from ``numpy.random.default_rng(seed)``.
+"""
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+MAX_LEVELS = 16
+
+
+def ijk_to_octpath(ijk, level):
+    """(i,j,k) integer cell coords at `level` -> octpath (int64)."""
+    ijk = np.asarray(ijk, dtype=np.int64)
+    level = np.asarray(level, dtype=np.int64).reshape(-1)
+    i, j, k = ijk[:, 0].copy(), ijk[:, 1].copy(), ijk[:, 2].copy()
+    path = np.zeros(len(level), dtype=np.int64)
+    for l in range(MAX_LEVELS):
+        bits = ((i & 1) << 2) | ((j & 1) << 1) | (k & 1)
+        path |= bits << (3 * l)
+        i >>= 1
+        j >>= 1
+        k >>= 1
+    return path << (3 * (MAX_LEVELS - level))
+
+
+def octpath_to_ijk(path, level):
+    path = np.asarray(path, dtype=np.int64).reshape(-1)
+    level = np.asarray(level, dtype=np.int64).reshape(-1)
+    p = path >> (3 * (MAX_LEVELS - level))
+    ijk = np.zeros((len(path), 3), dtype=np.int64)
+    for l in range(MAX_LEVELS):
+        bits = p & 7
+        ijk[:, 0] |= ((bits >> 2) & 1) << l
+        ijk[:, 1] |= ((bits >> 1) & 1) << l
+        ijk[:, 2] |= (bits & 1) << l
+        p >>= 3
+    return ijk
+
+
+def decode_voxels(path, level):
+    """Voxel centres [N,3] and sizes [N,1] (float32, exact) of octree cells."""
+    ijk = octpath_to_ijk(path, level)
+    size = np.ldexp(1.0, -np.asarray(level, dtype=np.int64).reshape(-1, 1))
+    centers = -0.5 + (ijk + 0.5) * size
+    return centers.astype(np.float32), size.astype(np.float32)
+
+
+def _cell_key(ijk, level):
+    level = np.asarray(level, dtype=np.int64)
+    side = np.left_shift(np.int64(1), level)
+    return ((level << 52) | (ijk[:, 0] * side * side + ijk[:, 1] * side + ijk[:, 2])).astype(np.int64)
+
+
+def _cells_from_points(pts, levels):
+    side = np.left_shift(np.int64(1), levels.astype(np.int64))
+    ijk = np.floor((pts + 0.5) * side[:, None]).astype(np.int64)
+    ijk = np.clip(ijk, 0, side[:, None] - 1)
+    return ijk
+
+
+def remove_overlaps(ijk, level):
+    """Unique non-overlapping cells: a cell is dropped when any ancestor is present.
+
+    Returns the indices (into the inputs) of kept cells, in input order of first
+    occurrence.
+    """
+    level = np.asarray(level, dtype=np.int64)
+    keys = _cell_key(ijk, level)
+    _, first = np.unique(keys, return_index=True)
+    first = np.sort(first)
+    ijk, level = ijk[first], level[first]
+    keys = keys[first]
+    keep = np.ones(len(first), dtype=bool)
+    present_levels = np.unique(level)
+    sorted_keys = np.sort(keys)
+    for l in present_levels:
+        sel = np.where(level == l)[0]
+        for la in present_levels:
+            if la >= l:
+                break
+            anc = ijk[sel] >> (l - la)
+            akeys = _cell_key(anc, np.full(len(sel), la))
+            pos = np.searchsorted(sorted_keys, akeys)
+            pos = np.minimum(pos, len(sorted_keys) - 1)
+            hit = sorted_keys[pos] == akeys
+            keep[sel[hit]] = False
+    return first[keep]
+
+
+def _sphere_points(rng, n, center, radius, jitter):
+    d = rng.standard_normal((n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True) + 1e-12
+    r = radius + rng.normal(0.0, jitter, size=(n, 1))
+    return center + d * r
+
+
+def _surface_points(rng, n, surf, n_surf=3):
+    """Points on `n_surf` seeded Gaussian-perturbed spheres (|p|_inf <= 0.3)."""
+    idx = rng.integers(0, n_surf, size=n)
+    c = surf[0][idx]
+    r = surf[1][idx][:, None]
+    return c + _unit(rng, n) * (r + rng.normal(0.0, 0.01, (n, 1)))
+
+
+def _unit(rng, n):
+    d = rng.standard_normal((n, 3))
+    return d / (np.linalg.norm(d, axis=1, keepdims=True) + 1e-12)
+
+
+def _shell_points(rng, n, inner=0.36):
+    """Points uniform in the cube shell inner < |p|_inf < 0.5."""
+    pts = []
+    got = 0
+    while got < n:
+        p = rng.uniform(-0.5, 0.5, size=(2 * n + 1024, 3))
+        p = p[np.abs(p).max(1) > inner]
+        pts.append(p)
+        got += len(p)
+    return np.concatenate(pts, 0)[:n]
+
+
+def _region_levels(pts, l0, l1, salt):
+    """Level of each point, constant over level-l0 regions (so cells never overlap)."""
+    if l0 == l1:
+        return np.full(len(pts), l0, np.int64)
+    side = 1 << l0
+    rid = np.clip(np.floor((pts + 0.5) * side).astype(np.int64), 0, side - 1)
+    h = (rid[:, 0] * 73856093) ^ (rid[:, 1] * 19349663) ^ (rid[:, 2] * 83492791) ^ (salt * 2654435761)
+    h = (h ^ (h >> 13)) * 0x5bd1e995
+    h = (h ^ (h >> 15)) & 0x7fffffff
+    return l0 + h % (l1 - l0 + 1)
+
+
+def _take(rng, arr, n):
+    if len(arr) <= n:
+        return arr
+    return np.sort(rng.choice(arr, size=n, replace=False))
+
+
+def make_voxels(n, seed, kind="sphere", surf_levels=(6, 8), bg_levels=(5, 7), surf_frac=0.7):
+    """Octree voxels: kind='sphere' (jittered sphere shell of radius 0.4) or
+    'mixed' (three surfaces + background shell).  Levels are drawn per
+    coarse region, so no voxel is an ancestor of another.
+    Returns (octpath int64 [N], level int8 [N])."""
+    rng = np.random.default_rng(seed)
+    if kind == "sphere":
+        groups = [("sphere", n, surf_levels)]
+    else:
+        n_s = int(round(n * surf_frac))
+        # Background first: its level range may hold fewer cells than asked
+        # for, and the surfaces then make up the difference.
+        groups = [("bg", n - n_s, bg_levels), ("surf", n_s, surf_levels)]
+    surf = (rng.uniform(-0.08, 0.08, size=(3, 3)), rng.uniform(0.1, 0.18, size=3))
+    all_ijk, all_lv = [], []
+    deficit = 0
+    for gi, (name, cnt, (l0, l1)) in enumerate(groups):
+        cnt += deficit
+        keys = np.zeros(0, np.int64)
+        m = max(4096, int(cnt * 1.3))
+        for _ in range(10):
+            if name == "sphere":
+                pts = _sphere_points(rng, m, np.zeros(3), 0.4, 0.02)
+            elif name == "surf":
+                pts = _surface_points(rng, m, surf)
+            else:
+                pts = _shell_points(rng, m)
+            pts = np.clip(pts, -0.5 + 1e-7, 0.5 - 1e-7)
+            lv = _region_levels(pts, l0, l1, seed * 7 + gi)
+            ijk = _cells_from_points(pts, lv)
+            before = len(keys)
+            keys = np.unique(np.concatenate([keys, _cell_key(ijk, lv)]))
+            if len(keys) >= cnt or len(keys) < before * 1.02:
+                break  # enough cells, or the level range is saturated
+            m = min(int(m * 1.5), 4 * cnt + 4096)
+        keys = _take(rng, keys, cnt)
+        deficit = cnt - len(keys)
+        lv = keys >> 52
+        idx = keys & ((np.int64(1) << 52) - 1)
+        side = np.left_shift(np.int64(1), lv)
+        ijk = np.stack([idx // (side * side), (idx // side) % side, idx % side], 1)
+        all_ijk.append(ijk)
+        all_lv.append(lv)
+    ijk = np.concatenate(all_ijk, 0)
+    lv = np.concatenate(all_lv, 0)
+    if len(groups) > 1:
+        keep = remove_overlaps(ijk, lv)
+        ijk, lv = ijk[keep], lv[keep]
+    perm = rng.permutation(len(lv))
+    ijk, lv = ijk[perm], lv[perm]
+    return ijk_to_octpath(ijk, lv), lv.astype(np.int8)
+
+
+def look_at(position, target=(0.0, 0.0, 0.0), up=(0.0, -1.0, 0.0)):
+    """OpenCV-convention (x right, y down, z forward) camera -> (w2c, c2w) float32 4x4."""
+    pos = np.asarray(position, np.float64)
+    fwd = np.asarray(target, np.float64) - pos
+    fwd /= np.linalg.norm(fwd)
+    upv = np.asarray(up, np.float64)
+    right = np.cross(fwd, upv)
+    if np.linalg.norm(right) < 1e-6:
+        right = np.cross(fwd, np.array([1.0, 0.0, 0.0]))
+    right /= np.linalg.norm(right)
+    down = np.cross(fwd, right)
+    c2w = np.eye(4)
+    c2w[:3, 0], c2w[:3, 1], c2w[:3, 2], c2w[:3, 3] = right, down, fwd, pos
+    w2c = np.linalg.inv(c2w)
+    return w2c.astype(np.float32), c2w.astype(np.float32)
+
+
+@dataclass
+class Camera:
+    width: int
+    height: int
+    tanfovx: float
+    tanfovy: float
+    cx: float
+    cy: float
+    w2c: np.ndarray
+    c2w: np.ndarray
+    near: float = 0.02
+
+    @property
+    def position(self):
+        return self.c2w[:3, 3]
+
+
+def make_camera(width, height, fovx_deg, position, target=(0.0, 0.0, 0.0)):
+    w2c, c2w = look_at(position, target)
+    tanfovx = math.tan(math.radians(fovx_deg) * 0.5)
+    tanfovy = tanfovx * height / width
+    return Camera(int(width), int(height), tanfovx, tanfovy, width * 0.5, height * 0.5, w2c, c2w)
+
+
+def orbit_cameras(n, seed, radius=(2.0, 4.0), size_range=((640, 480), (1600, 1200)), fovx_deg=50.0,
+                  hemisphere=False, fixed_size=None):
+    rng = np.random.default_rng(seed)
+    cams = []
+    for _ in range(n):
+        d = rng.standard_normal(3)
+        if hemisphere:
+            d[1] = -abs(d[1])  # y is down in the world frame used here: upper hemisphere
+        d /= np.linalg.norm(d)
+        r = rng.uniform(*radius)
+        if fixed_size is not None:
+            w, h = fixed_size
+        else:
+            w = int(rng.integers(size_range[0][0], size_range[1][0] + 1))
+            h = int(rng.integers(size_range[0][1], size_range[1][1] + 1))
+        cams.append(make_camera(w, h, fovx_deg, d * r))
+    return cams
+
+
+@dataclass
+class Scene:
+    name: str
+    octpath: np.ndarray
+    octlevel: np.ndarray
+    centers: np.ndarray
+    lengths: np.ndarray
+    geos: np.ndarray
+    sh0: np.ndarray
+    shs: np.ndarray
+    cameras: list
+    targets: list = field(default_factory=list)
+
+    @property
+    def n_voxels(self):
+        return len(self.octpath)
+
+    @property
+    def max_level(self):
+        return int(self.octlevel.max()) if len(self.octlevel) else 0
+
+
+def _params(rng, n, geo_mu, geo_sigma, sh_sigma=0.2, sh_deg=3):
+    geos = rng.normal(geo_mu, geo_sigma, size=(n, 8)).astype(np.float32)
+    m = (sh_deg + 1) ** 2
+    sh0 = rng.normal(0.0, sh_sigma, size=(n, 3)).astype(np.float32)
+    shs = rng.normal(0.0, sh_sigma, size=(n, m - 1, 3)).astype(np.float32)
+    return geos, sh0, shs
+
+
+def build_scene(name, n_voxels, seed, kind, surf_levels, bg_levels, geo_mu, geo_sigma, cameras, n_targets=1):
+    path, lv = make_voxels(n_voxels, seed, kind, surf_levels, bg_levels)
+    centers, lengths = decode_voxels(path, lv)
+    rng = np.random.default_rng(seed + 1)
+    geos, sh0, shs = _params(rng, len(path), geo_mu, geo_sigma)
+    trng = np.random.default_rng(seed + 2)
+    targets = [trng.uniform(0.0, 1.0, size=(3, c.height, c.width)).astype(np.float32) for c in cameras[:n_targets]]
+    return Scene(name, path, lv, centers, lengths, geos, sh0, shs, cameras, targets)
+
+
+def config_scene(name, seed=0, n_voxels=None):
+    """Synthetic stand-ins for the five benchmark configurations.
+
+    c1: 20k voxels, levels 6-8 on a jittered sphere (r=0.4), geos~N(-1,1),
+        256x256 fov 50 deg at distance 1.5 (+ a second generic camera, and a
+        200x136 camera inside the shell for multi-quadrant coverage).
+    c2: 2M voxels, 70% on three Gaussian-perturbed surfaces (levels 8-12),
+        30% in a background shell (levels 5-7), geos~N(-2,1.5), one 1297x840 view.
+    c3: the c2 scene seen by 16 orbit cameras (radius 2-4, 640x480..1600x1200).
+    c4: 8M voxels (levels 8-14, same mix), 8 views at 1920x1080.
+    c5: 16M voxels (levels 6-16), 32 views 960x540..1920x1080 on a hemisphere.
+    `n_voxels` overrides the voxel count (for scaled-down tests).
+    """
+    if name == "c1":
+        cams = [make_camera(256, 256, 50.0, (0.0, 0.0, -1.5)),
+                make_camera(256, 256, 50.0, np.array([0.9, -0.7, -1.0]) / np.linalg.norm([0.9, -0.7, -1.0]) * 1.5),
+                # inside the sphere shell: voxels straddle the camera's axis planes (multi-quadrant)
+                make_camera(200, 136, 70.0, (0.03, -0.02, 0.01), target=(0.4, 0.1, 0.3))]
+        return build_scene("c1", n_voxels or 20000, seed, "sphere", (6, 8), (6, 8), -1.0, 1.0, cams)
+    if name == "c2":
+        d = np.array([0.6, -0.5, -1.2])
+        cams = [make_camera(1297, 840, 50.0, d / np.linalg.norm(d) * 1.6)]
+        return build_scene("c2", n_voxels or 2_000_000, seed, "mixed", (8, 12), (5, 7), -2.0, 1.5, cams)
+    if name == "c3":
+        cams = orbit_cameras(16, seed + 10)
+        return build_scene("c3", n_voxels or 2_000_000, seed, "mixed", (8, 12), (5, 7), -2.0, 1.5, cams)
+    if name == "c4":
+        cams = orbit_cameras(8, seed + 20, radius=(1.5, 2.0), fixed_size=(1920, 1080))
+        return build_scene("c4", n_voxels or 8_000_000, seed, "mixed", (8, 14), (5, 7), -2.0, 1.5, cams)
+    if name == "c5":
+        rng = np.random.default_rng(seed + 30)
+        cams = []
+        for _ in range(32):
+            s = rng.uniform(0.5, 1.0)
+            cams += orbit_cameras(1, int(rng.integers(1 << 30)), radius=(1.5, 2.5), hemisphere=True,
+                                  fixed_size=(int(1920 * s) // 2 * 2, int(1080 * s) // 2 * 2))
+        return build_scene("c5", n_voxels or 16_000_000, seed, "mixed", (6, 16), (5, 7), -2.0, 1.5, cams)
+    raise ValueError(f"unknown config {name}")

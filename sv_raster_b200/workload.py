@@ -1,0 +1,200 @@
+"""Benchmark workloads: a scene, its views and one timed step (every view
+rendered and back-propagated), in the plain one-view-per-call form and the
+batched multi-view form.  Used by bench.py; kept in the package so the step
+is the same code a user would run.
+"""
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _C
+from ._native import Camera, check, lib
+
+RECORD_BYTES = 68  # bbox 8 + centre 12 + length 4 + 8 densities 32 + rgb 12
+
+
+def _t(a, dev, dt=torch.float32):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev, dt)
+
+
+class _Timer:
+    """CUDA-event timing of one kernel stage on the launching stream."""
+
+    def __init__(self, name):
+        self.name = name
+        self.pairs = []
+        self.bytes = []
+
+    def start(self, stream):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        self.pairs.append((e0, e1))
+        return e1
+
+    def stats(self):
+        ms = [a.elapsed_time(b) for a, b in self.pairs]
+        return dict(name=self.name, launches=len(ms), ms=float(sum(ms)), bytes=float(sum(self.bytes)),
+                    ms_per_launch=float(np.mean(ms)) if ms else 0.0,
+                    bytes_per_launch=float(np.mean(self.bytes)) if self.bytes else 0.0)
+
+
+class PlainWorkload:
+    """The reference's call pattern: one view per call, fp32, a host read of
+    the instance count per view (forward.cu:652-658)."""
+
+    def __init__(self, scene, dev):
+        self.sc = scene
+        self.dev = dev
+        self.octpath = _t(scene.octpath.reshape(-1, 1), dev, torch.int64)
+        self.centers = _t(scene.centers, dev)
+        self.lengths = _t(scene.lengths, dev)
+        self.geos = _t(scene.geos, dev)
+        self.sh0 = _t(scene.sh0, dev)
+        self.shs = _t(scene.shs, dev)
+        self.P = scene.n_voxels
+        self.cams = []
+        for c in scene.cameras:
+            self.cams.append((c, _t(c.w2c, dev), _t(c.c2w, dev)))
+        self.targets = [_t(t, dev) for t in scene.targets]
+        self.timers = {}
+        self._inst = []
+        self.empty_idx = torch.empty(0, dtype=torch.int64, device=dev)
+        self.n_passes = []
+
+    def reset_kernel_timers(self):
+        self.timers = {k: _Timer(k) for k in ("preprocess+scan", "binning", "render_fwd", "render_bwd", "sh")}
+        self._inst = []
+
+    def _stage(self, name, fn, nbytes=0.0):
+        if name not in self.timers:
+            return fn()
+        st = torch.cuda.current_stream(self.dev)
+        e1 = self.timers[name].start(st)
+        r = fn()
+        e1.record(st)
+        self.timers[name].bytes.append(nbytes)
+        return r
+
+    def view_fwd_bwd(self, i):
+        cam, w2c, c2w = self.cams[i]
+        W, H = cam.width, cam.height
+        L = lib()
+        dev = self.dev
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        cam_pos = c2w[:3, 3].contiguous()
+        ndup, geom = self._stage("preprocess+scan", lambda: _C.rasterize_preprocess(
+            W, H, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w, cam.near, self.octpath, self.centers,
+            self.lengths), 36.0 * self.P)
+        vis = torch.where(ndup > 0)[0]  # host sync, as the reference's renderer.py:83
+        V = int(vis.numel())
+        rgbs = self._stage("sh", lambda: _C.sh_compute(3, vis, self.centers, cam_pos, self.sh0, self.shs),
+                           V * (12 + 192 + 12.0))
+        R = _C.geom_num_rendered(geom)
+        self._inst.append(R)
+        T_ = math.ceil(W / 16) * math.ceil(H / 16)
+        binning = torch.empty(L.svr_binning_buffer_bytes(R, W, H), dtype=torch.uint8, device=dev)
+        img = torch.empty(L.svr_image_buffer_bytes(W, H), dtype=torch.uint8, device=dev)
+        color = torch.zeros(3, H, W, device=dev)
+        Tm = torch.zeros(1, H, W, device=dev)
+        ccam = Camera(W, H, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c.data_ptr(), c2w.data_ptr(), cam.near, 0.0)
+        p = lambda t: ctypes.c_void_p(t.data_ptr())
+        self._stage("binning", lambda: check(L.svr_rasterize_binning(
+            ctypes.byref(ccam), self.P, R, p(self.octpath), p(geom), p(binning), binning.numel(), p(img),
+            img.numel(), 0, stream), "binning"), 28.0 * V + 12.0 * R + 24.0 * R + 8.0 * R + 8.0 * T_)
+        self._stage("render_fwd", lambda: check(L.svr_rasterize_render(
+            ctypes.byref(ccam), 1, 0, 0, 0, 0, self.P, R, p(self.centers), p(self.lengths), p(self.geos), p(rgbs),
+            p(geom), p(binning), binning.numel(), p(img), img.numel(), p(color), None, None, p(Tm), None, 0,
+            stream), "render"), R * (4.0 + RECORD_BYTES) + 20.0 * W * H + 12.0 * T_)
+        tgt = self.targets[i % len(self.targets)]
+        dC = (2.0 / color.numel()) * (color - tgt)
+        dT = torch.zeros_like(Tm)
+        dgeo = torch.zeros(self.P, 8, device=dev)
+        drgb = torch.zeros(self.P, 3, device=dev)
+        sub = torch.zeros(self.P, 1, device=dev)
+        self._stage("render_bwd", lambda: check(L.svr_rasterize_backward(
+            ctypes.byref(ccam), 1, self.P, R, p(self.centers), p(self.lengths), p(self.geos), p(rgbs), p(geom),
+            p(binning), p(img), p(Tm), p(dC), None, None, p(dT), 0.0, None, 0.0, 0.0, 0, 0, None, None, p(dgeo),
+            p(drgb), p(sub), 0, stream), "render_bwd"), R * (4.0 + RECORD_BYTES) + 24.0 * W * H + 48.0 * V)
+        self._stage("sh", lambda: _C.sh_compute_bw(3, 16, vis, self.centers, cam_pos, rgbs, drgb),
+                    V * (12 * 3 + 192.0))
+        return dgeo
+
+    def step(self):
+        for i in range(len(self.cams)):
+            self.view_fwd_bwd(i)
+
+    def instances_per_view(self):
+        return int(np.mean(self._inst)) if self._inst else None
+
+    def launches_per_step(self):
+        n = 0
+        for cam, _, _ in self.cams:
+            T_ = math.ceil(cam.width / 16) * math.ceil(cam.height / 16)
+            passes = math.ceil((48 + int(T_).bit_length()) / 8)
+            # preprocess 1 + scan 3 + duplicate 1 + sort 3/pass + ranges 1 + fwd 1 + bwd 1 + sh 2
+            n += 1 + 3 + 1 + 3 * passes + 1 + 1 + 1 + 2
+        return n
+
+    def kernel_stats(self):
+        torch.cuda.synchronize()
+        table = [t.stats() for t in self.timers.values()]
+        dom = max(table, key=lambda s: s["ms"])
+        fwd = [s for s in table if s["name"] in ("preprocess+scan", "binning", "render_fwd", "sh")]
+        fwd_ms = sum(s["ms"] for s in fwd if s["name"] != "sh") + \
+            sum(s["ms"] for s in table if s["name"] == "sh") / 2.0
+        nviews = max(1, len(self.timers["render_fwd"].pairs))
+        return dict(table=[{k: (round(v, 4) if isinstance(v, float) else v) for k, v in s.items()} for s in table],
+                    dominant=dom, fwd_ms_per_view=fwd_ms / nviews)
+
+    def e2e(self, steps, warmup):
+        """Same step through the public autograd API; per step the targets and
+        camera matrices are copied from pinned host memory and the loss is
+        read back."""
+        from . import renderer
+        dev = self.dev
+        host_t = [torch.from_numpy(np.ascontiguousarray(t)).pin_memory() for t in self.sc.targets]
+        host_c = [(torch.from_numpy(c.w2c).pin_memory(), torch.from_numpy(c.c2w).pin_memory())
+                  for c in self.sc.cameras]
+        geos = self.geos.clone().requires_grad_(True)
+        sh0 = self.sh0.clone().requires_grad_(True)
+        shs = self.shs.clone().requires_grad_(True)
+        h2d = sum(t.numel() * 4 for t in host_t[: len(self.cams)]) + 2 * 64 * len(self.cams)
+        ones = torch.ones(self.P, 1, device=dev)
+
+        def one_step():
+            total = None
+            for i, (cam, _, _) in enumerate(self.cams):
+                tgt = host_t[i % len(host_t)].to(dev, non_blocking=True)
+                w2c = host_c[i][0].to(dev, non_blocking=True)
+                c2w = host_c[i][1].to(dev, non_blocking=True)
+                s = renderer.RasterSettings(color_mode="sh", n_samp_per_vox=1, image_width=cam.width,
+                                            image_height=cam.height, tanfovx=cam.tanfovx, tanfovy=cam.tanfovy,
+                                            cx=cam.cx, cy=cam.cy, w2c_matrix=w2c, c2w_matrix=c2w)
+
+                def vox_fn(idx, cam_pos, color_mode):
+                    rgbs = renderer.SH_eval.apply(3, idx, self.centers, cam_pos, None, sh0, shs)
+                    return {"geos": geos, "rgbs": rgbs, "subdiv_p": ones}
+
+                color, _, _, _, _ = renderer.rasterize_voxels(s, self.octpath, self.centers, self.lengths, vox_fn)
+                loss = ((color - tgt) ** 2).mean()
+                loss.backward()
+                total = loss.detach() if total is None else total + loss.detach()
+            return float(total.cpu())
+
+        for _ in range(warmup):
+            one_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = torch.cuda.current_stream(dev)
+        e0.record(st)
+        for _ in range(steps):
+            one_step()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return dict(ms_total=e0.elapsed_time(e1), h2d=h2d, d2h=4)
+
+
+class BatchedWorkload(PlainWorkload):
+    """Placeholder until the multi-view path lands: same as plain."""
