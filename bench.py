@@ -38,7 +38,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
-    ap.add_argument("--mode", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--mode", default="batched", choices=["plain", "batched"])
     ap.add_argument("--voxels", type=int, default=None, help="override the voxel count (smaller profiles)")
     ap.add_argument("--views", type=int, default=None, help="use only the first N views")
     ap.add_argument("--no-e2e", action="store_true")
@@ -109,7 +109,22 @@ def load_peaks():
 
 def scene_for(args, rank, world):
     from sv_raster_b200 import synthetic
-    sc = synthetic.config_scene(args.config, n_voxels=args.voxels)
+    cache = f"/tmp/svr_scene_{args.config}_{args.voxels or 0}.pkl"
+    sc = None
+    if os.path.exists(cache):
+        import pickle
+        try:
+            sc = pickle.load(open(cache, "rb"))
+        except Exception:
+            sc = None
+    if sc is None:
+        sc = synthetic.config_scene(args.config, n_voxels=args.voxels)
+        try:
+            import pickle
+            pickle.dump(sc, open(cache + ".tmp", "wb"), protocol=4)
+            os.replace(cache + ".tmp", cache)
+        except OSError:
+            pass
     cams = sc.cameras[: args.views] if args.views else sc.cameras
     if world > 1:
         # weak scaling: every rank renders its own set of views of the same size
@@ -164,6 +179,8 @@ def main():
     if world > 1:
         dist.barrier()
     clocks = sampler.stop()
+    if hasattr(wl, "check_errors"):
+        wl.check_errors()  # capacity / consistency flags of the batched step
     ms_total = ev0.elapsed_time(ev1)
     if world > 1:
         t = torch.tensor([ms_total], device=dev)
@@ -273,11 +290,10 @@ def run_reference(args):
     if rank != 0:
         return 0
     sc = scene_for(args, 0, 1)
-    vals = []
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
-    for _ in range(max(1, args.steps)):
-        vals.append(cpu_baseline(sc, budget_s=max(5.0, 60.0 / max(1, args.steps))))
+    per_step = min(30.0, max(5.0, 60.0 / max(1, args.steps)))
+    if args.warmup > 0:
+        cpu_baseline(sc, budget_s=1.0)
+    vals = [cpu_baseline(sc, budget_s=per_step) for _ in range(max(1, args.steps))]
     v = float(np.median([x["value"] for x in vals]))
     line = {"metric": "fwd+bwd ms/view", "value": round(v, 2), "unit": "ms/view", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",

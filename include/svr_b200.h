@@ -163,6 +163,51 @@ int svr_gather_grid_params_bw(int dim, int64_t n_care, const int64_t* vox_key, c
 /* Read and clear a device error word (synchronises `stream`). */
 int svr_read_error(uint32_t* device_word, uint32_t* host_value, void* stream);
 
+/* ---- multi-view batched path ------------------------------------------
+ * No reference counterpart: the reference renders one view per call and
+ * reads the instance count back to the host (forward.cu:601-734).
+ * N <= 64 views share one voxel set.  Per-view image arrays are laid out view
+ * after view: colour [sum_v 3*H_v*W_v] (each view planar [3,H,W]), T and
+ * dL_dT [sum_v H_v*W_v].  The plan fixes camera sizes and the DEVICE
+ * addresses of every view's w2c/c2w (their contents may change between
+ * calls); the workspace is caller-allocated (svr_batch_plan_create reports its
+ * size).  Nothing synchronises: an instance count above `capacity` sets
+ * SVR_DEVERR_CAPACITY (0x4) in the error word and leaves outputs invalid; the
+ * total instance count is at svr_batch_count_ptr.  Every voxel's octree level
+ * must be <= max_level (checked on the device: SVR_DEVERR_LEVEL, 0x10). */
+typedef struct svr_batch_plan svr_batch_plan;
+int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_t capacity, int n_samp_per_vox,
+                          int max_level, svr_batch_plan** plan, size_t* workspace_bytes);
+void svr_batch_plan_destroy(svr_batch_plan* plan);
+int64_t svr_batch_plan_pixels(const svr_batch_plan* plan);
+int64_t svr_batch_plan_tiles(const svr_batch_plan* plan);
+int svr_batch_plan_groups(const svr_batch_plan* plan);
+const uint32_t* svr_batch_count_ptr(const svr_batch_plan* plan, const void* workspace);
+uint32_t* svr_batch_error_ptr(const svr_batch_plan* plan, void* workspace);
+/* Device arrays inside a workspace: rgbs / dL_drgbs [V,P,3], ranges [T] (uint2
+ * as uint64), tile_last [T], n_contrib [pixels], n_dup [V,P], sorted values. */
+int svr_batch_arrays(const svr_batch_plan* plan, const void* workspace, const float** rgbs, const float** drgbs,
+                     const uint64_t** ranges, const uint32_t** tile_last, const uint32_t** n_contrib,
+                     const uint32_t** n_dup, const uint32_t** sorted_vals);
+/* Projection fused with SH colour (fp32 or bf16 coefficients, degree 0-3),
+ * scan, duplication, grouped sort and tile ranges of every view. */
+int svr_batch_prepare(svr_batch_plan* plan, void* workspace, const int64_t* octree_paths, const float* vox_centers,
+                      const float* vox_lengths, const void* sh0, const void* shs, int sh_bf16, int sh_degree, int M,
+                      void* stream);
+/* Compositing of every (view, tile) in one launch; geos fp32 or bf16 [P,8].
+ * out_color / out_T caller-zeroed. */
+int svr_batch_render(svr_batch_plan* plan, void* workspace, const float* vox_centers, const float* vox_lengths,
+                     const void* geos, int geos_bf16, float* out_color, float* out_T, void* stream);
+/* Recompute-backward of every (view, tile) in one launch: dL_dgeos [P,8] and
+ * subdiv [P] summed over views (caller-zeroed); per-view dL/drgb kept in the
+ * workspace for svr_batch_sh_backward. */
+int svr_batch_backward(svr_batch_plan* plan, void* workspace, const float* vox_centers, const float* vox_lengths,
+                       const void* geos, int geos_bf16, const float* out_T, const float* dL_dcolor,
+                       const float* dL_dT, float* dL_dgeos, float* subdiv, void* stream);
+/* dL/dsh0 [P,3] and dL/dshs [P,M-1,3] summed over views (overwritten). */
+int svr_batch_sh_backward(svr_batch_plan* plan, void* workspace, const float* vox_centers, int sh_degree, int M,
+                          float* dL_dsh0, float* dL_dshs, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,19 @@ _SIGS = {
     "svr_gather_grid_params": (c_int, [c_int, c_i64, c_p, c_p, c_p, c_p, c_p]),
     "svr_gather_grid_params_bw": (c_int, [c_int, c_i64, c_p, c_p, c_p, c_p, c_p]),
     "svr_read_error": (c_int, [c_p, ctypes.POINTER(ctypes.c_uint32), c_p]),
+    "svr_batch_plan_create": (c_int, [c_int, ctypes.POINTER(Camera), c_i64, c_i64, c_int, c_int,
+                                      ctypes.POINTER(c_p), ctypes.POINTER(c_sz)]),
+    "svr_batch_plan_destroy": (None, [c_p]),
+    "svr_batch_plan_pixels": (c_i64, [c_p]),
+    "svr_batch_plan_tiles": (c_i64, [c_p]),
+    "svr_batch_plan_groups": (c_int, [c_p]),
+    "svr_batch_count_ptr": (c_p, [c_p, c_p]),
+    "svr_batch_error_ptr": (c_p, [c_p, c_p]),
+    "svr_batch_arrays": (c_int, [c_p, c_p] + [ctypes.POINTER(c_p)] * 7),
+    "svr_batch_prepare": (c_int, [c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_int, c_int, c_int, c_p]),
+    "svr_batch_render": (c_int, [c_p, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_p]),
+    "svr_batch_backward": (c_int, [c_p, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_p, c_p, c_p, c_p]),
+    "svr_batch_sh_backward": (c_int, [c_p, c_p, c_p, c_int, c_int, c_p, c_p, c_p]),
 }
 
 _lib = None

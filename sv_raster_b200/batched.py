@@ -1,0 +1,193 @@
+"""Multi-view batched rasterization: many cameras of uneven resolution over
+one shared voxel set, one launch per stage, no host round trip, CUDA-graph
+capturable.  Densities and SH coefficients may be stored in bf16; all
+compositing, transmittance and gradient accumulation is fp32.
+
+This has no counterpart in the reference (which renders one view per call);
+per view it produces the plain path's images, contributor counts and tile
+lists.
+"""
+import ctypes
+import math
+
+import torch
+
+from ._native import Camera, check, lib
+
+TILE = 16
+
+
+class BatchedRasterizer:
+    """A plan over fixed cameras + a workspace sized for the scene.
+
+    ``cameras``: objects with width, height, tanfovx, tanfovy, cx, cy, near and
+    device tensors ``w2c`` / ``c2w`` (4x4 fp32).  The device addresses of
+    those matrices are baked into the plan; update them in place to move the
+    cameras (e.g. between CUDA-graph replays).  ``max_level`` bounds the
+    voxels' octree levels (shorter sort keys; checked on the device).
+    """
+
+    def __init__(self, cameras, octree_paths, vox_centers, vox_lengths, max_level=16, n_samp_per_vox=1,
+                 bg_color=0.0, capacity=None, headroom=1.25):
+        self.dev = vox_centers.device
+        self.cams = list(cameras)
+        self.octree_paths = octree_paths.reshape(-1).contiguous()
+        self.centers = vox_centers.contiguous()
+        self.lengths = vox_lengths.contiguous()
+        self.P = self.centers.shape[0]
+        self.max_level = int(max_level)
+        self.n_samp = int(n_samp_per_vox)
+        self.bg = float(bg_color)
+        self.headroom = headroom
+        self._c_cams = (Camera * len(self.cams))()
+        for i, c in enumerate(self.cams):
+            if c.w2c.device != self.dev or c.c2w.device != self.dev:
+                raise ValueError("camera matrices must live on the voxels' device")
+            self._c_cams[i] = Camera(c.width, c.height, c.tanfovx, c.tanfovy, c.cx, c.cy, c.w2c.data_ptr(),
+                                     c.c2w.data_ptr(), c.near, self.bg)
+        self.sizes = [(c.height, c.width) for c in self.cams]
+        self.pix_offsets = [0]
+        for h, w in self.sizes:
+            self.pix_offsets.append(self.pix_offsets[-1] + h * w)
+        self.plan = None
+        self._make_plan(0 if capacity is None else int(capacity))
+        self.capacity_auto = capacity is None
+
+    # -- plan / workspace ----------------------------------------------------
+    def _make_plan(self, capacity):
+        L = lib()
+        if self.plan is not None:
+            L.svr_batch_plan_destroy(self.plan)
+            self.plan = None
+        plan = ctypes.c_void_p()
+        nbytes = ctypes.c_size_t()
+        check(L.svr_batch_plan_create(len(self.cams), self._c_cams, self.P, capacity, self.n_samp, self.max_level,
+                                      ctypes.byref(plan), ctypes.byref(nbytes)), "batch_plan_create")
+        self.plan = plan
+        self.capacity = capacity
+        self.ws = torch.empty(nbytes.value, dtype=torch.uint8, device=self.dev)
+        self.n_pixels = int(L.svr_batch_plan_pixels(plan))
+        self.n_tiles = int(L.svr_batch_plan_tiles(plan))
+        self.n_groups = int(L.svr_batch_plan_groups(plan))
+
+    def __del__(self):
+        try:
+            if self.plan is not None:
+                lib().svr_batch_plan_destroy(self.plan)
+        except Exception:
+            pass
+
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def _p(self, t):
+        return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+    def header(self):
+        """(total instance count, device error word) -- synchronises."""
+        h = self.ws[:8].view(torch.int32).cpu()
+        return int(h[0]) & 0xFFFFFFFF, int(h[1]) & 0xFFFFFFFF
+
+    def fit_capacity(self, sh0, shs, sh_degree=3):
+        """Run the projection + scan once, read the instance count and re-plan
+        with `headroom` x that capacity (host sync; not for graph capture)."""
+        self.prepare(sh0, shs, sh_degree)
+        total, _ = self.header()
+        need = int(math.ceil(total * self.headroom)) + 1024
+        if need > self.capacity:
+            self._make_plan(min(need, 0xFFFFFFFF))
+        return total
+
+    # -- stages ----------------------------------------------------------------
+    def prepare(self, sh0, shs, sh_degree=3):
+        bf16 = sh0.dtype == torch.bfloat16
+        if bf16 != (shs.dtype == torch.bfloat16):
+            raise ValueError("sh0 and shs must share a dtype")
+        M = 1 + shs.shape[1]
+        check(lib().svr_batch_prepare(self.plan, self._p(self.ws), self._p(self.octree_paths), self._p(self.centers),
+                                      self._p(self.lengths), self._p(sh0.contiguous()),
+                                      self._p(shs.contiguous()) if shs.numel() else None, int(bf16), int(sh_degree),
+                                      M, self._stream()), "batch_prepare")
+
+    def render(self, geos, out_color=None, out_T=None):
+        """Composite every view; returns flat (color [sum 3HW], T [sum HW])."""
+        if out_color is None:
+            out_color = torch.zeros(3 * self.n_pixels, device=self.dev)
+            out_T = torch.zeros(self.n_pixels, device=self.dev)
+        else:
+            out_color.zero_()
+            out_T.zero_()
+        check(lib().svr_batch_render(self.plan, self._p(self.ws), self._p(self.centers), self._p(self.lengths),
+                                     self._p(geos), int(geos.dtype == torch.bfloat16), self._p(out_color),
+                                     self._p(out_T), self._stream()), "batch_render")
+        return out_color, out_T
+
+    def backward(self, geos, out_T, dL_dcolor, dL_dT, sh_degree, M, grads=None):
+        """Returns (dL_dgeos [P,8], subdiv [P], dL_dsh0 [P,3], dL_dshs [P,M-1,3]) fp32."""
+        if grads is None:
+            grads = (torch.zeros(self.P, 8, device=self.dev), torch.zeros(self.P, device=self.dev),
+                     torch.zeros(self.P, 3, device=self.dev), torch.zeros(self.P, M - 1, 3, device=self.dev))
+        else:
+            grads[0].zero_()
+            grads[1].zero_()
+        dgeo, sub, dsh0, dshs = grads
+        L = lib()
+        check(L.svr_batch_backward(self.plan, self._p(self.ws), self._p(self.centers), self._p(self.lengths),
+                                   self._p(geos), int(geos.dtype == torch.bfloat16), self._p(out_T),
+                                   self._p(dL_dcolor), self._p(dL_dT), self._p(dgeo), self._p(sub), self._stream()),
+              "batch_backward")
+        check(L.svr_batch_sh_backward(self.plan, self._p(self.ws), self._p(self.centers), int(sh_degree), int(M),
+                                      self._p(dsh0), self._p(dshs) if dshs.numel() else None, self._stream()),
+              "batch_sh_backward")
+        return grads
+
+    # -- views of the flat outputs ---------------------------------------------
+    def split_color(self, flat):
+        return [flat[3 * a:3 * b].view(3, h, w) for (h, w), a, b in
+                zip(self.sizes, self.pix_offsets[:-1], self.pix_offsets[1:])]
+
+    def split_pixels(self, flat):
+        return [flat[a:b].view(1, h, w) for (h, w), a, b in zip(self.sizes, self.pix_offsets[:-1],
+                                                                 self.pix_offsets[1:])]
+
+    def arrays(self):
+        """Device views of the workspace internals (rgbs, n_contrib, ...)."""
+        ptrs = [ctypes.c_void_p() for _ in range(7)]
+        check(lib().svr_batch_arrays(self.plan, self._p(self.ws), *[ctypes.byref(p) for p in ptrs]), "arrays")
+        base = self.ws.data_ptr()
+        off = [p.value - base for p in ptrs]
+        VP = len(self.cams) * self.P
+        ws = self.ws
+        return dict(
+            rgbs=ws[off[0]:off[0] + 12 * VP].view(torch.float32).view(len(self.cams), self.P, 3),
+            drgbs=ws[off[1]:off[1] + 12 * VP].view(torch.float32).view(len(self.cams), self.P, 3),
+            ranges=ws[off[2]:off[2] + 8 * self.n_tiles].view(torch.int32).view(self.n_tiles, 2),
+            tile_last=ws[off[3]:off[3] + 4 * self.n_tiles].view(torch.int32),
+            n_contrib=ws[off[4]:off[4] + 4 * self.n_pixels].view(torch.int32),
+            ndup=ws[off[5]:off[5] + 4 * VP].view(torch.int32).view(len(self.cams), self.P),
+            sorted_vals=ws[off[6]:off[6] + 4 * max(self.capacity, 1)].view(torch.int32),
+        )
+
+
+class BatchedRender(torch.autograd.Function):
+    """Autograd wrapper: (geos, sh0, shs) -> (color flat, T flat) over all views."""
+
+    @staticmethod
+    def forward(ctx, raster, sh_degree, geos, sh0, shs):
+        raster.prepare(sh0, shs, sh_degree)
+        color, T = raster.render(geos)
+        ctx.raster = raster
+        ctx.sh_degree = sh_degree
+        ctx.M = 1 + shs.shape[1]
+        ctx.sh_dtype = sh0.dtype
+        ctx.save_for_backward(geos, T)
+        return color, T
+
+    @staticmethod
+    def backward(ctx, dL_dcolor, dL_dT):
+        geos, T = ctx.saved_tensors
+        r = ctx.raster
+        if dL_dT is None:
+            dL_dT = torch.zeros_like(T)
+        dgeo, _sub, dsh0, dshs = r.backward(geos, T, dL_dcolor.contiguous(), dL_dT.contiguous(), ctx.sh_degree, ctx.M)
+        return None, None, dgeo.to(geos.dtype), dsh0.to(ctx.sh_dtype), dshs.to(ctx.sh_dtype)

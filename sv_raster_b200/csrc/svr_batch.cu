@@ -1,0 +1,499 @@
+// Multi-view batched path: N views of one voxel set projected, binned,
+// composited and back-propagated with one launch per stage over all views,
+// without any host round trip (capturable in a CUDA graph).
+//
+// No reference counterpart: the reference renders one view per call and
+// reads the instance count back to the host (forward.cu:601-734).  Per view,
+// the results are those of the plain path:
+//   - projection is project_voxel (preprocess.cu:24-132 arithmetic), fused
+//     with the SH colour of each visible (voxel, view) (sh_compute.cu:54-106);
+//   - instances of all views share one flat array, view-major; views are
+//     grouped so that a group's [tile | Morton rank] key fits in 64 bits and
+//     each group is sorted as one segment.  Keys use a compressed rank: with
+//     every voxel at octree level <= L < 16, the rank's lowest 3*(16-L) bits
+//     are the quadrant repeated, so (rank >> 3*(16-L)) << 3 | quadrant orders
+//     instances exactly as the full 48-bit rank does;
+//   - compositing / backward are the same per-tile device functions.
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/svr_b200.h"
+#include "svr_common.cuh"
+#include "svr_kernels.h"
+#include "svr_project.cuh"
+#include "svr_render.cuh"
+#include "svr_render_bwd.cuh"
+#include "svr_render_fwd.cuh"
+#include "svr_sh.cuh"
+
+using namespace svr;
+
+namespace {
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+struct GroupTable {
+  int n;
+  int v0[kMaxViews + 1];          // first view of each group (+ end)
+  uint32_t tile_base[kMaxViews];  // first global tile of each group
+};
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+template <int DEG, typename TS>
+__global__ void __launch_bounds__(256)
+project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* __restrict__ centers,
+                  const float* __restrict__ lengths, const TS* __restrict__ sh0, const TS* __restrict__ shs, int M,
+                  uint32_t* __restrict__ ndup, uint2* __restrict__ bboxes, uint32_t* __restrict__ quads,
+                  float* __restrict__ rgbs) {
+  const int view = blockIdx.y;
+  const ViewParams& vp = views.v[view];
+  __shared__ float s_m[24];
+  if (threadIdx.x < 12) s_m[threadIdx.x] = vp.w2c[threadIdx.x];
+  else if (threadIdx.x < 24) s_m[threadIdx.x] = vp.c2w[threadIdx.x - 12];
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  const size_t o = (size_t)view * P + i;
+  const float cx = centers[3 * (size_t)i], cy = centers[3 * (size_t)i + 1], cz = centers[3 * (size_t)i + 2];
+  const Projection pr = project_voxel(vp, s_m, s_m + 12, cx, cy, cz, lengths[i]);
+  ndup[o] = pr.n;
+  bboxes[o] = pr.bbox;
+  quads[o] = pr.quads;
+  if (pr.n == 0) return;
+  // View-dependent colour of this visible voxel (sh_compute.cu:54-106).
+  float dx = cx - s_m[12 + 3], dy = cy - s_m[12 + 7], dz = cz - s_m[12 + 11];
+  const float rn = rnorm3df(dx, dy, dz);
+  dx = dx * rn; dy = dy * rn; dz = dz * rn;
+  const TS* sh = shs + (size_t)i * (M - 1) * 3;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) rgbs[3 * o + c] = sh_channel<DEG>(dx, dy, dz, ldf(sh0, 3 * (size_t)i + c), sh, c);
+}
+
+// Instance segment [start, start + count) of each sort group, clamped to the
+// capacity so that an overflowing step still stays inside the buffers.
+__global__ void group_segments_kernel(const __grid_constant__ GroupTable gt, int P, const uint32_t* __restrict__ scan,
+                                      uint32_t cap, uint32_t* __restrict__ segs) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= gt.n) return;
+  const size_t v0 = gt.v0[g], v1 = gt.v0[g + 1];
+  const uint32_t start = min(v0 == 0 ? 0u : scan[v0 * P - 1], cap);
+  const uint32_t end = min(scan[v1 * P - 1], cap);
+  segs[2 * g] = start;
+  segs[2 * g + 1] = end - start;
+}
+
+__global__ void __launch_bounds__(256)
+duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const int64_t* __restrict__ octpaths,
+                       const uint2* __restrict__ bboxes, const uint32_t* __restrict__ quads,
+                       const uint32_t* __restrict__ ndup, const uint32_t* __restrict__ scan, int rank_bits,
+                       uint64_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t cap,
+                       uint32_t* __restrict__ err) {
+  const int view = blockIdx.y;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= P) return;
+  const size_t o = (size_t)view * P + idx;
+  const uint32_t n = ndup[o];
+  if (n == 0) return;
+  const ViewParams& vp = views.v[view];
+  const uint32_t end = scan[o];
+  // Past the capacity: flag it, and still write the instances that fit so
+  // that every slot below the capacity holds a valid key.
+  if (end > cap) atomicOr(err, SVR_DEVERR_CAPACITY);
+  const uint32_t wend = min(end, cap);
+  uint32_t off = end - n;
+  int tx0, ty0, tx1, ty1;
+  bbox_tile_rect(bboxes[o], vp.grid_x, vp.grid_y, tx0, ty0, tx1, ty1);
+  const uint64_t path = (uint64_t)octpaths[idx];
+  const int low = (rank_bits == kRankBits) ? 0 : kRankBits - (rank_bits - 3);  // 3*(16-L)
+  if (low > 0 && (path & ((1ull << low) - 1ull)) != 0ull) atomicOr(err, SVR_DEVERR_LEVEL);
+  const uint32_t qb = quads[o];
+  for (uint32_t q = 0; q < 8; ++q) {
+    if (!(qb & (1u << q))) continue;
+    const uint64_t full = order_rank(path, q);
+    const uint64_t rank = (low == 0) ? full : (((full >> low) << 3) | q);
+    const uint32_t val = make_sort_val((uint32_t)idx, q);
+    for (int y = ty0; y <= ty1; ++y) {
+      for (int x = tx0; x <= tx1; ++x) {
+        const uint64_t tile = (uint64_t)(vp.sort_tile_off + (uint32_t)(y * vp.grid_x + x));
+        if (off < wend) {
+          keys[off] = (tile << rank_bits) | rank;
+          vals[off] = val;
+        }
+        ++off;
+      }
+    }
+  }
+  if (off != end) atomicOr(err, SVR_DEVERR_DUP_MISMATCH);
+}
+
+// dL/dSH of every voxel summed over views: sum_v basis(dir_v) * dL/drgb_v
+// (sh_compute.cu:110-176 per view).  Views where the voxel got no gradient
+// are skipped.
+template <int DEG>
+__global__ void __launch_bounds__(256)
+sh_bw_batch_kernel(const __grid_constant__ ViewTable views, int P, int M, const float* __restrict__ centers,
+                   const float* __restrict__ drgbs, float* __restrict__ dsh0, float* __restrict__ dshs) {
+  __shared__ float s_pos[kMaxViews][3];
+  for (int v = threadIdx.x; v < views.n; v += blockDim.x) {
+    s_pos[v][0] = views.v[v].c2w[3];
+    s_pos[v][1] = views.v[v].c2w[7];
+    s_pos[v][2] = views.v[v].c2w[11];
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  const float cx = centers[3 * (size_t)i], cy = centers[3 * (size_t)i + 1], cz = centers[3 * (size_t)i + 2];
+  float a0[3] = {0.f, 0.f, 0.f};
+  float acc[15][3];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.f;
+  for (int v = 0; v < views.n; ++v) {
+    const float* g = drgbs + 3 * ((size_t)v * P + i);
+    const float g0 = g[0], g1 = g[1], g2 = g[2];
+    if (g0 == 0.f && g1 == 0.f && g2 == 0.f) continue;
+    float x = cx - s_pos[v][0], y = cy - s_pos[v][1], z = cz - s_pos[v][2];
+    const float rn = rnorm3df(x, y, z);
+    x = x * rn; y = y * rn; z = z * rn;
+    float basis[15];
+    sh_basis_rest<DEG>(x, y, z, basis);
+    a0[0] += kC0 * g0; a0[1] += kC0 * g1; a0[2] += kC0 * g2;
+#pragma unroll
+    for (int k = 0; k < (DEG + 1) * (DEG + 1) - 1; ++k) {
+      acc[k][0] += basis[k] * g0;
+      acc[k][1] += basis[k] * g1;
+      acc[k][2] += basis[k] * g2;
+    }
+  }
+  dsh0[3 * (size_t)i + 0] = a0[0];
+  dsh0[3 * (size_t)i + 1] = a0[1];
+  dsh0[3 * (size_t)i + 2] = a0[2];
+  float* d = dshs + (size_t)i * (M - 1) * 3;
+#pragma unroll
+  for (int k = 0; k < (DEG + 1) * (DEG + 1) - 1; ++k) {
+    d[3 * k + 0] = acc[k][0];
+    d[3 * k + 1] = acc[k][1];
+    d[3 * k + 2] = acc[k][2];
+  }
+}
+
+inline int bit_width_u64(uint64_t n) {
+  int b = 0;
+  while (b < 64 && (n >> b)) ++b;
+  return b;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+struct svr_batch_plan {
+  ViewTable vt;
+  GroupTable gt;
+  int V;
+  int64_t P;
+  size_t cap;
+  int n_samp;
+  int rank_bits;
+  int key_bits;  // widest group key (all groups sorted with this many passes)
+  int64_t total_tiles, total_pixels;
+  // workspace layout (byte offsets)
+  size_t o_header, o_ndup, o_scan, o_bbox, o_quad, o_scan_tmp, o_rgbs, o_drgbs;
+  size_t o_ka, o_kb, o_va, o_vb, o_sort_tmp, o_ranges, o_tile_last, o_ncontrib;
+  size_t bytes;
+};
+
+namespace {
+
+struct BatchPtrs {
+  uint32_t* header;
+  uint32_t* ndup;
+  uint32_t* scan;
+  uint2* bbox;
+  uint32_t* quad;
+  void* scan_tmp;
+  float* rgbs;
+  float* drgbs;
+  uint64_t *ka, *kb;
+  uint32_t *va, *vb;
+  void* sort_tmp;
+  uint2* ranges;
+  uint32_t* tile_last;
+  uint32_t* ncontrib;
+};
+
+BatchPtrs ptrs(const svr_batch_plan* p, void* ws) {
+  char* b = static_cast<char*>(ws);
+  BatchPtrs q;
+  q.header = reinterpret_cast<uint32_t*>(b + p->o_header);
+  q.ndup = reinterpret_cast<uint32_t*>(b + p->o_ndup);
+  q.scan = reinterpret_cast<uint32_t*>(b + p->o_scan);
+  q.bbox = reinterpret_cast<uint2*>(b + p->o_bbox);
+  q.quad = reinterpret_cast<uint32_t*>(b + p->o_quad);
+  q.scan_tmp = b + p->o_scan_tmp;
+  q.rgbs = reinterpret_cast<float*>(b + p->o_rgbs);
+  q.drgbs = reinterpret_cast<float*>(b + p->o_drgbs);
+  q.ka = reinterpret_cast<uint64_t*>(b + p->o_ka);
+  q.kb = reinterpret_cast<uint64_t*>(b + p->o_kb);
+  q.va = reinterpret_cast<uint32_t*>(b + p->o_va);
+  q.vb = reinterpret_cast<uint32_t*>(b + p->o_vb);
+  q.sort_tmp = b + p->o_sort_tmp;
+  q.ranges = reinterpret_cast<uint2*>(b + p->o_ranges);
+  q.tile_last = reinterpret_cast<uint32_t*>(b + p->o_tile_last);
+  q.ncontrib = reinterpret_cast<uint32_t*>(b + p->o_ncontrib);
+  return q;
+}
+
+constexpr int kHeaderWords = 16 + 2 * kMaxViews;  // [0] count, [1] error, [16..] group segments
+
+inline int check_last() { return cudaGetLastError() == cudaSuccess ? SVR_OK : SVR_ERR_CUDA; }
+
+}  // namespace
+
+extern "C" {
+
+int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_t capacity, int n_samp_per_vox,
+                          int max_level, svr_batch_plan** out, size_t* workspace_bytes) {
+  if (!out || !workspace_bytes || !cams || n_views < 1 || n_views > kMaxViews || P < 1 ||
+      P >= (1ll << kVoxIdBits) || capacity < 0 || capacity > 0xffffffffll || n_samp_per_vox < 1 ||
+      n_samp_per_vox > kMaxSamples || max_level < 1 || max_level > kMaxLevels)
+    return SVR_ERR_SHAPE;
+  svr_batch_plan* p = new svr_batch_plan();
+  memset(&p->vt, 0, sizeof(p->vt));
+  p->V = n_views;
+  p->P = P;
+  p->cap = (size_t)capacity;
+  p->n_samp = n_samp_per_vox;
+  p->rank_bits = (max_level >= kMaxLevels) ? kRankBits : 3 * max_level + 3;
+  p->vt.n = n_views;
+  int64_t tiles = 0, pix = 0;
+  for (int v = 0; v < n_views; ++v) {
+    const svr_camera& c = cams[v];
+    if (c.width <= 0 || c.height <= 0 || c.width >= 65536 || c.height >= 65536 || !c.w2c || !c.c2w) {
+      delete p;
+      return SVR_ERR_SHAPE;
+    }
+    ViewParams& vp = p->vt.v[v];
+    vp.W = c.width;
+    vp.H = c.height;
+    vp.grid_x = (c.width + kTileX - 1) / kTileX;
+    vp.grid_y = (c.height + kTileY - 1) / kTileY;
+    vp.tanfovx = c.tanfovx;
+    vp.tanfovy = c.tanfovy;
+    vp.cx = c.cx;
+    vp.cy = c.cy;
+    vp.focal_x = 0.5f * c.width / c.tanfovx;
+    vp.focal_y = 0.5f * c.height / c.tanfovy;
+    vp.near_plane = c.near_plane;
+    vp.bg = c.bg_color;
+    vp.w2c = c.w2c;
+    vp.c2w = c.c2w;
+    vp.tile_base = (uint32_t)tiles;
+    vp.pix_base = (uint32_t)pix;
+    tiles += (int64_t)vp.grid_x * vp.grid_y;
+    pix += (int64_t)c.width * c.height;
+  }
+  if (pix > 0xffffffffll) {
+    delete p;
+    return SVR_ERR_SHAPE;
+  }
+  p->total_tiles = tiles;
+  p->total_pixels = pix;
+  // Greedy sort groups: consecutive views while the group's key fits 64 bits
+  // (SVR_MAX_KEY_BITS lowers that limit, to exercise grouping in tests).
+  int key_limit = 64;
+  if (const char* e = getenv("SVR_MAX_KEY_BITS")) key_limit = std::max(1, std::min(64, atoi(e)));
+  p->gt.n = 0;
+  p->key_bits = 0;
+  int v = 0;
+  while (v < n_views) {
+    const int g = p->gt.n++;
+    p->gt.v0[g] = v;
+    p->gt.tile_base[g] = p->vt.v[v].tile_base;
+    uint64_t gt_tiles = 0;
+    int kb = 0;
+    while (v < n_views) {
+      const uint64_t t2 = gt_tiles + (uint64_t)p->vt.v[v].grid_x * p->vt.v[v].grid_y;
+      const int kb2 = p->rank_bits + bit_width_u64(t2);
+      if (kb2 > key_limit && gt_tiles > 0) break;
+      if (kb2 > 64) {  // a single view does not fit
+        delete p;
+        return SVR_ERR_KEYBITS;
+      }
+      p->vt.v[v].sort_group = g;
+      p->vt.v[v].sort_tile_off = (uint32_t)gt_tiles;
+      gt_tiles = t2;
+      kb = kb2;
+      ++v;
+    }
+    p->key_bits = std::max(p->key_bits, kb);
+  }
+  p->gt.v0[p->gt.n] = n_views;
+  // workspace layout
+  const size_t VP = (size_t)n_views * (size_t)P;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    off = align_up(off);
+    const size_t r = off;
+    off += bytes;
+    return r;
+  };
+  p->o_header = take(kHeaderWords * sizeof(uint32_t));
+  p->o_ndup = take(VP * 4);
+  p->o_scan = take(VP * 4);
+  p->o_bbox = take(VP * 8);
+  p->o_quad = take(VP * 4);
+  p->o_scan_tmp = take(scan_temp_bytes(VP));
+  p->o_rgbs = take(VP * 12);
+  p->o_drgbs = take(VP * 12);
+  p->o_ka = take(p->cap * 8);
+  p->o_kb = take(p->cap * 8);
+  p->o_va = take(p->cap * 4);
+  p->o_vb = take(p->cap * 4);
+  p->o_sort_tmp = take(sort_temp_bytes(p->cap));
+  p->o_ranges = take((size_t)tiles * 8);
+  p->o_tile_last = take((size_t)tiles * 4);
+  p->o_ncontrib = take((size_t)pix * 4);
+  p->bytes = align_up(off) + kAlign;
+  ensure_sort_attributes();
+  *out = p;
+  *workspace_bytes = p->bytes;
+  return SVR_OK;
+}
+
+void svr_batch_plan_destroy(svr_batch_plan* plan) { delete plan; }
+int64_t svr_batch_plan_pixels(const svr_batch_plan* p) { return p ? p->total_pixels : 0; }
+int64_t svr_batch_plan_tiles(const svr_batch_plan* p) { return p ? p->total_tiles : 0; }
+int svr_batch_plan_groups(const svr_batch_plan* p) { return p ? p->gt.n : 0; }
+
+const uint32_t* svr_batch_count_ptr(const svr_batch_plan* p, const void* ws) {
+  return reinterpret_cast<const uint32_t*>(static_cast<const char*>(ws) + p->o_header);
+}
+uint32_t* svr_batch_error_ptr(const svr_batch_plan* p, void* ws) {
+  return reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + p->o_header) + 1;
+}
+
+int svr_batch_arrays(const svr_batch_plan* p, const void* ws, const float** rgbs, const float** drgbs,
+                     const uint64_t** ranges, const uint32_t** tile_last, const uint32_t** n_contrib,
+                     const uint32_t** ndup, const uint32_t** sorted_vals) {
+  if (!p || !ws) return SVR_ERR_SHAPE;
+  BatchPtrs q = ptrs(p, const_cast<void*>(ws));
+  const bool odd = (sort_passes(p->key_bits) & 1) != 0;
+  (void)odd;
+  if (rgbs) *rgbs = q.rgbs;
+  if (drgbs) *drgbs = q.drgbs;
+  if (ranges) *ranges = reinterpret_cast<const uint64_t*>(q.ranges);
+  if (tile_last) *tile_last = q.tile_last;
+  if (n_contrib) *n_contrib = q.ncontrib;
+  if (ndup) *ndup = q.ndup;
+  if (sorted_vals) *sorted_vals = q.vb;
+  return SVR_OK;
+}
+
+int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, const float* vox_centers,
+                      const float* vox_lengths, const void* sh0, const void* shs, int sh_bf16, int sh_degree, int M,
+                      void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (!p || !ws || !octree_paths || !vox_centers || !vox_lengths || !sh0 || sh_degree < 0 || sh_degree > 3 ||
+      M - 1 < (sh_degree + 1) * (sh_degree + 1) - 1 || (M > 1 && !shs))
+    return SVR_ERR_SHAPE;
+  BatchPtrs q = ptrs(p, ws);
+  const int P = (int)p->P;
+  const size_t VP = (size_t)p->V * p->P;
+  cudaMemsetAsync(q.header, 0, kHeaderWords * sizeof(uint32_t), stream);
+  dim3 grid((P + 255) / 256, p->V);
+#define SVR_PROJ(D)                                                                                           \
+  if (sh_bf16)                                                                                                \
+    project_sh_kernel<D, __nv_bfloat16><<<grid, 256, 0, stream>>>(                                            \
+        p->vt, P, vox_centers, vox_lengths, (const __nv_bfloat16*)sh0, (const __nv_bfloat16*)shs, M, q.ndup, \
+        q.bbox, q.quad, q.rgbs);                                                                              \
+  else                                                                                                        \
+    project_sh_kernel<D, float><<<grid, 256, 0, stream>>>(p->vt, P, vox_centers, vox_lengths,                \
+                                                          (const float*)sh0, (const float*)shs, M, q.ndup,   \
+                                                          q.bbox, q.quad, q.rgbs);
+  switch (sh_degree) {
+    case 0: SVR_PROJ(0) break;
+    case 1: SVR_PROJ(1) break;
+    case 2: SVR_PROJ(2) break;
+    default: SVR_PROJ(3) break;
+  }
+#undef SVR_PROJ
+  launch_scan_inclusive(q.ndup, q.scan, VP, q.scan_tmp, q.header, (unsigned long long)p->cap, q.header + 1, stream);
+  uint32_t* segs = q.header + 16;
+  group_segments_kernel<<<1, 64, 0, stream>>>(p->gt, P, q.scan, (uint32_t)p->cap, segs);
+  cudaMemsetAsync(q.ranges, 0, (size_t)p->total_tiles * sizeof(uint2), stream);
+  if (p->cap > 0) {
+    const bool odd = (sort_passes(p->key_bits) & 1) != 0;
+    uint64_t* k0 = odd ? q.ka : q.kb;
+    uint32_t* v0 = odd ? q.va : q.vb;
+    uint64_t* k1 = odd ? q.kb : q.ka;
+    uint32_t* v1 = odd ? q.vb : q.va;
+    duplicate_batch_kernel<<<grid, 256, 0, stream>>>(p->vt, P, octree_paths, q.bbox, q.quad, q.ndup, q.scan,
+                                                     p->rank_bits, k0, v0, (uint32_t)p->cap, q.header + 1);
+    for (int g = 0; g < p->gt.n; ++g) {
+      launch_radix_sort(k0, v0, k1, v1, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, p->key_bits, q.sort_tmp,
+                        stream);
+      const uint32_t g_tiles = (g + 1 < p->gt.n ? p->gt.tile_base[g + 1] : (uint32_t)p->total_tiles) -
+                               p->gt.tile_base[g];
+      launch_tile_ranges(q.kb, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, p->rank_bits, p->gt.tile_base[g],
+                         g_tiles, q.ranges, stream);
+    }
+  }
+  return check_last();
+}
+
+int svr_batch_render(svr_batch_plan* p, void* ws, const float* vox_centers, const float* vox_lengths,
+                     const void* geos, int geos_bf16, float* out_color, float* out_T, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (!p || !ws || !vox_centers || !vox_lengths || !geos || !out_color || !out_T) return SVR_ERR_SHAPE;
+  if ((reinterpret_cast<uintptr_t>(geos) & 15u) != 0) return SVR_ERR_ALIGN;
+  BatchPtrs q = ptrs(p, ws);
+  VoxelArrays va{q.bbox, vox_centers, vox_lengths, geos_bf16 ? nullptr : (const float*)geos,
+                 geos_bf16 ? (const __nv_bfloat16*)geos : nullptr, q.rgbs};
+  FwdTileOut out{q.tile_last, q.ncontrib, out_color, nullptr, nullptr, out_T, nullptr};
+  launch_render_fwd_batch(p->vt, (int)p->total_tiles, q.ranges, p->cap > 0 ? q.vb : nullptr, va, (int)p->P,
+                          (size_t)p->P * 3, out, p->n_samp, false, false, false, false, stream);
+  return check_last();
+}
+
+int svr_batch_backward(svr_batch_plan* p, void* ws, const float* vox_centers, const float* vox_lengths,
+                       const void* geos, int geos_bf16, const float* out_T, const float* dL_dcolor,
+                       const float* dL_dT, float* dL_dgeos, float* subdiv, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (!p || !ws || !vox_centers || !vox_lengths || !geos || !out_T || !dL_dcolor || !dL_dT || !dL_dgeos || !subdiv)
+    return SVR_ERR_SHAPE;
+  if ((reinterpret_cast<uintptr_t>(geos) & 15u) != 0) return SVR_ERR_ALIGN;
+  BatchPtrs q = ptrs(p, ws);
+  cudaMemsetAsync(q.drgbs, 0, (size_t)p->V * p->P * 12, stream);
+  VoxelArrays va{q.bbox, vox_centers, vox_lengths, geos_bf16 ? nullptr : (const float*)geos,
+                 geos_bf16 ? (const __nv_bfloat16*)geos : nullptr, q.rgbs};
+  BwdTileIn in{out_T, q.ncontrib, dL_dcolor, nullptr, nullptr, dL_dT, nullptr, nullptr, 0.f, 0.f, 0.f};
+  BwdTileOut out{dL_dgeos, q.drgbs, subdiv, q.header + 1};
+  launch_render_bwd_batch(p->vt, (int)p->total_tiles, q.ranges, q.tile_last, p->cap > 0 ? q.vb : nullptr, va,
+                          (int)p->P, (size_t)p->P * 3, in, out, p->n_samp, false, false, false, stream);
+  return check_last();
+}
+
+int svr_batch_sh_backward(svr_batch_plan* p, void* ws, const float* vox_centers, int sh_degree, int M,
+                          float* dL_dsh0, float* dL_dshs, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (!p || !ws || !vox_centers || !dL_dsh0 || sh_degree < 0 || sh_degree > 3 ||
+      M - 1 < (sh_degree + 1) * (sh_degree + 1) - 1 || (M > 1 && !dL_dshs))
+    return SVR_ERR_SHAPE;
+  BatchPtrs q = ptrs(p, ws);
+  const int P = (int)p->P;
+  const int g = (P + 255) / 256;
+  switch (sh_degree) {
+    case 0: sh_bw_batch_kernel<0><<<g, 256, 0, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
+    case 1: sh_bw_batch_kernel<1><<<g, 256, 0, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
+    case 2: sh_bw_batch_kernel<2><<<g, 256, 0, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
+    default: sh_bw_batch_kernel<3><<<g, 256, 0, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
+  }
+  return check_last();
+}
+
+}  // extern "C"

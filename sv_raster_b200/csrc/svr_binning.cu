@@ -18,6 +18,8 @@
 #include "svr_views.cuh"
 #include "svr_kernels.h"
 
+#include <mutex>
+
 namespace svr {
 
 // --------------------------------------------------------------------------
@@ -179,10 +181,10 @@ duplicate_kernel(const __grid_constant__ ViewTable views, int P,
   const ViewParams& vp = views.v[view];
   const uint32_t end = scan[o];
   uint32_t off = end - n;
-  if (end > cap) {
-    atomicOr(err, SVR_DEVERR_CAPACITY);
-    return;
-  }
+  // Past the capacity: flag it, and still write the instances that fit so
+  // that every slot below the capacity holds a valid key.
+  if (end > cap) atomicOr(err, SVR_DEVERR_CAPACITY);
+  const uint32_t wend = min(end, cap);
   if ((uint32_t)idx >= (1u << kVoxIdBits)) {
     atomicOr(err, SVR_DEVERR_VOXID);
     return;
@@ -198,7 +200,7 @@ duplicate_kernel(const __grid_constant__ ViewTable views, int P,
     for (int y = ty0; y <= ty1; ++y) {
       for (int x = tx0; x <= tx1; ++x) {
         const uint64_t tile = (uint64_t)(y * vp.grid_x + x);
-        if (off < end) {
+        if (off < wend) {
           keys[off] = make_sort_key(tile, rank);
           vals[off] = val;
         }
@@ -243,12 +245,14 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 }
 
 __global__ void __launch_bounds__(kSortThreads)
-radix_upsweep_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ d_n, uint32_t cap,
-                     int shift, uint32_t* __restrict__ hist, int nblocks) {
+radix_upsweep_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ d_start,
+                     const uint32_t* __restrict__ d_n, uint32_t cap, int shift, uint32_t* __restrict__ hist,
+                     int nblocks) {
   __shared__ uint32_t s_hist[kSortWarps][kRadix];
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&s_hist[0][0])[i] = 0u;
   __syncthreads();
   const uint32_t n = min(*d_n, cap);
+  if (d_start) keys += *d_start;
   const size_t start = (size_t)blockIdx.x * kSortTile;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (start < n) {
@@ -309,7 +313,7 @@ struct DownsweepSmem {
 __global__ void __launch_bounds__(kSortThreads)
 radix_downsweep_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                        uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
-                       const uint32_t* __restrict__ d_n, uint32_t cap, int shift,
+                       const uint32_t* __restrict__ d_start, const uint32_t* __restrict__ d_n, uint32_t cap, int shift,
                        const uint32_t* __restrict__ hist, const uint32_t* __restrict__ digit_total,
                        int nblocks) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -317,6 +321,10 @@ radix_downsweep_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restr
   const uint32_t n = min(*d_n, cap);
   const size_t start = (size_t)blockIdx.x * kSortTile;
   if (start >= n) return;
+  if (d_start) {
+    const uint32_t s0 = *d_start;
+    kin += s0; vin += s0; kout += s0; vout += s0;
+  }
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   for (int i = tid; i < kSortWarps * kRadix; i += kSortThreads) (&sm.warp_cnt[0][0])[i] = 0u;
@@ -381,28 +389,39 @@ radix_downsweep_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restr
   }
 }
 
-// Sorts `n` (read on the device) pairs held in (k0, v0) using (k1, v1) as the
-// ping-pong buffer.  Returns 0 if the result is in (k0, v0), 1 if in (k1, v1).
-int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, const uint32_t* d_n, uint32_t cap,
-                      int key_bits, void* temp, cudaStream_t stream) {
+// Opt the downsweep kernel into >48 KB of dynamic shared memory, once per
+// device (a function attribute, so it must not be set inside graph capture
+// for the first time: plan creation and every plain call reach it first).
+void ensure_sort_attributes() {
+  static std::once_flag flags[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  std::call_once(flags[dev], [] {
+    cudaFuncSetAttribute(radix_downsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(DownsweepSmem));
+  });
+}
+
+// Sorts the `*d_n` pairs starting at element `*d_start` (both read on the
+// device; d_start may be null for 0) of (k0, v0), using (k1, v1) as the
+// ping-pong buffer; `cap` bounds the count and sizes the grid.  Returns 0 if
+// the result is in (k0, v0), 1 if in (k1, v1).
+int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, const uint32_t* d_start,
+                      const uint32_t* d_n, uint32_t cap, int key_bits, void* temp, cudaStream_t stream) {
   const int passes = sort_passes(key_bits);
   if (cap == 0 || passes == 0) return 0;
   const int nb = sort_blocks(cap);
   uint32_t* hist = reinterpret_cast<uint32_t*>(temp);
   uint32_t* digit_total = hist + (size_t)nb * kRadix;
   const size_t smem = sizeof(DownsweepSmem);
-  static bool attr_set = false;  // idempotent attribute, safe to repeat
-  if (!attr_set) {
-    cudaFuncSetAttribute(radix_downsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_set = true;
-  }
+  ensure_sort_attributes();
   uint64_t* kin = k0; uint32_t* vin = v0; uint64_t* kout = k1; uint32_t* vout = v1;
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
-    radix_upsweep_kernel<<<nb, kSortThreads, 0, stream>>>(kin, d_n, cap, shift, hist, nb);
+    radix_upsweep_kernel<<<nb, kSortThreads, 0, stream>>>(kin, d_start, d_n, cap, shift, hist, nb);
     radix_scan_rows_kernel<<<kRadix, 1024, 0, stream>>>(hist, nb, digit_total);
-    radix_downsweep_kernel<<<nb, kSortThreads, smem, stream>>>(kin, vin, kout, vout, d_n, cap, shift, hist,
-                                                               digit_total, nb);
+    radix_downsweep_kernel<<<nb, kSortThreads, smem, stream>>>(kin, vin, kout, vout, d_start, d_n, cap, shift,
+                                                               hist, digit_total, nb);
     std::swap(kin, kout);
     std::swap(vin, vout);
   }
@@ -411,30 +430,39 @@ int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, co
 
 // --------------------------------------------------------------------------
 // Tile ranges from the sorted keys (forward.cu:576-598); `ranges` must be
-// zeroed beforehand.
+// zeroed beforehand.  The segment [*d_start, *d_start + *d_n) holds keys
+// whose bits above `rank_bits` are a tile id relative to `tile_base`; ranges
+// are written as absolute element offsets.
 // --------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
-tile_ranges_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ d_n, uint32_t cap,
-                   uint2* __restrict__ ranges) {
+tile_ranges_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ d_start,
+                   const uint32_t* __restrict__ d_n, uint32_t cap, int rank_bits, uint32_t tile_base,
+                   uint32_t n_tiles, uint2* __restrict__ ranges) {
   const uint32_t n = min(*d_n, cap);
+  const uint32_t s0 = d_start ? *d_start : 0u;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint32_t cur = (uint32_t)(keys[i] >> kRankBits);
+  keys += s0;
+  ranges += tile_base;
+  const uint32_t cur = (uint32_t)(keys[i] >> rank_bits);
+  const uint32_t prv = i > 0 ? (uint32_t)(keys[i - 1] >> rank_bits) : 0u;
+  if (cur >= n_tiles || prv >= n_tiles) return;  // cannot happen for keys written by duplication
   if (i == 0) {
-    ranges[cur].x = 0;
+    ranges[cur].x = s0;
   } else {
-    const uint32_t prev = (uint32_t)(keys[i - 1] >> kRankBits);
-    if (cur != prev) {
-      ranges[prev].y = i;
-      ranges[cur].x = i;
+    if (cur != prv) {
+      ranges[prv].y = s0 + i;
+      ranges[cur].x = s0 + i;
     }
   }
-  if (i == n - 1) ranges[cur].y = n;
+  if (i == n - 1) ranges[cur].y = s0 + n;
 }
 
-void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_n, uint32_t cap, uint2* ranges, cudaStream_t stream) {
+void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_start, const uint32_t* d_n, uint32_t cap,
+                        int rank_bits, uint32_t tile_base, uint32_t n_tiles, uint2* ranges, cudaStream_t stream) {
   if (cap == 0) return;
-  tile_ranges_kernel<<<(cap + 255) / 256, 256, 0, stream>>>(keys, d_n, cap, ranges);
+  tile_ranges_kernel<<<(cap + 255) / 256, 256, 0, stream>>>(keys, d_start, d_n, cap, rank_bits, tile_base, n_tiles,
+                                                           ranges);
 }
 
 }  // namespace svr

@@ -253,8 +253,9 @@ int svr_rasterize_binning(const svr_camera* cam, int64_t P, int64_t num_rendered
     uint32_t* v1 = odd ? c.bl.vals_b : c.bl.vals_a;
     launch_duplicate(c.vt, (int)P, octree_paths, c.g.bbox, c.g.quad, c.g.ndup, c.g.scan, k0, v0, (uint32_t)c.n,
                      c.g.header + 1, stream);
-    launch_radix_sort(k0, v0, k1, v1, c.g.header, (uint32_t)c.n, c.key_bits, c.bl.sort_temp, stream);
-    launch_tile_ranges(c.bl.keys_b, c.g.header, (uint32_t)c.n, c.im.ranges, stream);
+    launch_radix_sort(k0, v0, k1, v1, nullptr, c.g.header, (uint32_t)c.n, c.key_bits, c.bl.sort_temp, stream);
+    launch_tile_ranges(c.bl.keys_b, nullptr, c.g.header, (uint32_t)c.n, kRankBits, 0u,
+                       (uint32_t)(vp.grid_x * vp.grid_y), c.im.ranges, stream);
   }
   return check_launch(debug, stream);
 }

@@ -27,23 +27,25 @@ void launch_duplicate(const ViewTable& views, int P, const int64_t* octpaths, co
                       const uint32_t* quads, const uint32_t* ndup, const uint32_t* scan, uint64_t* keys,
                       uint32_t* vals, uint32_t cap, uint32_t* err, cudaStream_t stream);
 size_t sort_temp_bytes(size_t cap);
+void ensure_sort_attributes();
 int sort_passes(int key_bits);
-int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, const uint32_t* d_n, uint32_t cap,
-                      int key_bits, void* temp, cudaStream_t stream);
-void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_n, uint32_t cap, uint2* ranges, cudaStream_t stream);
+int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, const uint32_t* d_start,
+                      const uint32_t* d_n, uint32_t cap, int key_bits, void* temp, cudaStream_t stream);
+void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_start, const uint32_t* d_n, uint32_t cap,
+                        int rank_bits, uint32_t tile_base, uint32_t n_tiles, uint2* ranges, cudaStream_t stream);
 
 // svr_render_fwd.cu / svr_render_bwd.cu
 void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t* vals, const VoxelArrays& va,
                        const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
                        cudaStream_t stream);
-void launch_render_fwd_batch(const ViewTable& views, int n_items, const int* item_view, const uint2* ranges,
+void launch_render_fwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* vals, const VoxelArrays& va, int P, size_t rgb_view_stride,
                              const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
                              cudaStream_t stream);
 void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t* tile_last, const uint32_t* vals,
                        const VoxelArrays& va, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
                        bool dist, bool normal, cudaStream_t stream);
-void launch_render_bwd_batch(const ViewTable& views, int n_items, const int* item_view, const uint2* ranges,
+void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
                              size_t rgb_view_stride, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
                              bool dist, bool normal, cudaStream_t stream);

@@ -49,12 +49,12 @@ struct BwdBatchArgs {
 
 template <int NS, bool DEPTH, bool DIST, bool NORMAL>
 __global__ void __launch_bounds__(kBatch)
-render_bwd_batch_kernel(const __grid_constant__ BwdBatchArgs a, const int* __restrict__ item_view) {
+render_bwd_batch_kernel(const __grid_constant__ BwdBatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BwdSmem& sm = *reinterpret_cast<BwdSmem*>(smem_raw);
   const int item = blockIdx.x;
   if (item >= a.n_items) return;
-  const int view = item_view[item];
+  const int view = view_of_tile(a.views, item);
   const ViewParams& vp = a.views.v[view];
   if (threadIdx.x < 12) sm.c2w[threadIdx.x] = vp.c2w[threadIdx.x];
   __syncthreads();
@@ -79,14 +79,10 @@ render_bwd_batch_kernel(const __grid_constant__ BwdBatchArgs a, const int* __res
                                            in, o, sm.s, sm.grad);
 }
 
-template <typename F>
-static void set_smem(F* f, size_t bytes) {
-  cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
+static_assert(sizeof(BwdSmem) <= 48 * 1024, "backward staging must fit the default shared-memory limit");
 
 #define SVR_BWD_CASE(KERNEL, NS_, D_, T_, N_)                                    \
   if (ns == NS_ && depth == D_ && dist == T_ && normal == N_) {                  \
-    set_smem(KERNEL<NS_, D_, T_, N_>, sizeof(BwdSmem));                          \
     KERNEL<NS_, D_, T_, N_><<<grid, kBatch, sizeof(BwdSmem), stream>>>(ARGS);    \
     return;                                                                      \
   }
@@ -108,14 +104,14 @@ void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t
 #undef ARGS
 }
 
-void launch_render_bwd_batch(const ViewTable& views, int n_items, const int* item_view, const uint2* ranges,
+void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
                              size_t rgb_view_stride, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
                              bool dist, bool normal, cudaStream_t stream) {
   if (n_items <= 0) return;
   BwdBatchArgs args{views, n_items, ranges, tile_last, vals, va, P, rgb_view_stride, in, out};
   dim3 grid(n_items);
-#define ARGS args, item_view
+#define ARGS args
   SVR_BWD_SWITCH(render_bwd_batch_kernel)
 #undef ARGS
 }

@@ -1,5 +1,6 @@
-// Forward compositing kernels (plain one-view grid and the multi-view
-// persistent work-queue form) and their template dispatch.
+// Forward compositing kernels (plain one-view grid and the multi-view form,
+// one CTA per (view, tile) of every view in a single launch) and their
+// template dispatch.
 #include "svr_kernels.h"
 #include "svr_render_fwd.cuh"
 
@@ -41,13 +42,13 @@ struct FwdBatchArgs {
 
 template <int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
 __global__ void __launch_bounds__(kBatch)
-render_fwd_batch_kernel(const __grid_constant__ FwdBatchArgs a, const int* __restrict__ item_view) {
+render_fwd_batch_kernel(const __grid_constant__ FwdBatchArgs a) {
   __shared__ StageSmem s;
   __shared__ float s_c2w[12];
   __shared__ uint32_t s_red[kBatch / 32];
   const int item = blockIdx.x;
   if (item >= a.n_items) return;
-  const int view = item_view[item];
+  const int view = view_of_tile(a.views, item);
   const ViewParams& vp = a.views.v[view];
   if (threadIdx.x < 12) s_c2w[threadIdx.x] = vp.c2w[threadIdx.x];
   __syncthreads();
@@ -104,14 +105,14 @@ void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t
   SVR_FWD_DISPATCH(render_fwd_kernel, grid, stream, args);
 }
 
-void launch_render_fwd_batch(const ViewTable& views, int n_items, const int* item_view, const uint2* ranges,
+void launch_render_fwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* vals, const VoxelArrays& va, int P, size_t rgb_view_stride,
                              const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
                              cudaStream_t stream) {
   if (n_items <= 0) return;
   FwdBatchArgs args{views, n_items, ranges, vals, va, P, rgb_view_stride, out};
   dim3 grid(n_items);
-  SVR_FWD_DISPATCH(render_fwd_batch_kernel, grid, stream, args, item_view);
+  SVR_FWD_DISPATCH(render_fwd_batch_kernel, grid, stream, args);
 }
 
 }  // namespace svr

@@ -15,5 +15,6 @@
 #define SVR_DEVERR_RANGE 0x2u          /* tile_last outside its range (backward.cu:122-133) */
 #define SVR_DEVERR_CAPACITY 0x4u       /* instances exceeded the caller's capacity */
 #define SVR_DEVERR_VOXID 0x8u          /* voxel id does not fit in 29 bits */
+#define SVR_DEVERR_LEVEL 0x10u         /* an octree path is deeper than the declared max level */
 
 #endif

@@ -19,11 +19,24 @@ struct ViewParams {
   const float* c2w;      // device, row-major 4x4 (first 12 read)
   uint32_t tile_base;    // first global tile id of this view (batched path)
   uint32_t pix_base;     // first global pixel of this view (batched path)
+  uint32_t sort_tile_off;  // tile id offset of this view inside its sort group
+  int sort_group;          // sort group of this view
 };
 
 struct ViewTable {
   int n;
   ViewParams v[kMaxViews];
 };
+
+// View owning global tile `item` (views are laid out by ascending tile_base).
+__device__ __forceinline__ int view_of_tile(const ViewTable& t, int item) {
+  int lo = 0, hi = t.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if ((int)t.v[mid].tile_base <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
 
 }  // namespace svr

@@ -196,5 +196,193 @@ class PlainWorkload:
         return dict(ms_total=e0.elapsed_time(e1), h2d=h2d, d2h=4)
 
 
-class BatchedWorkload(PlainWorkload):
-    """Placeholder until the multi-view path lands: same as plain."""
+class _DevCam:
+    def __init__(self, c, dev):
+        self.width, self.height = c.width, c.height
+        self.tanfovx, self.tanfovy, self.cx, self.cy, self.near = c.tanfovx, c.tanfovy, c.cx, c.cy, c.near
+        self.w2c = _t(c.w2c, dev)
+        self.c2w = _t(c.c2w, dev)
+
+
+class BatchedWorkload:
+    """All views in one launch per stage, bf16 storage of densities and SH,
+    fp32 compositing / gradients, no host sync inside a step (the step is
+    also captured as a CUDA graph)."""
+
+    def __init__(self, scene, dev, storage=torch.bfloat16, graph=True):
+        from .batched import BatchedRasterizer
+        self.sc = scene
+        self.dev = dev
+        self.P = scene.n_voxels
+        self.octpath = _t(scene.octpath.reshape(-1, 1), dev, torch.int64)
+        self.centers = _t(scene.centers, dev)
+        self.lengths = _t(scene.lengths, dev)
+        self.geos = _t(scene.geos, dev).to(storage).contiguous()
+        self.sh0 = _t(scene.sh0, dev).to(storage).contiguous()
+        self.shs = _t(scene.shs, dev).to(storage).contiguous()
+        self.cams = [_DevCam(c, dev) for c in scene.cameras]
+        self.raster = BatchedRasterizer(self.cams, self.octpath, self.centers, self.lengths,
+                                        max_level=scene.max_level)
+        self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
+        r = self.raster
+        tg = [_t(t, dev).reshape(-1) for t in scene.targets]
+        self.target = torch.cat([tg[i % len(tg)] for i in range(len(self.cams))])
+        scale = [torch.full((3 * h * w,), 2.0 / (3 * h * w), device=dev) for h, w in r.sizes]
+        self.scale = torch.cat(scale)
+        self.color = torch.zeros(3 * r.n_pixels, device=dev)
+        self.T = torch.zeros(r.n_pixels, device=dev)
+        self.dT = torch.zeros(r.n_pixels, device=dev)
+        self.dC = torch.zeros_like(self.color)
+        self.grads = (torch.zeros(self.P, 8, device=dev), torch.zeros(self.P, device=dev),
+                      torch.zeros(self.P, 3, device=dev), torch.zeros(self.P, 15, 3, device=dev))
+        self.timers = {}
+        self.graph = None
+        self.use_graph = graph
+
+    def reset_kernel_timers(self):
+        self.timers = {k: _Timer(k) for k in ("prepare", "render_fwd", "render_bwd", "sh_bwd")}
+
+    def _stage(self, name, fn, nbytes=0.0):
+        if name not in self.timers:
+            return fn()
+        st = torch.cuda.current_stream(self.dev)
+        e1 = self.timers[name].start(st)
+        r = fn()
+        e1.record(st)
+        self.timers[name].bytes.append(nbytes)
+        return r
+
+    def _bytes(self):
+        I, V = self.total, self._visible()
+        px, T_ = self.raster.n_pixels, self.raster.n_tiles
+        geo_b = 2 * 8 if self.geos.dtype == torch.bfloat16 else 4 * 8
+        rec = 8 + 12 + 4 + geo_b + 12
+        sh_b = 48 * (2 if self.sh0.dtype == torch.bfloat16 else 4)
+        return dict(
+            prepare=36.0 * self.P * len(self.cams) + V * (sh_b + 12) + 8.0 * self.P * len(self.cams) +
+            (28.0 * V + 12.0 * I) + 24.0 * I * 1 + 8.0 * I + 8.0 * T_,
+            render_fwd=I * (4.0 + rec) + 20.0 * px + 12.0 * T_,
+            render_bwd=I * (4.0 + rec) + 24.0 * px + 48.0 * V,
+            sh_bwd=self.P * len(self.cams) * 12.0 + V * 12.0 + self.P * (12 + 192.0))
+
+    def _visible(self):
+        if not hasattr(self, "_V"):
+            self._V = int((self.raster.arrays()["ndup"] > 0).sum())
+        return self._V
+
+    def _eager_step(self, timed):
+        r = self.raster
+        b = self._bytes() if timed else {}
+        st = (lambda n, f: self._stage(n, f, b[n])) if timed else (lambda n, f: f())
+        st("prepare", lambda: r.prepare(self.sh0, self.shs, 3))
+        st("render_fwd", lambda: r.render(self.geos, self.color, self.T))
+        torch.mul(self.scale, self.color - self.target, out=self.dC)
+        g = self.grads
+        st("render_bwd", lambda: self._bwd_render())
+        st("sh_bwd", lambda: self._bwd_sh())
+        return g
+
+    def _bwd_render(self):
+        r = self.raster
+        L = lib()
+        g = self.grads
+        g[0].zero_()
+        g[1].zero_()
+        p = lambda t: ctypes.c_void_p(t.data_ptr())
+        s = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+        check(L.svr_batch_backward(r.plan, p(r.ws), p(self.centers), p(self.lengths), p(self.geos),
+                                   int(self.geos.dtype == torch.bfloat16), p(self.T), p(self.dC), p(self.dT),
+                                   p(g[0]), p(g[1]), s), "batch_backward")
+
+    def _bwd_sh(self):
+        r = self.raster
+        g = self.grads
+        p = lambda t: ctypes.c_void_p(t.data_ptr())
+        s = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+        check(lib().svr_batch_sh_backward(r.plan, p(r.ws), p(self.centers), 3, 16, p(g[2]), p(g[3]), s),
+              "batch_sh_backward")
+
+    def capture(self):
+        """Capture one step as a CUDA graph (after warm-up launches)."""
+        s = torch.cuda.Stream(self.dev)
+        s.wait_stream(torch.cuda.current_stream(self.dev))
+        with torch.cuda.stream(s):
+            self._eager_step(False)
+        torch.cuda.current_stream(self.dev).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._eager_step(False)
+        self.graph = g
+
+    def step(self):
+        if self.timers:
+            return self._eager_step(True)
+        if self.use_graph:
+            if self.graph is None:
+                self.capture()
+            self.graph.replay()
+        else:
+            self._eager_step(False)
+
+    def check_errors(self):
+        total, err = self.raster.header()
+        if err:
+            raise RuntimeError(f"batched step reported device error word 0x{err:x} (instances {total}, "
+                               f"capacity {self.raster.capacity})")
+        return total
+
+    def instances_per_view(self):
+        return int(self.total / max(1, len(self.cams)))
+
+    def launches_per_step(self):
+        T_ = max(self.raster.n_tiles, 1)
+        passes = math.ceil((3 * self.sc.max_level + 3 + int(T_).bit_length()) / 8)
+        g = self.raster.n_groups
+        # project 1 + scan 3 + segments 1 + duplicate 1 + (sort 3/pass + ranges 1) per group + fwd 1 + bwd 1 + sh 1
+        return 1 + 3 + 1 + 1 + g * (3 * passes + 1) + 1 + 1 + 1
+
+    def kernel_stats(self):
+        torch.cuda.synchronize()
+        table = [t.stats() for t in self.timers.values()]
+        dom = max(table, key=lambda s: s["ms"])
+        nsteps = max(1, len(self.timers["render_fwd"].pairs))
+        fwd_ms = sum(s["ms"] for s in table if s["name"] in ("prepare", "render_fwd")) / nsteps
+        return dict(table=[{k: (round(v, 4) if isinstance(v, float) else v) for k, v in s.items()} for s in table],
+                    dominant=dom, fwd_ms_per_view=fwd_ms / len(self.cams))
+
+    def e2e(self, steps, warmup):
+        """Public autograd API (BatchedRender) with the targets and camera
+        matrices copied from pinned host memory each step and the loss read
+        back; cameras are updated in place so the plan stays valid."""
+        from .batched import BatchedRender
+        dev = self.dev
+        host_t = self.target.cpu().pin_memory()
+        host_w2c = [torch.from_numpy(c.w2c).pin_memory() for c in self.sc.cameras]
+        host_c2w = [torch.from_numpy(c.c2w).pin_memory() for c in self.sc.cameras]
+        tgt = torch.empty_like(self.target)
+        geos = self.geos.clone().requires_grad_(True)
+        sh0 = self.sh0.clone().requires_grad_(True)
+        shs = self.shs.clone().requires_grad_(True)
+        h2d = host_t.numel() * 4 + len(self.cams) * 2 * 64
+
+        def one_step():
+            tgt.copy_(host_t, non_blocking=True)
+            for c, a, b in zip(self.cams, host_w2c, host_c2w):
+                c.w2c.copy_(a, non_blocking=True)
+                c.c2w.copy_(b, non_blocking=True)
+            color, T = BatchedRender.apply(self.raster, 3, geos, sh0, shs)
+            loss = (self.scale * 0.5 * (color - tgt) ** 2).sum()
+            loss.backward()
+            return float(loss.detach().cpu())
+
+        for _ in range(warmup):
+            one_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = torch.cuda.current_stream(dev)
+        e0.record(st)
+        for _ in range(steps):
+            one_step()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return dict(ms_total=e0.elapsed_time(e1), h2d=h2d, d2h=4)

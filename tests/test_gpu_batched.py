@@ -1,0 +1,197 @@
+"""GPU tests of the multi-view batched path: per view it must reproduce the
+plain path (bit-identical images and contributor counts in fp32 storage),
+gradients summed over views must match the plain per-view sums, bf16 storage
+must stay within the PSNR budget of the FP64 oracle, the CUDA-graph replay
+must equal eager execution, and capacity overflow must be reported, not
+crash."""
+import math
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from refutil import SceneTensors, rel_err
+from sv_raster_b200 import _C as mC
+from sv_raster_b200 import synthetic
+from sv_raster_b200.batched import BatchedRasterizer, BatchedRender
+
+pytestmark = pytest.mark.gpu
+
+
+class DevCam:
+    def __init__(self, c):
+        self.width, self.height = c.width, c.height
+        self.tanfovx, self.tanfovy, self.cx, self.cy, self.near = c.tanfovx, c.tanfovy, c.cx, c.cy, c.near
+        self.w2c = torch.from_numpy(c.w2c).cuda()
+        self.c2w = torch.from_numpy(c.c2w).cuda()
+
+
+@pytest.fixture(scope="module")
+def c1():
+    return SceneTensors(synthetic.config_scene("c1"))
+
+
+def _plain_view(C, cam_i, sh0, shs, geos):
+    cam, w2c, c2w = C.cam(cam_i)
+    ndup, geom = mC.rasterize_preprocess(cam.width, cam.height, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w,
+                                         cam.near, C.octpath, C.centers, C.lengths)
+    vis = torch.where(ndup > 0)[0]
+    rgbs = mC.sh_compute(3, vis, C.centers, c2w[:3, 3].contiguous(), sh0, shs)
+    out = mC.rasterize_voxels(1, cam.width, cam.height, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w, 0.0,
+                              False, False, False, False, C.octpath, C.centers, C.lengths, geos, rgbs, geom)
+    return dict(ndup=ndup, geom=geom, R=out[0], binning=out[1], img=out[2], color=out[3], T=out[6], rgbs=rgbs,
+                vis=vis, cam=cam, w2c=w2c, c2w=c2w)
+
+
+def _raster(C, max_level=None, views=(0, 1, 2), **kw):
+    cams = [DevCam(C.scene.cameras[i]) for i in views]
+    r = BatchedRasterizer(cams, C.octpath, C.centers, C.lengths,
+                          max_level=max_level or C.scene.max_level, **kw)
+    return r, cams
+
+
+@pytest.mark.parametrize("max_key_bits", [None, 38])
+def test_batched_forward_equals_plain(c1, max_key_bits, monkeypatch):
+    if max_key_bits:
+        monkeypatch.setenv("SVR_MAX_KEY_BITS", str(max_key_bits))  # forces one sort group per view
+    r, _ = _raster(c1)
+    if max_key_bits:
+        assert r.n_groups == 3
+    total = r.fit_capacity(c1.sh0, c1.shs, 3)
+    r.prepare(c1.sh0, c1.shs, 3)
+    color, T = r.render(c1.geos)
+    torch.cuda.synchronize()
+    n, err = r.header()
+    assert err == 0 and n == total
+    arr = r.arrays()
+    cols, Ts = r.split_color(color), r.split_pixels(T)
+    tile0 = 0
+    for k in range(3):
+        p = _plain_view(c1, k, c1.sh0, c1.shs, c1.geos)
+        assert torch.equal(arr["ndup"][k], p["ndup"])
+        assert torch.equal(arr["rgbs"][k][p["vis"]], p["rgbs"][p["vis"]])
+        assert torch.equal(cols[k], p["color"]), f"view {k}: colour differs"
+        assert torch.equal(Ts[k], p["T"]), f"view {k}: T differs"
+        cam = p["cam"]
+        pr, ptl, pnc = mC.unpack_ImageState(cam.width, cam.height, p["img"])
+        H, W = cam.height, cam.width
+        nc = arr["n_contrib"][r.pix_offsets[k]:r.pix_offsets[k + 1]].view(H, W)
+        assert torch.equal(nc, pnc), f"view {k}: n_contrib differs"
+        nt = pr.shape[0] * pr.shape[1]
+        br = arr["ranges"][tile0:tile0 + nt].view(pr.shape)
+        btl = arr["tile_last"][tile0:tile0 + nt].view(ptl.shape)
+        assert torch.equal(br[..., 1] - br[..., 0], pr[..., 1] - pr[..., 0])
+        assert torch.equal(btl - br[..., 0], ptl - pr[..., 0])
+        # the tile lists themselves (values) are the plain path's, tile by tile
+        _, pv = mC.unpack_sorted_list(p["binning"], p["R"], W, H)
+        bv = arr["sorted_vals"]
+        nz = (pr[..., 1] > pr[..., 0]).reshape(-1).nonzero().reshape(-1)
+        for t in nz[:: max(1, len(nz) // 25)].tolist():
+            a0, a1 = int(pr.view(-1, 2)[t, 0]), int(pr.view(-1, 2)[t, 1])
+            b0 = int(br.view(-1, 2)[t, 0])
+            assert torch.equal(bv[b0:b0 + a1 - a0], pv[a0:a1])
+        tile0 += nt
+
+
+def test_batched_backward_equals_plain_sum(c1):
+    r, _ = _raster(c1)
+    r.fit_capacity(c1.sh0, c1.shs, 3)
+    geos = c1.geos.clone().requires_grad_(True)
+    sh0 = c1.sh0.clone().requires_grad_(True)
+    shs = c1.shs.clone().requires_grad_(True)
+    color, T = BatchedRender.apply(r, 3, geos, sh0, shs)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    wC = torch.randn(color.shape, device="cuda", generator=g)
+    wT = torch.randn(T.shape, device="cuda", generator=g)
+    ((color * wC).sum() + (T * wT).sum()).backward()
+    # plain path, one view at a time through the reference-compatible autograd surface
+    from sv_raster_b200 import renderer
+    geos2 = c1.geos.clone().requires_grad_(True)
+    sh02 = c1.sh0.clone().requires_grad_(True)
+    shs2 = c1.shs.clone().requires_grad_(True)
+    wCs, wTs = r.split_color(wC), r.split_pixels(wT)
+    for k in range(3):
+        cam, w2c, c2w = c1.cam(k)
+        s = renderer.RasterSettings("sh", 1, cam.width, cam.height, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c,
+                                    c2w)
+
+        def vox_fn(idx, cam_pos, mode):
+            rg = renderer.SH_eval.apply(3, idx, c1.centers, cam_pos, None, sh02, shs2)
+            return {"geos": geos2, "rgbs": rg, "subdiv_p": torch.ones(len(c1.centers), 1, device="cuda")}
+
+        col, _, _, Tk, _ = renderer.rasterize_voxels(s, c1.octpath, c1.centers, c1.lengths, vox_fn)
+        ((col * wCs[k]).sum() + (Tk * wTs[k]).sum()).backward()
+    assert rel_err(geos.grad, geos2.grad) < 1e-5
+    assert rel_err(sh0.grad, sh02.grad) < 1e-5
+    assert rel_err(shs.grad, shs2.grad) < 1e-5
+
+
+def _psnr(a, b):
+    mse = float(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2))
+    return 10 * math.log10(1.0 / max(mse, 1e-30))
+
+
+def test_bf16_storage_psnr_vs_fp64_oracle(c1):
+    """bf16 storage, fp32 compositing: the image's PSNR against a target is
+    within 0.01 dB of the FP64 oracle's on the same (bf16-rounded) parameters."""
+    geos16 = c1.geos.to(torch.bfloat16)
+    sh016, shs16 = c1.sh0.to(torch.bfloat16), c1.shs.to(torch.bfloat16)
+    r, _ = _raster(c1)
+    r.fit_capacity(sh016, shs16, 3)
+    r.prepare(sh016, shs16, 3)
+    color, T = r.render(geos16)
+    cols = r.split_color(color)
+    sc = c1.scene
+    g64 = geos16.float().cpu().numpy()
+    for k in range(3):
+        cam = sc.cameras[k]
+        rgbs = O.sh_fwd(3, np.arange(sc.n_voxels), sc.centers, cam.position, sh016.float().cpu().numpy(),
+                        shs16.float().cpu().numpy(), mode="f64")
+        o = O.render_view(cam, sc.octpath, sc.centers, sc.lengths, g64, rgbs.astype(np.float32), mode="f64")
+        tgt = np.random.default_rng(k).uniform(0, 1, size=o["color"].shape)
+        ours = cols[k].cpu().numpy()
+        assert abs(_psnr(ours, tgt) - _psnr(o["color"], tgt)) < 0.01
+        assert np.abs(ours - o["color"]).max() < 1e-4
+
+
+def test_graph_replay_equals_eager(c1):
+    from sv_raster_b200.workload import BatchedWorkload
+    sc = synthetic.config_scene("c1")
+    sc.targets = [np.random.default_rng(1).uniform(0, 1, (3, c.height, c.width)).astype(np.float32)
+                  for c in sc.cameras]
+    wl = BatchedWorkload(sc, torch.device("cuda"), storage=torch.float32)
+    wl._eager_step(False)
+    torch.cuda.synchronize()
+    c_eager, dgeo_eager = wl.color.clone(), wl.grads[0].clone()
+    wl.capture()
+    wl.graph.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(wl.color, c_eager)
+    assert rel_err(wl.grads[0], dgeo_eager) < 1e-6
+    # moving a camera in place is picked up by the replay
+    wl.cams[0].c2w[0, 3] += 0.01
+    wl.cams[0].w2c.copy_(torch.linalg.inv(wl.cams[0].c2w))
+    wl.graph.replay()
+    torch.cuda.synchronize()
+    assert not torch.equal(wl.color, c_eager)
+    assert wl.check_errors() > 0
+
+
+def test_capacity_overflow_is_reported(c1):
+    r, _ = _raster(c1, capacity=1000)
+    r.prepare(c1.sh0, c1.shs, 3)
+    r.render(c1.geos)
+    torch.cuda.synchronize()
+    total, err = r.header()
+    assert total > 1000
+    assert err & 0x4
+
+
+def test_level_bound_is_checked(c1):
+    r, _ = _raster(c1, max_level=5)  # the c1 voxels are at levels 6-8
+    r.fit_capacity(c1.sh0, c1.shs, 3)
+    r.prepare(c1.sh0, c1.shs, 3)
+    torch.cuda.synchronize()
+    assert r.header()[1] & 0x10

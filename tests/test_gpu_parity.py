@@ -220,11 +220,10 @@ def test_empty_scene_and_empty_view(c1):
                                        torch.zeros(0, 1, dtype=torch.int64, device="cuda"), e3,
                                        torch.zeros(0, 1, device="cuda"))
     assert nd.numel() == 0
-    # camera looking away from the scene
-    w2c_away = w2c.clone()
-    w2c_away[2, :3] *= -1
-    w2c_away[0, :3] *= -1
-    c2w_away = torch.linalg.inv(w2c_away)
+    # camera outside the scene looking away from it
+    away = synthetic.make_camera(64, 48, 50.0, (0.0, 0.0, -1.5), target=(0.0, 0.0, -3.0))
+    w2c_away = torch.from_numpy(away.w2c).cuda()
+    c2w_away = torch.from_numpy(away.c2w).cuda()
     rg = torch.rand(c1.centers.shape[0], 3, device="cuda")
     nd, geom = mC.rasterize_preprocess(64, 48, cam.tanfovx, cam.tanfovy, 32, 24, w2c_away, c2w_away, 0.02,
                                        c1.octpath, c1.centers, c1.lengths)
