@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--voxels", type=int, default=None, help="override the voxel count (smaller profiles)")
     ap.add_argument("--views", type=int, default=None, help="use only the first N views")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg (profiling runs)")
     return ap.parse_args()
 
 
@@ -192,6 +193,21 @@ def main():
     value = ms_total / (args.steps * views_all)  # device ms per view over the whole job
     kstats = wl.kernel_stats()
 
+    graph_ms = None
+    if args.mode == "batched":
+        # the same step replayed from a captured CUDA graph (no per-kernel events)
+        wl.timers = {}
+        wl.step()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(args.steps):
+            wl.step()
+        g1.record(stream)
+        torch.cuda.synchronize()
+        wl.check_errors()
+        graph_ms = g0.elapsed_time(g1) / args.steps
+
     # end to end through the public API with host buffers
     e2e = None
     if not args.no_e2e:
@@ -202,7 +218,7 @@ def main():
             e2e["ms_total"] = float(t.item())
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(sc, budget_s=15.0)
 
     if rank == 0:
@@ -222,6 +238,7 @@ def main():
             "rays_per_s": round(sum(c.width * c.height for c in sc.cameras) * world / (ms_total / args.steps * 1e-3),
                                 1),
             "gpu_launches": wl.launches_per_step() * args.steps,
+            "graph_ms_per_step": round(graph_ms, 4) if graph_ms else None,
             "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": round(achieved, 2),
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "peak_kind": peak_kind, "traffic": dom.get("traffic"),

@@ -88,6 +88,19 @@ __device__ __forceinline__ float density_act_grad(float x) {
   return (x > 1.1f) ? 1.0f : 0.909090909091f * expf(0.909090909091f * x - 0.904689820196f);
 }
 
+// Both at once from a single expf: the same exponential the two functions
+// above evaluate separately, so the values are identical.
+__device__ __forceinline__ void density_act_and_grad(float x, float& act, float& grad) {
+  if (x > 1.1f) {
+    act = x;
+    grad = 1.0f;
+  } else {
+    const float e = expf(0.909090909091f * x - 0.904689820196f);
+    act = e;
+    grad = 0.909090909091f * e;
+  }
+}
+
 __device__ __forceinline__ float contract_depth(float x) {  // auxiliary.h:235-238
   return (x < 1.f) ? x : 2.f - 1.f / x;
 }
@@ -126,7 +139,11 @@ __device__ __forceinline__ PixelRay make_pixel_ray(float pixx, float pixy, int W
   const float cdx = (pixx + 0.5f - cx) * 2.f * tanfovx / (float)W;
   const float cdy = (pixy + 0.5f - cy) * 2.f * tanfovy / (float)H;
   const float cdz = 1.f;
-  const float rd_norm = sqrtf(cdx * cdx + cdy * cdy + cdz * cdz);
+  // |rd|^2 with the y term fused onto the x product: the reference build
+  // evaluates its dot() in this order, and leaving the contraction to the
+  // compiler here picks the other operand (measured: images then differ
+  // from the reference's in a few ulp at some pixels).
+  const float rd_norm = sqrtf(__fmaf_rn(cdy, cdy, __fmul_rn(cdx, cdx)) + cdz * cdz);
   const float rx = c2w[0] * cdx + c2w[1] * cdy + c2w[2] * cdz;
   const float ry = c2w[4] * cdx + c2w[5] * cdy + c2w[6] * cdz;
   const float rz = c2w[8] * cdx + c2w[9] * cdy + c2w[10] * cdz;

@@ -20,6 +20,10 @@ namespace svr {
 
 constexpr int kBatch = 256;              // records staged per round (one per thread)
 constexpr int kGroups = kBatch / 32;     // 32-record ballot groups per round
+// Resident CTAs per SM the compositing kernels are register-bounded for
+// (occupancy vs spills, chosen from -Xptxas -v and ncu measurements).
+constexpr int kFwdMinBlocks = 5;
+constexpr int kBwdMinBlocks = 3;
 
 // Voxel attributes of one view as the kernels read them.
 struct VoxelArrays {
@@ -31,20 +35,33 @@ struct VoxelArrays {
   const float* rgbs;          // [P,3] (this view)
 };
 
+// One staged record.  Besides the raw attributes it holds the per-record
+// terms of the slab test and of the sample position, computed once here
+// instead of once per pixel: (c - o) -/+ l/2, c - l/2 and 1/l.  Each is the
+// same IEEE operation on the same operands as in the per-pixel form, so the
+// per-pixel results are unchanged bit for bit.
 struct StageSmem {
   uint2 bbox[kBatch];
-  float4 cl[kBatch];          // centre xyz, edge length
-  float4 geo[kBatch][2];      // 8 corner densities
-  float4 rgbv[kBatch];        // rgb, voxel id (as int bits)
   uint32_t val[kBatch];       // sorted value (quadrant << 29 | voxel id)
+  float4 slab_lo[kBatch];     // (c - o) - l/2 (xyz), 1/l (w)
+  float4 slab_hi[kBatch];     // (c - o) + l/2 (xyz), l (w)
+  float4 corner[kBatch];      // c - l/2 (xyz), voxel id as int bits (w)
+  float4 geo[kBatch][2];      // 8 corner densities
+  float4 rgb[kBatch];         // rgb (xyz)
 };
 
-__device__ __forceinline__ void stage_record(StageSmem& s, int slot, uint32_t val, const VoxelArrays& va) {
+__device__ __forceinline__ void stage_record(StageSmem& s, int slot, uint32_t val, const VoxelArrays& va,
+                                             float ox, float oy, float oz) {
   const uint32_t vid = val_vox_id(val);
   s.val[slot] = val;
   s.bbox[slot] = va.bboxes[vid];
   const float* c = va.centers + 3 * (size_t)vid;
-  s.cl[slot] = make_float4(c[0], c[1], c[2], va.lengths[vid]);
+  const float cx = c[0], cy = c[1], cz = c[2], len = va.lengths[vid];
+  const float rad = 0.5f * len;
+  const float dx = cx - ox, dy = cy - oy, dz = cz - oz;
+  s.slab_lo[slot] = make_float4(dx - rad, dy - rad, dz - rad, 1.f / len);
+  s.slab_hi[slot] = make_float4(dx + rad, dy + rad, dz + rad, len);
+  s.corner[slot] = make_float4(cx - 0.5f * len, cy - 0.5f * len, cz - 0.5f * len, __int_as_float((int)vid));
   if (va.geos_bf16) {
     const uint4 raw = *reinterpret_cast<const uint4*>(va.geos_bf16 + 8 * (size_t)vid);
     const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&raw);
@@ -58,7 +75,16 @@ __device__ __forceinline__ void stage_record(StageSmem& s, int slot, uint32_t va
     s.geo[slot][1] = g[1];
   }
   const float* rgb = va.rgbs + 3 * (size_t)vid;
-  s.rgbv[slot] = make_float4(rgb[0], rgb[1], rgb[2], __int_as_float((int)vid));
+  s.rgb[slot] = make_float4(rgb[0], rgb[1], rgb[2], 0.f);
+}
+
+// Slab test from the staged per-record terms (auxiliary.h:240-253).
+__device__ __forceinline__ float2 staged_ray_box(const float4& lo, const float4& hi, const PixelRay& r) {
+  const float ax = lo.x * r.ix, ay = lo.y * r.iy, az = lo.z * r.iz;
+  const float bx = hi.x * r.ix, by = hi.y * r.iy, bz = hi.z * r.iz;
+  const float nx = fminf(ax, bx), ny = fminf(ay, by), nz = fminf(az, bz);
+  const float fx = fmaxf(ax, bx), fy = fmaxf(ay, by), fz = fmaxf(az, bz);
+  return make_float2(fmaxf(fmaxf(nx, ny), nz), fminf(fminf(fx, fy), fz));
 }
 
 // Does staged record `slot` possibly touch a pixel of this warp's 8x4

@@ -22,7 +22,7 @@ struct BwdSmem {
 };
 
 template <int NS, bool DEPTH, bool DIST, bool NORMAL>
-__global__ void __launch_bounds__(kBatch)
+__global__ void __launch_bounds__(kBatch, kBwdMinBlocks)
 render_bwd_kernel(const __grid_constant__ BwdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BwdSmem& sm = *reinterpret_cast<BwdSmem*>(smem_raw);
@@ -48,7 +48,7 @@ struct BwdBatchArgs {
 };
 
 template <int NS, bool DEPTH, bool DIST, bool NORMAL>
-__global__ void __launch_bounds__(kBatch)
+__global__ void __launch_bounds__(kBatch, kBwdMinBlocks)
 render_bwd_batch_kernel(const __grid_constant__ BwdBatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BwdSmem& sm = *reinterpret_cast<BwdSmem*>(smem_raw);

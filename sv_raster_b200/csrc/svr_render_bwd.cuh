@@ -43,6 +43,52 @@ __device__ __forceinline__ float warp_sum(float x) {
   return x;
 }
 
+// Reduce-scatter of 12 per-lane values over the warp in 13 shuffles (the
+// values are padded to 16 slots): after five halving steps lane l holds in
+// v[0] the warp total of slot (l >> 1) & 15; returns that slot for the even
+// lane that should publish it (-1 otherwise or for a padding slot).
+__device__ __forceinline__ int warp_reduce_scatter12(float v[12], int lane) {
+  float a[8];
+  // step 1 (xor 16): keep slots 0-7 (lanes 0-15) or 8-15 (lanes 16-31)
+  const bool hi16 = lane & 16;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const float lo_v = v[k];
+    const float hi_v = (k + 8 < 12) ? v[k + 8] : 0.f;
+    const float send = hi16 ? lo_v : hi_v;
+    const float keep = hi16 ? hi_v : lo_v;
+    a[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+  // step 2 (xor 8): keep 4 of 8
+  float b[4];
+  const bool hi8 = lane & 8;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float send = hi8 ? a[k] : a[k + 4];
+    const float keep = hi8 ? a[k + 4] : a[k];
+    b[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  // step 3 (xor 4): keep 2 of 4
+  float c2[2];
+  const bool hi4 = lane & 4;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float send = hi4 ? b[k] : b[k + 2];
+    const float keep = hi4 ? b[k + 2] : b[k];
+    c2[k] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  // step 4 (xor 2): keep 1 of 2
+  const bool hi2 = lane & 2;
+  const float send = hi2 ? c2[0] : c2[1];
+  const float keep = hi2 ? c2[1] : c2[0];
+  float d = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  // step 5 (xor 1): full sum on both lanes of the pair
+  d += __shfl_xor_sync(0xffffffffu, d, 1);
+  v[0] = d;
+  const int slot = (hi16 ? 8 : 0) + (hi8 ? 4 : 0) + (hi4 ? 2 : 0) + (hi2 ? 1 : 0);
+  return ((lane & 1) == 0 && slot < 12) ? slot : -1;
+}
+
 template <int NS, bool DEPTH, bool DIST, bool NORMAL>
 __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const float* __restrict__ c2w_s, int tile_x,
                                                 int tile_y, uint2 range_raw, uint32_t tile_last,
@@ -114,7 +160,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
     __syncthreads();
     const int base = r * kBatch;                     // records [base, base+n_here) from the back
     const int n_here = min(kBatch, todo_total - base);
-    if (tid < n_here) stage_record(s, tid, vals[range.y - base - tid - 1], va);
+    if (tid < n_here) stage_record(s, tid, vals[range.y - base - tid - 1], va, ray.ox, ray.oy, ray.oz);
     __syncthreads();
 
     // Position (relative to range.x) of staged slot j is todo_total - base - j - 1.
@@ -132,8 +178,8 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
         if (inside && jpos < last_contrib) {
           const uint32_t val = s.val[j];
           if (pixel_in_bbox(px, py, s.bbox[j]) && ray.quad == val_quadrant(val)) {
-            const float4 cl = s.cl[j];
-            const float2 ab = ray_box(cl.x, cl.y, cl.z, cl.w, ray);
+            const float4 slo = s.slab_lo[j], shi = s.slab_hi[j];
+            const float2 ab = staged_ray_box(slo, shi, ray);
             const float a = ab.x, b = ab.y;
             if (!(a > b)) {
               float geo[8];
@@ -148,14 +194,15 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
               float each_dI[NS][8];
               float w[8];
               float local_alpha[NS];
-              const float vox_l_inv = 1.f / cl.w;
+              const float vox_l_inv = slo.w;
+              const float4 cr = s.corner[j];
               const float step_sz = (b - a) * (1.f / NS);
               const float stx = step_sz * ray.dx, sty = step_sz * ray.dy, stz = step_sz * ray.dz;
               const float t0 = a + 0.5f * step_sz;
               const float ptx = ray.ox + t0 * ray.dx, pty = ray.oy + t0 * ray.dy, ptz = ray.oz + t0 * ray.dz;
-              float qx = (ptx - (cl.x - 0.5f * cl.w)) * vox_l_inv;
-              float qy = (pty - (cl.y - 0.5f * cl.w)) * vox_l_inv;
-              float qz = (ptz - (cl.z - 0.5f * cl.w)) * vox_l_inv;
+              float qx = (ptx - cr.x) * vox_l_inv;
+              float qy = (pty - cr.y) * vox_l_inv;
+              float qz = (ptz - cr.z) * vox_l_inv;
               const float qsx = stx * vox_l_inv, qsy = sty * vox_l_inv, qsz = stz * vox_l_inv;
 #pragma unroll
               for (int k = 0; k < NS; ++k) {
@@ -163,10 +210,12 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
                 float d = 0.f;
 #pragma unroll
                 for (int c = 0; c < 8; ++c) d += geo[c] * w[c];
-                const float lvi = kStepScale * step_sz * density_act(d);
+                float act, act_grad;
+                density_act_and_grad(d, act, act_grad);
+                const float lvi = kStepScale * step_sz * act;
                 vol_int += lvi;
                 if (DEPTH && NS > 1) local_alpha[k] = fminf(kMaxAlpha, 1.f - expf(-lvi));
-                const float dd_dd = kStepScale * step_sz * density_act_grad(d);
+                const float dd_dd = kStepScale * step_sz * act_grad;
 #pragma unroll
                 for (int c = 0; c < 8; ++c) {
                   const float tmp = dd_dd * w[c];
@@ -181,7 +230,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
                 contrib = true;
                 T = T / (1.f - alpha);
                 const float pt_w = alpha * T;
-                const float4 rgbv = s.rgbv[j];
+                const float4 rgbv = s.rgb[j];
                 float dL_dpt_w = gx * rgbv.x + gy * rgbv.y + gz * rgbv.z;
                 if (DIST) {
                   const float adist = contract_depth(a), bdist = contract_depth(b);
@@ -259,7 +308,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
                   }
                 }
                 if (in.lambda_ascending > 0) {
-                  const float lo_x = cl.x - 0.5f * cl.w, lo_y = cl.y - 0.5f * cl.w, lo_z = cl.z - 0.5f * cl.w;
+                  const float lo_x = cr.x, lo_y = cr.y, lo_z = cr.z;
                   const float pax = ray.ox + a * ray.dx, pay = ray.oy + a * ray.dy, paz = ray.oz + a * ray.dz;
                   const float pbx = ray.ox + b * ray.dx, pby = ray.oy + b * ray.dy, pbz = ray.oz + b * ray.dz;
                   float wa[8], wb[8];
@@ -291,20 +340,21 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
           }
         }
         // Warp reduction of this record's gradients into its shared accumulator.
-        const uint32_t act = __ballot_sync(0xffffffffu, contrib);
-        if (act == 0u) continue;
+        const uint32_t act_mask = __ballot_sync(0xffffffffu, contrib);
+        if (act_mask == 0u) continue;
         float* acc = s_grad + j * kGradStride;
-        if (__popc(act) == 1) {
+        if (__popc(act_mask) == 1) {
           if (contrib) {
 #pragma unroll
             for (int c = 0; c < 12; ++c) atomicAdd(acc + c, gp[c]);
           }
         } else {
+          if (!contrib) {
 #pragma unroll
-          for (int c = 0; c < 12; ++c) {
-            const float v = warp_sum(contrib ? gp[c] : 0.f);
-            if (lane == c) atomicAdd(acc + c, v);
+            for (int c = 0; c < 12; ++c) gp[c] = 0.f;
           }
+          const int slot = warp_reduce_scatter12(gp, lane);
+          if (slot >= 0) atomicAdd(acc + slot, gp[0]);
         }
       }
     }

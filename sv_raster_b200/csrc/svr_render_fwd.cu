@@ -15,7 +15,7 @@ struct FwdArgs {
 };
 
 template <int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
-__global__ void __launch_bounds__(kBatch)
+__global__ void __launch_bounds__(kBatch, kFwdMinBlocks)
 render_fwd_kernel(const __grid_constant__ FwdArgs a) {
   __shared__ StageSmem s;
   __shared__ float s_c2w[12];
@@ -41,7 +41,7 @@ struct FwdBatchArgs {
 };
 
 template <int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
-__global__ void __launch_bounds__(kBatch)
+__global__ void __launch_bounds__(kBatch, kFwdMinBlocks)
 render_fwd_batch_kernel(const __grid_constant__ FwdBatchArgs a) {
   __shared__ StageSmem s;
   __shared__ float s_c2w[12];

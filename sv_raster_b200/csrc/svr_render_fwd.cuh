@@ -58,7 +58,7 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
     if (__syncthreads_count(done) == kBatch) break;
     const int base = r * kBatch;
     const int n_here = min(kBatch, todo_total - base);
-    if (tid < n_here) stage_record(s, tid, vals[range.x + base + tid], va);
+    if (tid < n_here) stage_record(s, tid, vals[range.x + base + tid], va, ray.ox, ray.oy, ray.oz);
     __syncthreads();
 
     const uint32_t quad_mask = __reduce_or_sync(0xffffffffu, done ? 0u : (1u << ray.quad));
@@ -73,8 +73,8 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
         if (done) continue;
         const uint32_t val = s.val[j];
         if (!pixel_in_bbox(px, py, s.bbox[j]) || ray.quad != val_quadrant(val)) continue;
-        const float4 cl = s.cl[j];
-        const float2 ab = ray_box(cl.x, cl.y, cl.z, cl.w, ray);
+        const float4 slo = s.slab_lo[j], shi = s.slab_hi[j];
+        const float2 ab = staged_ray_box(slo, shi, ray);
         const float a = ab.x, b = ab.y;
         if (a > b) continue;
 
@@ -83,14 +83,15 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
         float vol_int = 0.f;
         float w[8];
         float local_alpha[NS];
-        const float vox_l_inv = 1.f / cl.w;
+        const float vox_l_inv = slo.w;
+        const float4 cr = s.corner[j];
         const float step_sz = (b - a) * (1.f / NS);
         const float stx = step_sz * ray.dx, sty = step_sz * ray.dy, stz = step_sz * ray.dz;
         const float t0 = a + 0.5f * step_sz;
         const float ptx = ray.ox + t0 * ray.dx, pty = ray.oy + t0 * ray.dy, ptz = ray.oz + t0 * ray.dz;
-        float qx = (ptx - (cl.x - 0.5f * cl.w)) * vox_l_inv;
-        float qy = (pty - (cl.y - 0.5f * cl.w)) * vox_l_inv;
-        float qz = (ptz - (cl.z - 0.5f * cl.w)) * vox_l_inv;
+        float qx = (ptx - cr.x) * vox_l_inv;
+        float qy = (pty - cr.y) * vox_l_inv;
+        float qz = (ptz - cr.z) * vox_l_inv;
         const float qsx = stx * vox_l_inv, qsy = sty * vox_l_inv, qsz = stz * vox_l_inv;
 #pragma unroll
         for (int k = 0; k < NS; ++k) {
@@ -107,7 +108,8 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
         if (alpha < kMinAlpha) continue;
 
         const float pt_w = T * alpha;
-        const float4 rgbv = s.rgbv[j];
+        const float4 rgbv = s.rgb[j];
+        const int vid = __float_as_int(cr.w);
         Cx = Cx + pt_w * rgbv.x;
         Cy = Cy + pt_w * rgbv.y;
         Cz = Cz + pt_w * rgbv.z;
@@ -128,7 +130,7 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
           }
           D = D + T * dval;
           if (T > 0.5f) {
-            dmed_vid = __float_as_int(rgbv.w);
+            dmed_vid = vid;
             dmed_T = T;
           }
         }
@@ -144,7 +146,7 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
         T *= (1.f - alpha);
         done |= (T < kEarlyStopT);
         last_contrib = (uint32_t)(base + j + 1);
-        if (MAXW) atomicMax(reinterpret_cast<int*>(out.max_w) + __float_as_int(rgbv.w), __float_as_int(pt_w));
+        if (MAXW) atomicMax(reinterpret_cast<int*>(out.max_w) + vid, __float_as_int(pt_w));
       }
     }
   }

@@ -52,7 +52,7 @@ def _raster(C, max_level=None, views=(0, 1, 2), **kw):
     return r, cams
 
 
-@pytest.mark.parametrize("max_key_bits", [None, 38])
+@pytest.mark.parametrize("max_key_bits", [None, 35])
 def test_batched_forward_equals_plain(c1, max_key_bits, monkeypatch):
     if max_key_bits:
         monkeypatch.setenv("SVR_MAX_KEY_BITS", str(max_key_bits))  # forces one sort group per view
