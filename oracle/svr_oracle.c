@@ -246,8 +246,9 @@ static REAL quadrature(const Ray* r, REAL cx, REAL cy, REAL cz, REAL l, REAL a, 
     tri_w(qx, qy, qz, w);
     REAL d = g[0] * w[0];
     for (int c = 1; c < 8; ++c) d = MAD(g[c], w[c], d);
-    const REAL lvi = STEP_SCALE * step * act(d);
-    vol += lvi;
+    const REAL a_ = act(d);
+    const REAL lvi = STEP_SCALE * step * a_;
+    vol = MAD(STEP_SCALE * step, a_, vol); /* nvcc fuses the sum into the product */
     if (lalpha) lalpha[k] = rmin(MAX_ALPHA, 1 - EXP(-lvi));
     if (dI) {
       const REAL dd = STEP_SCALE * step * act_grad(d);
@@ -533,7 +534,8 @@ void SFX(orc_sh_fwd)(int deg, int n, const int64_t* idx, int M, const float* cen
   const int nb = (deg + 1) * (deg + 1);
   for (int t = 0; t < n; ++t) {
     const int64_t i = idx[t];
-    REAL x = centers[3 * i] - campos[0], y = centers[3 * i + 1] - campos[1], z = centers[3 * i + 2] - campos[2];
+    REAL x = (REAL)centers[3 * i] - (REAL)campos[0], y = (REAL)centers[3 * i + 1] - (REAL)campos[1],
+         z = (REAL)centers[3 * i + 2] - (REAL)campos[2];
     const REAL rn = 1 / SQRT(x * x + y * y + z * z);
     x *= rn; y *= rn; z *= rn;
     REAL bs[16];
@@ -552,7 +554,8 @@ void SFX(orc_sh_bwd)(int deg, int n, const int64_t* idx, int M, const float* cen
   const int nb = (deg + 1) * (deg + 1);
   for (int t = 0; t < n; ++t) {
     const int64_t i = idx[t];
-    REAL x = centers[3 * i] - campos[0], y = centers[3 * i + 1] - campos[1], z = centers[3 * i + 2] - campos[2];
+    REAL x = (REAL)centers[3 * i] - (REAL)campos[0], y = (REAL)centers[3 * i + 1] - (REAL)campos[1],
+         z = (REAL)centers[3 * i + 2] - (REAL)campos[2];
     const REAL rn = 1 / SQRT(x * x + y * y + z * z);
     x *= rn; y *= rn; z *= rn;
     REAL bs[16];

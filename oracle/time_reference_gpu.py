@@ -1,0 +1,90 @@
+"""Time the reference CUDA backend (oracle/_ref) on the same GPU -- the GPU
+comparator for the benchmark.  TEST / MEASUREMENT INFRASTRUCTURE ONLY.
+
+Per view it runs the reference's own call sequence (renderer.py:66-127 and
+sparse_voxel_gears/renderer.py:35-94): rasterize_preprocess, the visible-index
+host sync, sh_compute, rasterize_voxels (which reads the instance count back),
+an L2-loss gradient, rasterize_voxels_backward and sh_compute_bw.  Prints one
+JSON line with ms/view (CUDA events around all views of a step, fp32).
+
+Usage: python oracle/time_reference_gpu.py [--config c4] [--steps 3] [--warmup 1]
+"""
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config", default="c4")
+    ap.add_argument("--voxels", type=int, default=None)
+    ap.add_argument("--views", type=int, default=None)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=1)
+    a = ap.parse_args()
+    import build_ref
+    from sv_raster_b200 import synthetic
+    ref = build_ref.load()
+    cache = f"/tmp/svr_scene_{a.config}_{a.voxels or 0}.pkl"
+    if os.path.exists(cache):
+        import pickle
+        sc = pickle.load(open(cache, "rb"))
+    else:
+        sc = synthetic.config_scene(a.config, n_voxels=a.voxels)
+    cams = sc.cameras[: a.views] if a.views else sc.cameras
+    dev = "cuda"
+    t = lambda x, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(x)).to(dev, dt)
+    octpath, centers, lengths = t(sc.octpath.reshape(-1, 1), torch.int64), t(sc.centers), t(sc.lengths)
+    geos, sh0, shs = t(sc.geos), t(sc.sh0), t(sc.shs)
+    mats = [(c, t(c.w2c), t(c.c2w)) for c in cams]
+    rng = np.random.default_rng(0)
+    targets = [t(rng.uniform(0, 1, (3, c.height, c.width)).astype(np.float32)) for c in cams]
+    e = torch.empty(0, device=dev)
+
+    def view(i):
+        cam, w2c, c2w = mats[i]
+        W, H = cam.width, cam.height
+        ndup, geom = ref.rasterize_preprocess(W, H, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w, cam.near,
+                                              octpath, centers, lengths, False)
+        vis = torch.where(ndup > 0)[0]
+        pos = c2w[:3, 3].contiguous()
+        rgbs = ref.sh_compute(3, vis, centers, pos, sh0, shs)
+        out = ref.rasterize_voxels(1, W, H, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w, 0.0, False, False,
+                                   False, False, octpath, centers, lengths, geos, rgbs, geom, False)
+        color, T = out[3], out[6]
+        dC = (2.0 / color.numel()) * (color - targets[i])
+        g = ref.rasterize_voxels_backward(out[0], 1, W, H, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w, 0.0,
+                                          octpath, centers, lengths, geos, rgbs, geom, out[1], out[2], T, dC, e, e,
+                                          torch.zeros_like(T), 0.0, e, 0.0, 0.0, False, False, out[4], out[5], False)
+        ref.sh_compute_bw(3, 16, vis, centers, pos, rgbs, g[1])
+        return out[0]
+
+    for _ in range(a.warmup):
+        for i in range(len(mats)):
+            view(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    inst = 0
+    for _ in range(a.steps):
+        for i in range(len(mats)):
+            inst += view(i)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / (a.steps * len(mats))
+    print(json.dumps({"impl": "reference-cuda-backend", "config": a.config, "voxels": sc.n_voxels,
+                      "views": len(mats), "size": [cams[0].width, cams[0].height], "ms_per_view": round(ms, 3),
+                      "instances_per_view": inst // (a.steps * len(mats)), "dtype": "f32",
+                      "device": torch.cuda.get_device_name()}))
+
+
+if __name__ == "__main__":
+    main()
