@@ -67,6 +67,21 @@ int svr_rasterize_preprocess(const svr_camera* cam, int64_t P, const int64_t* oc
                              const float* vox_centers, const float* vox_lengths, int32_t* out_n_duplicates,
                              void* geom_buffer, size_t geom_bytes, int debug, void* stream);
 
+/* svr_rasterize_preprocess without any caller-provided scratch.  No
+ * counterpart in the reference.  For callers that cannot allocate device
+ * memory (an embedding host that owns every device buffer, code inside CUDA
+ * graph capture, real-time loops): the scan's partial sums live in a static
+ * device array of the library, so P is limited to svr_noalloc_max_voxels()
+ * (67,108,864); larger P returns SVR_ERR_CAPACITY.  Same arguments and
+ * outputs as svr_rasterize_preprocess; the geom buffer is still the caller's
+ * output.  The first call on a device looks up the array's device address
+ * (make it before any stream capture).  All calls share the array: calls that
+ * overlap on the GPU race.  The function allocates nothing. */
+int svr_rasterize_preprocess_noalloc(const svr_camera* cam, int64_t P, const int64_t* octree_paths,
+                                     const float* vox_centers, const float* vox_lengths, int32_t* out_n_duplicates,
+                                     void* geom_buffer, size_t geom_bytes, int debug, void* stream);
+int64_t svr_noalloc_max_voxels(void);
+
 /* Device address of the uint32 instance count ("num_rendered", read back by
  * the reference at forward.cu:652-658) inside a geom buffer. */
 const uint32_t* svr_geom_count_ptr(const void* geom_buffer);

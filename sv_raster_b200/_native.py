@@ -39,6 +39,9 @@ _SIGS = {
     "svr_image_buffer_bytes": (c_sz, [c_int, c_int]),
     "svr_binning_buffer_bytes": (c_sz, [c_i64, c_int, c_int]),
     "svr_rasterize_preprocess": (c_int, [ctypes.POINTER(Camera), c_i64, c_p, c_p, c_p, c_p, c_p, c_sz, c_int, c_p]),
+    "svr_rasterize_preprocess_noalloc": (c_int, [ctypes.POINTER(Camera), c_i64, c_p, c_p, c_p, c_p, c_p, c_sz, c_int,
+                                                 c_p]),
+    "svr_noalloc_max_voxels": (c_i64, []),
     "svr_geom_count_ptr": (c_p, [c_p]),
     "svr_geom_error_ptr": (c_p, [c_p]),
     "svr_rasterize_forward": (c_int, [ctypes.POINTER(Camera), c_int, c_int, c_int, c_int, c_int, c_i64, c_i64,

@@ -2,6 +2,7 @@
 // of the plain (one view per call) path.  See include/svr_b200.h.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/svr_b200.h"
 #include "svr_common.cuh"
@@ -477,3 +478,81 @@ int svr_read_error(uint32_t* device_word, uint32_t* host_value, void* stream_) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Scratch-free variant of svr_rasterize_preprocess.
+//
+// For callers that cannot allocate device memory at all (a renderer embedded
+// in a host application whose allocator owns every device buffer, code running
+// inside a CUDA-graph capture, or a real-time loop that forbids cudaMalloc).
+// The only scratch of the projection + scan sequence -- the per-CTA partial
+// sums of the scan -- lives in the file-scope device array below instead of
+// in the caller's geom buffer.  It bounds P to kNoAllocMaxVoxels.
+//
+// The array is a host-side stand-in in host code, not a device address: its
+// device address is taken with cudaGetSymbolAddress once per device, on the
+// first call made with that device current (so that first call should come
+// before any stream capture).  Every call shares the array: calls that
+// overlap on the GPU (two streams, or two threads) race on it.  Nothing in it
+// needs clearing between calls: each call writes every partial sum it later
+// reads.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kNoAllocScanTile = 4096;                 // items per scan CTA (svr_binning.cu)
+constexpr int64_t kNoAllocMaxBlocks = 16384;               // 128 KB of partial sums
+constexpr int64_t kNoAllocMaxVoxels = kNoAllocScanTile * kNoAllocMaxBlocks;  // 67,108,864
+
+__device__ __align__(256) unsigned long long g_noalloc_scan_partials[kNoAllocMaxBlocks + 32];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::once_flag g_noalloc_once[kNoAllocMaxDevices];
+void* g_noalloc_ptr[kNoAllocMaxDevices];
+cudaError_t g_noalloc_status[kNoAllocMaxDevices];
+
+// Device address of the partial-sum array on the current device.
+void* noalloc_scratch(int& status) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    status = SVR_ERR_CUDA;
+    return nullptr;
+  }
+  std::call_once(g_noalloc_once[dev], [dev] {
+    void* ptr = nullptr;
+    g_noalloc_status[dev] = cudaGetSymbolAddress(&ptr, g_noalloc_scan_partials);
+    g_noalloc_ptr[dev] = ptr;
+  });
+  if (g_noalloc_status[dev] != cudaSuccess || !g_noalloc_ptr[dev]) {
+    status = SVR_ERR_CUDA;
+    return nullptr;
+  }
+  status = SVR_OK;
+  return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+
+extern "C" int svr_rasterize_preprocess_noalloc(const svr_camera* cam, int64_t P, const int64_t* octree_paths,
+                                                const float* vox_centers, const float* vox_lengths,
+                                                int32_t* out_n_duplicates, void* geom_buffer, size_t geom_bytes,
+                                                int debug, void* stream_) {
+  (void)octree_paths;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (P < 0 || P >= (1ll << kVoxIdBits) || !valid_camera(cam)) return SVR_ERR_SHAPE;
+  if (P > kNoAllocMaxVoxels) return SVR_ERR_CAPACITY;
+  if (P == 0) return SVR_OK;
+  GeomLayout g = geom_layout(geom_buffer, P);
+  if (!geom_buffer || geom_bytes < g.bytes || !vox_centers || !vox_lengths || !out_n_duplicates) return SVR_ERR_SHAPE;
+  int st = SVR_OK;
+  void* partials = noalloc_scratch(st);
+  if (st != SVR_OK) return st;
+  ViewTable vt;
+  vt.n = 1;
+  vt.v[0] = make_view(*cam);
+  cudaMemsetAsync(g.header, 0, 16 * sizeof(uint32_t), stream);
+  launch_preprocess(vt, (int)P, vox_centers, vox_lengths, out_n_duplicates, g.ndup, g.bbox, g.quad, stream);
+  launch_scan_inclusive(g.ndup, g.scan, (size_t)P, partials, g.header, 0xffffffffull, g.header + 1, stream);
+  return check_launch(debug, stream);
+}
+
+extern "C" int64_t svr_noalloc_max_voxels(void) { return kNoAllocMaxVoxels; }
