@@ -175,6 +175,15 @@ int svr_gather_grid_params(int dim, int64_t n_care, const int64_t* vox_key, cons
 int svr_gather_grid_params_bw(int dim, int64_t n_care, const int64_t* vox_key, const int64_t* care_idx,
                               const float* dL_dvox, float* dL_dgrid, void* stream);
 
+/* Replaces TV_COMPUTE::total_variation_bw (tv_compute.cu:84-110): adds the
+ * total-variation gradient of grid_pts [M,C] over the N voxels' 8 corners
+ * (vox_key [N,8]) into grid_pts_grad in place.  tv_sparse needs a caller
+ * scratch of N*C bytes; the sparse test uses the gradient as it was before
+ * the call (the reference's reads race with its own updates). */
+int svr_total_variation_bw(const float* grid_pts, const int64_t* vox_key, float weight, const float* vox_size_inv,
+                           int no_tv_s, int tv_sparse, int64_t N, int C, uint8_t* sparse_scratch,
+                           float* grid_pts_grad, void* stream);
+
 /* Read and clear a device error word (synchronises `stream`). */
 int svr_read_error(uint32_t* device_word, uint32_t* host_value, void* stream);
 

@@ -30,9 +30,11 @@
 using namespace svr;
 
 namespace {
-
 constexpr size_t kAlign = 256;
 inline size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+}  // namespace
+
+namespace svr {
 
 struct GroupTable {
   int n;
@@ -186,7 +188,7 @@ inline int bit_width_u64(uint64_t n) {
   return b;
 }
 
-}  // namespace
+}  // namespace svr
 
 // ---------------------------------------------------------------------------
 // plan

@@ -11,7 +11,7 @@
 // launched for a caller-given capacity, so the whole chain can be captured in
 // a CUDA graph without a host round trip.  The sort is a three-kernel-per-pass
 // LSD radix sort (upsweep histogram, per-digit row scan, stable downsweep)
-// with 8-bit digits and 4096-item CTA tiles; ranks within a CTA come from
+// with 8-bit digits and 2048-item CTA tiles; ranks within a CTA come from
 // warp __match_any_sync, which keeps it stable, so it reproduces the order of
 // any other stable sort of the same keys.
 #include "svr_common.cuh"
@@ -224,9 +224,9 @@ void launch_duplicate(const ViewTable& views, int P, const int64_t* octpaths, co
 // --------------------------------------------------------------------------
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortRounds = 16;                       // items per thread
-constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096
-constexpr int kWarpSpan = 32 * kSortRounds;            // 512 items per warp
+constexpr int kSortRounds = 8;                        // items per thread (registers: keep >= 3 CTAs/SM)
+constexpr int kSortTile = kSortThreads * kSortRounds;  // 2048
+constexpr int kWarpSpan = 32 * kSortRounds;            // 256 items per warp
 constexpr int kRadix = 256;
 
 static inline int sort_blocks(size_t cap) { return (int)((cap + kSortTile - 1) / kSortTile); }
@@ -310,7 +310,7 @@ struct DownsweepSmem {
   uint32_t scan_tmp[kSortThreads / 32 + 1];
 };
 
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, 3)
 radix_downsweep_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                        uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                        const uint32_t* __restrict__ d_start, const uint32_t* __restrict__ d_n, uint32_t cap, int shift,

@@ -467,6 +467,18 @@ int svr_gather_grid_params_bw(int dim, int64_t n_care, const int64_t* vox_key, c
   return check_launch(0, stream);
 }
 
+int svr_total_variation_bw(const float* grid_pts, const int64_t* vox_key, float weight, const float* vox_size_inv,
+                           int no_tv_s, int tv_sparse, int64_t N, int C, uint8_t* sparse_scratch,
+                           float* grid_pts_grad, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (N < 0 || C < 1 || (N > 0 && (!grid_pts || !vox_key || !grid_pts_grad || (!no_tv_s && !vox_size_inv))) ||
+      (tv_sparse && N > 0 && !sparse_scratch))
+    return SVR_ERR_SHAPE;
+  launch_total_variation_bw(grid_pts, vox_key, weight, vox_size_inv, no_tv_s != 0, tv_sparse ? sparse_scratch : nullptr,
+                            N, C, grid_pts_grad, stream);
+  return check_launch(0, stream);
+}
+
 int svr_read_error(uint32_t* device_word, uint32_t* host_value, void* stream_) {
   cudaStream_t stream = static_cast<cudaStream_t>(stream_);
   uint32_t v = 0;

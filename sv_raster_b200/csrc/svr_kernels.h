@@ -81,4 +81,8 @@ void launch_gather(int dim, int n_care, const int64_t* vox_key, const int64_t* c
 void launch_gather_bw(int dim, int n_care, const int64_t* vox_key, const int64_t* care_idx, const float* dL_dvox,
                       float* dL_dgrid, cudaStream_t stream);
 
+// svr_tv.cu
+void launch_total_variation_bw(const float* grid, const int64_t* vox_key, float weight, const float* vox_size_inv,
+                               bool no_tv_s, uint8_t* active, int64_t N, int C, float* grad, cudaStream_t stream);
+
 }  // namespace svr

@@ -232,3 +232,45 @@ def test_empty_scene_and_empty_view(c1):
                               False, False, c1.octpath, c1.centers, c1.lengths, c1.geos, rg, geom)
     assert out[0] == 0
     assert torch.all(out[3] == 0.5) and torch.all(out[6] == 1.0)
+
+
+@pytest.mark.parametrize("no_tv_s", [False, True])
+def test_total_variation_matches_reference_dense(ref, no_tv_s):
+    from sv_raster_b200 import grid_loss_bw
+    g = torch.Generator(device="cuda").manual_seed(11)
+    M, N = 4000, 1500
+    key = torch.randint(0, M, (N, 8), device="cuda", generator=g)
+    pts = torch.randn(M, 1, device="cuda", generator=g)
+    sinv = torch.rand(N, device="cuda", generator=g) * 100
+    a = torch.randn(M, 1, device="cuda", generator=g)
+    b = a.clone()
+    grid_loss_bw.total_variation(pts, key, 0.1, sinv, no_tv_s, False, a)
+    ref.total_variation_bw(pts, key, 0.1, sinv, no_tv_s, False, b)
+    assert rel_err(a, b) < 1e-6
+
+
+def test_total_variation_sparse_rule():
+    """Sparse mode touches only voxels with a non-zero corner gradient, judged on
+    the gradient as it was before the call (numpy statement of the rule)."""
+    from sv_raster_b200 import grid_loss_bw
+    rng = np.random.default_rng(12)
+    M, N, C = 3000, 800, 3
+    key = rng.integers(0, M, (N, 8))
+    pts = rng.standard_normal((M, C)).astype(np.float32)
+    grad0 = np.where(rng.uniform(size=(M, C)) < 0.2, rng.standard_normal((M, C)), 0).astype(np.float32)
+    sinv = rng.uniform(1, 50, N).astype(np.float32)
+    want = grad0.astype(np.float64).copy()
+    for n in range(N):
+        for c in range(C):
+            k = key[n]
+            if not np.any(grad0[k, c] != 0):
+                continue
+            v = pts[k, c]
+            w = 0.5 * 0.01 * sinv[n]
+            for i in range(8):
+                s = sum((1 if v[i] > v[i ^ m] else -1) for m in (1, 2, 4))
+                want[k[i], c] += w * s
+    got = torch.from_numpy(grad0).cuda()
+    grid_loss_bw.total_variation(torch.from_numpy(pts).cuda(), torch.from_numpy(key).cuda(), 0.5,
+                                 torch.from_numpy(sinv).cuda(), False, True, got)
+    assert np.abs(got.cpu().numpy() - want).max() < 1e-4
