@@ -225,6 +225,14 @@ def main():
         peak, peak_kind = load_peaks()
         dom = kstats["dominant"]
         achieved = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9 if dom["ms"] > 0 else 0.0
+        # measured DRAM bytes per launch: committed ncu capture of the same
+        # kernel on a smaller case, scaled by instances per launch
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "render_traffic.json")
+        if os.path.exists(tf) and dom["name"] in ("render_fwd", "render_bwd"):
+            t = json.load(open(tf))
+            inst = wl.instances_per_view() * (n_views if args.mode == "batched" else 1)
+            traffic = round(t[dom["name"]]["dram_bytes"] / t["instances_per_launch"] * inst)
         line = {
             "metric": "fwd+bwd ms/view", "value": round(value, 4), "unit": "ms/view", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
@@ -241,7 +249,7 @@ def main():
             "graph_ms_per_step": round(graph_ms, 4) if graph_ms else None,
             "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": round(achieved, 2),
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "peak_kind": peak_kind, "traffic": dom.get("traffic"),
+                         "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": dom["bytes_per_launch"],
                          "ms_per_launch": round(dom["ms_per_launch"], 4)},
             "kernels": kstats["table"],

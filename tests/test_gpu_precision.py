@@ -116,8 +116,9 @@ def test_bf16_storage_precision_c4_window():
     res = {}
     for name, dt in (("fp32", torch.float32), ("bf16", torch.bfloat16)):
         r = BatchedRasterizer([_DevCam(cam)], octpath, centers, lengths, max_level=sc.max_level)
-        geos = geos32.to(dt).requires_grad_(True)
-        sh0, shs = sh032.to(dt).requires_grad_(True), shs32.to(dt).requires_grad_(True)
+        geos = geos32.detach().to(dt).clone().requires_grad_(True)
+        sh0 = sh032.detach().to(dt).clone().requires_grad_(True)
+        shs = shs32.detach().to(dt).clone().requires_grad_(True)
         r.fit_capacity(sh0.detach(), shs.detach(), 3)
         color, T = BatchedRender.apply(r, 3, geos, sh0, shs)
         loss = ((color.view(3, cam.height, cam.width) - t(tgt)) ** 2).mean()
