@@ -126,14 +126,9 @@ def scene_for(args, rank, world):
             os.replace(cache + ".tmp", cache)
         except OSError:
             pass
+    from sv_raster_b200.workload import rank_cameras
     cams = sc.cameras[: args.views] if args.views else sc.cameras
-    if world > 1:
-        # weak scaling: every rank renders its own set of views of the same size
-        extra = synthetic.orbit_cameras(len(cams) * world, 1000 + 7, radius=(1.5, 2.0),
-                                        fixed_size=(cams[0].width, cams[0].height)) if args.config == "c4" else None
-        if extra is not None and rank > 0:
-            cams = extra[rank * len(cams):(rank + 1) * len(cams)]
-    sc.cameras = cams
+    sc.cameras = rank_cameras(cams, rank, world)  # weak scaling: each rank its own views
     trng = np.random.default_rng(1234 + rank)
     sc.targets = [trng.uniform(0, 1, size=(3, c.height, c.width)).astype(np.float32) for c in cams]
     return sc
@@ -182,11 +177,7 @@ def main():
     clocks = sampler.stop()
     if hasattr(wl, "check_errors"):
         wl.check_errors()  # capacity / consistency flags of the batched step
-    ms_total = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms_total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = workload.max_over_ranks(ev0.elapsed_time(ev1), device=dev)
     ms_per_step = ms_total / args.steps
     ms_per_view = ms_per_step / n_views  # per-rank views; all ranks in parallel
     views_all = n_views * world
@@ -206,16 +197,13 @@ def main():
         g1.record(stream)
         torch.cuda.synchronize()
         wl.check_errors()
-        graph_ms = g0.elapsed_time(g1) / args.steps
+        graph_ms = workload.max_over_ranks(g0.elapsed_time(g1), device=dev) / args.steps
 
     # end to end through the public API with host buffers
     e2e = None
     if not args.no_e2e:
         e2e = wl.e2e(args.steps, args.warmup)
-        if world > 1:
-            t = torch.tensor([e2e["ms_total"]], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e["ms_total"] = float(t.item())
+        e2e["ms_total"] = workload.max_over_ranks(e2e["ms_total"], device=dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -41,8 +41,7 @@ struct VoxelArrays {
 // same IEEE operation on the same operands as in the per-pixel form, so the
 // per-pixel results are unchanged bit for bit.
 struct StageSmem {
-  uint2 bbox[kBatch];
-  uint32_t val[kBatch];       // sorted value (quadrant << 29 | voxel id)
+  uint4 box[kBatch];          // xmin, xmax - xmin, ymin, (ymax - ymin) | quadrant << 16
   float4 slab_lo[kBatch];     // (c - o) - l/2 (xyz), 1/l (w)
   float4 slab_hi[kBatch];     // (c - o) + l/2 (xyz), l (w)
   float4 corner[kBatch];      // c - l/2 (xyz), voxel id as int bits (w)
@@ -53,8 +52,9 @@ struct StageSmem {
 __device__ __forceinline__ void stage_record(StageSmem& s, int slot, uint32_t val, const VoxelArrays& va,
                                              float ox, float oy, float oz) {
   const uint32_t vid = val_vox_id(val);
-  s.val[slot] = val;
-  s.bbox[slot] = va.bboxes[vid];
+  const uint2 bb = va.bboxes[vid];
+  s.box[slot] = make_uint4(bb_xmin(bb), bb_xmax(bb) - bb_xmin(bb), bb_ymin(bb),
+                           (bb_ymax(bb) - bb_ymin(bb)) | (val_quadrant(val) << 16));
   const float* c = va.centers + 3 * (size_t)vid;
   const float cx = c[0], cy = c[1], cz = c[2], len = va.lengths[vid];
   const float rad = 0.5f * len;
@@ -91,10 +91,18 @@ __device__ __forceinline__ float2 staged_ray_box(const float4& lo, const float4&
 // micro-tile with a matching ray quadrant?
 __device__ __forceinline__ bool record_hits_warp(const StageSmem& s, int slot, uint32_t wx0, uint32_t wy0,
                                                  uint32_t quad_mask) {
-  const uint2 bb = s.bbox[slot];
-  const uint32_t q = val_quadrant(s.val[slot]);
-  return bb_xmin(bb) <= wx0 + 7u && bb_xmax(bb) >= wx0 && bb_ymin(bb) <= wy0 + 3u && bb_ymax(bb) >= wy0 &&
-         ((quad_mask >> q) & 1u);
+  const uint4 b = s.box[slot];
+  return b.x <= wx0 + 7u && b.x + b.y >= wx0 && b.z <= wy0 + 3u && b.z + (b.w & 0xFFFFu) >= wy0 &&
+         ((quad_mask >> (b.w >> 16)) & 1u);
+}
+
+// The reference's per-pixel test: pixel inside the packed bbox and ray
+// quadrant equal to the instance's (forward.cu:186), as two unsigned range
+// checks on the staged (min, extent) form.
+__device__ __forceinline__ bool record_hits_pixel(const StageSmem& s, int j, uint32_t px, uint32_t py,
+                                                  uint32_t quad) {
+  const uint4 b = s.box[j];
+  return (px - b.x) <= b.y && (py - b.z) <= (b.w & 0xFFFFu) && (b.w >> 16) == quad;
 }
 
 __device__ __forceinline__ void load_geo(const StageSmem& s, int j, float g[8]) {

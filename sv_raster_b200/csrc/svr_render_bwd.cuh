@@ -176,8 +176,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
         bool contrib = false;
         float gp[12];
         if (inside && jpos < last_contrib) {
-          const uint32_t val = s.val[j];
-          if (pixel_in_bbox(px, py, s.bbox[j]) && ray.quad == val_quadrant(val)) {
+          if (record_hits_pixel(s, j, px, py, ray.quad)) {
             const float4 slo = s.slab_lo[j], shi = s.slab_hi[j];
             const float2 ab = staged_ray_box(slo, shi, ray);
             const float a = ab.x, b = ab.y;
@@ -343,7 +342,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
         const uint32_t act_mask = __ballot_sync(0xffffffffu, contrib);
         if (act_mask == 0u) continue;
         float* acc = s_grad + j * kGradStride;
-        if (__popc(act_mask) == 1) {
+        if (__popc(act_mask) <= 2) {  // few lanes: direct shared atomics beat the shuffle tree
           if (contrib) {
 #pragma unroll
             for (int c = 0; c < 12; ++c) atomicAdd(acc + c, gp[c]);
@@ -366,7 +365,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
 #pragma unroll
       for (int c = 0; c < 12; ++c) gsum += fabsf(acc[c]);
       if (gsum != 0.f) {
-        const uint32_t vid = val_vox_id(s.val[tid]);
+        const uint32_t vid = (uint32_t)__float_as_int(s.corner[tid].w);
 #pragma unroll
         for (int c = 0; c < 8; ++c) atomicAdd(out.dL_dgeos + 8 * (size_t)vid + c, acc[c]);
 #pragma unroll

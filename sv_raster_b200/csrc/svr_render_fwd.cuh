@@ -71,8 +71,7 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
         const int j = g * 32 + __ffs(m) - 1;
         m &= m - 1;
         if (done) continue;
-        const uint32_t val = s.val[j];
-        if (!pixel_in_bbox(px, py, s.bbox[j]) || ray.quad != val_quadrant(val)) continue;
+        if (!record_hits_pixel(s, j, px, py, ray.quad)) continue;
         const float4 slo = s.slab_lo[j], shi = s.slab_hi[j];
         const float2 ab = staged_ray_box(slo, shi, ray);
         const float a = ab.x, b = ab.y;

@@ -15,6 +15,31 @@ from ._native import Camera, check, lib
 RECORD_BYTES = 68  # bbox 8 + centre 12 + length 4 + 8 densities 32 + rgb 12
 
 
+def rank_cameras(cameras, rank, world, seed=1007):
+    """Views rendered by `rank` of `world` (weak scaling: every rank renders
+    as many views as the single-GPU workload, all at the same resolution).
+    Rank 0 keeps the workload's own cameras; other ranks get distinct seeded
+    orbit cameras of the same size, deterministic for a given (rank, world)."""
+    if world <= 1 or rank == 0:
+        return list(cameras)
+    from . import synthetic
+    n = len(cameras)
+    extra = synthetic.orbit_cameras(n * world, seed, radius=(1.5, 2.0),
+                                    fixed_size=(cameras[0].width, cameras[0].height))
+    return extra[rank * n:(rank + 1) * n]
+
+
+def max_over_ranks(value, group=None, device=None):
+    """Max of a per-rank float over the process group (the job's time is its
+    slowest rank's)."""
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized():
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
+
+
 def _t(a, dev, dt=torch.float32):
     return torch.from_numpy(np.ascontiguousarray(a)).to(dev, dt)
 
