@@ -168,6 +168,15 @@ int svr_fused_adam_step(int n_groups, int sparse, void* const* params, const int
                         const int64_t* numels, const double* steps, const double* lrs, double beta1, double beta2,
                         float eps, void* stream);
 
+/* The same with the step count kept on the device: *d_step is incremented
+ * on the stream and the bias correction computed from it on the device, so a
+ * captured training step replays with an advancing step (no reference
+ * counterpart). */
+int svr_fused_adam_step_device(int n_groups, int sparse, void* const* params, const int* param_bf16,
+                               const float* const* grads, float* const* exp_avgs, float* const* exp_avg_sqs,
+                               const int64_t* numels, const double* lrs, double beta1, double beta2, float eps,
+                               int* d_step, void* stream);
+
 /* Replace GEO_PARAMS_GATHER::gather_triinterp_geo_params(_bw) and the feat
  * variants (geo_params_gather.cu:134-222).  dim = 1 (geo) or 3 (feat). */
 int svr_gather_grid_params(int dim, int64_t n_care, const int64_t* vox_key, const int64_t* care_idx,

@@ -67,6 +67,9 @@ _SIGS = {
     "svr_fused_adam_step": (c_int, [c_int, c_int, ctypes.POINTER(c_p), ctypes.POINTER(c_int), ctypes.POINTER(c_p),
                                     ctypes.POINTER(c_p), ctypes.POINTER(c_p), ctypes.POINTER(c_i64),
                                     ctypes.POINTER(c_d), ctypes.POINTER(c_d), c_d, c_d, c_f, c_p]),
+    "svr_fused_adam_step_device": (c_int, [c_int, c_int, ctypes.POINTER(c_p), ctypes.POINTER(c_int),
+                                           ctypes.POINTER(c_p), ctypes.POINTER(c_p), ctypes.POINTER(c_p),
+                                           ctypes.POINTER(c_i64), ctypes.POINTER(c_d), c_d, c_d, c_f, c_p, c_p]),
     "svr_gather_grid_params": (c_int, [c_int, c_i64, c_p, c_p, c_p, c_p, c_p]),
     "svr_gather_grid_params_bw": (c_int, [c_int, c_i64, c_p, c_p, c_p, c_p, c_p]),
     "svr_read_error": (c_int, [c_p, ctypes.POINTER(ctypes.c_uint32), c_p]),

@@ -451,6 +451,44 @@ int svr_fused_adam_step(int n_groups, int sparse, void* const* params, const int
   return check_launch(0, stream);
 }
 
+int svr_fused_adam_step_device(int n_groups, int sparse, void* const* params, const int* param_bf16,
+                               const float* const* grads, float* const* exp_avgs, float* const* exp_avg_sqs,
+                               const int64_t* numels, const double* lrs, double beta1, double beta2, float eps,
+                               int* d_step, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (n_groups < 0 || n_groups > kMaxAdamGroups || !d_step) return SVR_ERR_SHAPE;
+  AdamGroupTable t;
+  memset(&t, 0, sizeof(t));
+  t.n = n_groups;
+  t.sparse = sparse != 0;
+  t.d_step = d_step;
+  t.beta1d = beta1;
+  t.beta2d = beta2;
+  for (int i = 0; i < n_groups; ++i) {
+    if (numels[i] < 0) return SVR_ERR_SHAPE;
+    if (!aligned16(grads[i]) || !aligned16(exp_avgs[i]) || !aligned16(exp_avg_sqs[i]) ||
+        (reinterpret_cast<uintptr_t>(params[i]) & (param_bf16[i] ? 7u : 15u)))
+      return SVR_ERR_ALIGN;
+    AdamGroup& G = t.g[i];
+    G.param = params[i];
+    G.param_bf16 = param_bf16[i];
+    G.grad = grads[i];
+    G.exp_avg = exp_avgs[i];
+    G.exp_avg_sq = exp_avg_sqs[i];
+    G.numel = numels[i];
+    G.lr = lrs[i];
+    G.beta1 = (float)beta1;
+    G.beta2 = (float)beta2;
+    G.eps = eps;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  launch_step_increment(d_step, stream);
+  launch_adam_fused(t, sms, stream);
+  return check_launch(0, stream);
+}
+
 int svr_gather_grid_params(int dim, int64_t n_care, const int64_t* vox_key, const int64_t* care_idx,
                            const float* grid_pts, float* out, void* stream_) {
   cudaStream_t stream = static_cast<cudaStream_t>(stream_);

@@ -68,12 +68,16 @@ struct AdamGroup {
   int64_t numel;
   float step_size, beta1, beta2, rsqrt_bc2, eps;
   int param_bf16;
+  double lr;           // used with a device step counter
 };
 struct AdamGroupTable {
   int n;
   int sparse;
+  const int* d_step;   // optional device step counter (bias correction on the device)
+  double beta1d, beta2d;
   AdamGroup g[kMaxAdamGroups];
 };
+void launch_step_increment(int* d_step, cudaStream_t stream);
 void launch_adam_fused(const AdamGroupTable& t, int num_sms, cudaStream_t stream);
 
 void launch_gather(int dim, int n_care, const int64_t* vox_key, const int64_t* care_idx, const float* grid_pts,

@@ -23,7 +23,7 @@ constexpr int kGroups = kBatch / 32;     // 32-record ballot groups per round
 // Resident CTAs per SM the compositing kernels are register-bounded for
 // (occupancy vs spills, chosen from -Xptxas -v and ncu measurements).
 constexpr int kFwdMinBlocks = 5;
-constexpr int kBwdMinBlocks = 3;
+constexpr int kBwdMinBlocks = 4;
 
 // Voxel attributes of one view as the kernels read them.
 struct VoxelArrays {

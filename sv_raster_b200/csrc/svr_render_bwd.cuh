@@ -342,7 +342,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
         const uint32_t act_mask = __ballot_sync(0xffffffffu, contrib);
         if (act_mask == 0u) continue;
         float* acc = s_grad + j * kGradStride;
-        if (__popc(act_mask) <= 2) {  // few lanes: direct shared atomics beat the shuffle tree
+        if (__popc(act_mask) == 1) {  // one lane: its values are the totals
           if (contrib) {
 #pragma unroll
             for (int c = 0; c < 12; ++c) atomicAdd(acc + c, gp[c]);

@@ -167,6 +167,21 @@ adam_fused_kernel(const __grid_constant__ AdamGroupTable t) {
   const int grp = blockIdx.y;
   if (grp >= t.n) return;
   const AdamGroup& G = t.g[grp];
+  // Bias correction: from the host (step_size, rsqrt_bc2) or, for a step
+  // counter kept on the device (graph replays), computed here in double
+  // exactly as the host would (adam_step.cu:117-122).
+  __shared__ float s_step_size, s_rbc2;
+  float step_size = G.step_size, rbc2 = G.rsqrt_bc2;
+  if (t.d_step) {
+    if (threadIdx.x == 0) {
+      const double st = (double)*t.d_step;
+      s_step_size = (float)(G.lr / (1.0 - pow(t.beta1d, st)));
+      s_rbc2 = (float)(1.0 / sqrt(1.0 - pow(t.beta2d, st)));
+    }
+    __syncthreads();
+    step_size = s_step_size;
+    rbc2 = s_rbc2;
+  }
   const int64_t n4 = G.numel / 4;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < (G.numel + 3) / 4; q += stride) {
@@ -202,8 +217,8 @@ adam_fused_kernel(const __grid_constant__ AdamGroupTable t) {
       if (t.sparse && g == 0.0f) continue;
       float m = adam_lerp(g, m4[k], G.beta1);
       float v = adam_lerp(g * g, v4[k], G.beta2);
-      const float denom = fmaf(sqrtf(v), G.rsqrt_bc2, G.eps);
-      const float step = G.step_size * (m / denom);
+      const float denom = fmaf(sqrtf(v), rbc2, G.eps);
+      const float step = step_size * (m / denom);
       p4[k] -= step;
       m4[k] = m;
       v4[k] = v;
@@ -229,6 +244,10 @@ adam_fused_kernel(const __grid_constant__ AdamGroupTable t) {
     }
   }
 }
+
+__global__ void step_increment_kernel(int* d_step) { *d_step += 1; }
+
+void launch_step_increment(int* d_step, cudaStream_t stream) { step_increment_kernel<<<1, 1, 0, stream>>>(d_step); }
 
 void launch_adam_fused(const AdamGroupTable& t, int num_sms, cudaStream_t stream) {
   if (t.n <= 0) return;

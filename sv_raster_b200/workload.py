@@ -411,3 +411,168 @@ class BatchedWorkload:
         e1.record(st)
         torch.cuda.synchronize()
         return dict(ms_total=e0.elapsed_time(e1), h2d=h2d, d2h=4)
+
+
+class DeviceAdam:
+    """Fused unbiased Adam over several parameter tensors with the step count
+    on the device, so one captured training step can be replayed."""
+
+    def __init__(self, params, lrs, betas=(0.1, 0.99), eps=1e-15, sparse=False):
+        self.params = list(params)
+        dev = self.params[0].device
+        self.m = [torch.zeros(p.shape, dtype=torch.float32, device=dev) for p in self.params]
+        self.v = [torch.zeros(p.shape, dtype=torch.float32, device=dev) for p in self.params]
+        self.d_step = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.lrs, self.betas, self.eps, self.sparse = list(lrs), betas, eps, sparse
+        n = len(self.params)
+        self._P = (ctypes.c_void_p * n)(*[p.data_ptr() for p in self.params])
+        self._B = (ctypes.c_int * n)(*[int(p.dtype == torch.bfloat16) for p in self.params])
+        self._M = (ctypes.c_void_p * n)(*[t.data_ptr() for t in self.m])
+        self._V = (ctypes.c_void_p * n)(*[t.data_ptr() for t in self.v])
+        self._N = (ctypes.c_int64 * n)(*[p.numel() for p in self.params])
+        self._LR = (ctypes.c_double * n)(*[float(x) for x in self.lrs])
+
+    def step(self, grads):
+        n = len(self.params)
+        G = (ctypes.c_void_p * n)(*[g.data_ptr() for g in grads])
+        check(lib().svr_fused_adam_step_device(
+            n, int(self.sparse), self._P, self._B, G, self._M, self._V, self._N, self._LR, float(self.betas[0]),
+            float(self.betas[1]), float(self.eps), ctypes.c_void_p(self.d_step.data_ptr()),
+            ctypes.c_void_p(torch.cuda.current_stream(self.params[0].device).cuda_stream)), "fused_adam_step_device")
+
+
+class BatchedTrainWorkload:
+    """One training step over all views: batched projection + SH, binning,
+    compositing, L2 loss, recompute backward, multi-view SH backward and a
+    fused Adam update of densities and SH (bf16 storage, fp32 moments);
+    capturable as one CUDA graph (the step count lives on the device)."""
+
+    def __init__(self, scene, dev, storage=torch.bfloat16, lr_geo=0.025, lr_sh=0.01, betas=(0.1, 0.99),
+                 eps=1e-15):
+        from .batched import BatchedRasterizer
+        self.sc, self.dev, self.P = scene, dev, scene.n_voxels
+        self.octpath = _t(scene.octpath.reshape(-1, 1), dev, torch.int64)
+        self.centers = _t(scene.centers, dev)
+        self.lengths = _t(scene.lengths, dev)
+        self.geos = _t(scene.geos, dev).to(storage).contiguous()
+        self.sh0 = _t(scene.sh0, dev).to(storage).contiguous()
+        self.shs = _t(scene.shs, dev).to(storage).contiguous()
+        self.cams = [_DevCam(c, dev) for c in scene.cameras]
+        self.raster = BatchedRasterizer(self.cams, self.octpath, self.centers, self.lengths,
+                                        max_level=scene.max_level)
+        self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
+        r = self.raster
+        tg = [_t(t, dev).reshape(-1) for t in scene.targets]
+        self.target = torch.cat([tg[i % len(tg)] for i in range(len(self.cams))])
+        nv = len(self.cams)
+        self.scale = torch.cat([torch.full((3 * h * w,), 2.0 / (3 * h * w * nv), device=dev) for h, w in r.sizes])
+        self.color = torch.zeros(3 * r.n_pixels, device=dev)
+        self.T = torch.zeros(r.n_pixels, device=dev)
+        self.dT = torch.zeros(r.n_pixels, device=dev)
+        self.dC = torch.zeros_like(self.color)
+        self.loss = torch.zeros((), device=dev)
+        self.grads = (torch.zeros(self.P, 8, device=dev), torch.zeros(self.P, device=dev),
+                      torch.zeros(self.P, 3, device=dev), torch.zeros(self.P, 15, 3, device=dev))
+        self.adam = DeviceAdam([self.geos, self.sh0, self.shs], [lr_geo, lr_sh, lr_sh], betas, eps)
+        self.graph = None
+
+    def _step(self):
+        r = self.raster
+        r.prepare(self.sh0, self.shs, 3)
+        r.render(self.geos, self.color, self.T)
+        diff = self.color - self.target
+        torch.mul(self.scale, diff, out=self.dC)
+        self.loss.copy_((self.dC * diff).sum() * 0.5)  # mean over views of MSE (scale = 2 / (N_v V))
+        r.backward(self.geos, self.T, self.dC, self.dT, 3, 16, grads=self.grads)
+        self.adam.step([self.grads[0], self.grads[2], self.grads[3]])
+
+    def capture(self):
+        s = torch.cuda.Stream(self.dev)
+        s.wait_stream(torch.cuda.current_stream(self.dev))
+        with torch.cuda.stream(s):  # warm-up launches (sets kernel attributes, allocator pools)
+            self._eager_probe()
+        torch.cuda.current_stream(self.dev).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._step()
+        self.graph = g
+
+    def _eager_probe(self):
+        # one forward/backward without the optimizer update, so parameters are untouched
+        r = self.raster
+        r.prepare(self.sh0, self.shs, 3)
+        r.render(self.geos, self.color, self.T)
+        diff = self.color - self.target
+        torch.mul(self.scale, diff, out=self.dC)
+        r.backward(self.geos, self.T, self.dC, self.dT, 3, 16, grads=self.grads)
+
+    def run(self, steps):
+        if self.graph is None:
+            self.capture()
+        losses = torch.zeros(steps, device=self.dev)
+        st = torch.cuda.current_stream(self.dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for i in range(steps):
+            self.graph.replay()
+            losses[i].copy_(self.loss)
+        e1.record(st)
+        torch.cuda.synchronize()
+        total, err = self.raster.header()
+        if err:
+            raise RuntimeError(f"training step reported device error word 0x{err:x}")
+        return e0.elapsed_time(e1) / steps, losses.cpu().tolist()
+
+
+class PlainTrainWorkload:
+    """The same training step in the reference's form: fp32 parameters, one
+    view per call with its host syncs (visible-index and instance-count
+    reads), gradients accumulated over the views, then SparseAdam's
+    per-parameter launches with host-side bias correction."""
+
+    def __init__(self, scene, dev, lr_geo=0.025, lr_sh=0.01, betas=(0.1, 0.99), eps=1e-15):
+        from .sparse_adam import SparseAdam
+        self.sc, self.dev, self.P = scene, dev, scene.n_voxels
+        self.octpath = _t(scene.octpath.reshape(-1, 1), dev, torch.int64)
+        self.centers = _t(scene.centers, dev)
+        self.lengths = _t(scene.lengths, dev)
+        self.geos = _t(scene.geos, dev).requires_grad_(True)
+        self.sh0 = _t(scene.sh0, dev).requires_grad_(True)
+        self.shs = _t(scene.shs, dev).requires_grad_(True)
+        self.cams = [(c, _t(c.w2c, dev), _t(c.c2w, dev)) for c in scene.cameras]
+        self.targets = [_t(t, dev) for t in scene.targets]
+        self.opt = SparseAdam([{"params": [self.geos], "lr": lr_geo}, {"params": [self.sh0], "lr": lr_sh},
+                               {"params": [self.shs], "lr": lr_sh}], betas=betas, eps=eps)
+
+    def _step(self):
+        from . import renderer
+        for p in (self.geos, self.sh0, self.shs):
+            p.grad = None
+        total = None
+        nv = len(self.cams)
+        ones = torch.ones(self.P, 1, device=self.dev)
+        for i, (cam, w2c, c2w) in enumerate(self.cams):
+            s = renderer.RasterSettings("sh", 1, cam.width, cam.height, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy,
+                                        w2c, c2w)
+
+            def vox_fn(idx, cam_pos, mode):
+                rg = renderer.SH_eval.apply(3, idx, self.centers, cam_pos, None, self.sh0, self.shs)
+                return {"geos": self.geos, "rgbs": rg, "subdiv_p": ones}
+
+            color, _, _, _, _ = renderer.rasterize_voxels(s, self.octpath, self.centers, self.lengths, vox_fn)
+            loss = ((color - self.targets[i % len(self.targets)]) ** 2).mean() / nv
+            loss.backward()
+            total = loss.detach() if total is None else total + loss.detach()
+        self.opt.step()
+        return total
+
+    def run(self, steps):
+        st = torch.cuda.current_stream(self.dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        losses = []
+        e0.record(st)
+        for _ in range(steps):
+            losses.append(self._step())
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, [float(x) for x in torch.stack(losses).cpu()]
