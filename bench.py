@@ -163,14 +163,15 @@ def main():
         wl.step()
     torch.cuda.synchronize()
 
-    # timed region: K steps bracketed by barrier + sync; events on the launch stream
+    # Timed region: K steps bracketed by barrier + sync, CUDA events on the
+    # launch stream.  Batched mode replays the captured step graph (its
+    # production form); plain mode runs the reference's per-view calls.
     stream = torch.cuda.current_stream(dev)
     sampler = ClockSampler(dev.index if dev.index is not None else 0)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     sampler.start()
-    wl.reset_kernel_timers()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
@@ -184,25 +185,21 @@ def main():
         wl.check_errors()  # capacity / consistency flags of the batched step
     ms_total = workload.max_over_ranks(ev0.elapsed_time(ev1), device=dev)
     ms_per_step = ms_total / args.steps
-    ms_per_view = ms_per_step / n_views  # per-rank views; all ranks in parallel
     views_all = n_views * world
     value = ms_total / (args.steps * views_all)  # device ms per view over the whole job
-    kstats = wl.kernel_stats()
 
-    graph_ms = None
-    if args.mode == "batched":
-        # the same step replayed from a captured CUDA graph (no per-kernel events)
-        wl.timers = {}
+    # Per-kernel durations (roofline): the same K steps again, launched eagerly
+    # with CUDA events around every stage on the launch stream.
+    wl.reset_kernel_timers()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
         wl.step()
-        torch.cuda.synchronize()
-        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        g0.record(stream)
-        for _ in range(args.steps):
-            wl.step()
-        g1.record(stream)
-        torch.cuda.synchronize()
-        wl.check_errors()
-        graph_ms = workload.max_over_ranks(g0.elapsed_time(g1), device=dev) / args.steps
+    t1.record(stream)
+    torch.cuda.synchronize()
+    eager_ms = workload.max_over_ranks(t0.elapsed_time(t1), device=dev) / args.steps
+    kstats = wl.kernel_stats()
+    wl.timers = {}
 
     # end to end through the public API with host buffers
     e2e = None
@@ -239,7 +236,8 @@ def main():
             "rays_per_s": round(sum(c.width * c.height for c in sc.cameras) * world / (ms_total / args.steps * 1e-3),
                                 1),
             "gpu_launches": wl.launches_per_step() * args.steps,
-            "graph_ms_per_step": round(graph_ms, 4) if graph_ms else None,
+            "timed_form": "cuda-graph replay" if args.mode == "batched" else "eager per-view calls",
+            "eager_instrumented_ms_per_step": round(eager_ms, 4),
             "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": round(achieved, 2),
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "peak_kind": peak_kind, "traffic": traffic,
@@ -264,16 +262,18 @@ def run_train(args, sc, dev, world, rank):
     reference-pattern step, from the same initial parameters."""
     import torch
     from sv_raster_b200 import workload
-    torch.cuda.reset_peak_memory_stats(dev)
+    torch.cuda.set_device(dev)
+    torch.zeros(1, device=dev)
+    torch.cuda.reset_peak_memory_stats()
     wl = workload.BatchedTrainWorkload(sc, dev)
     ms_b, loss_b = wl.run(args.steps)
-    peak_b = torch.cuda.max_memory_allocated(dev)
+    peak_b = torch.cuda.max_memory_allocated()
     del wl
     torch.cuda.empty_cache()
-    torch.cuda.reset_peak_memory_stats(dev)
+    torch.cuda.reset_peak_memory_stats()
     wp = workload.PlainTrainWorkload(sc, dev)
     ms_p, loss_p = wp.run(args.plain_steps)
-    peak_p = torch.cuda.max_memory_allocated(dev)
+    peak_p = torch.cuda.max_memory_allocated()
     n = min(len(loss_b), len(loss_p))
     dev_rel = max(abs(a - b) / abs(b) for a, b in zip(loss_b[:n], loss_p[:n]))
     if rank == 0:
