@@ -356,7 +356,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->o_kb = take(p->cap * 8);
   p->o_va = take(p->cap * 4);
   p->o_vb = take(p->cap * 4);
-  p->o_sort_tmp = take(sort_temp_bytes(p->cap));
+  p->o_sort_tmp = take(std::max(sort_temp_bytes(p->cap), seg_sort_temp_bytes(p->cap, (int)tiles)));
   p->o_ranges = take((size_t)tiles * 8);
   p->o_tile_last = take((size_t)tiles * 4);
   p->o_ncontrib = take((size_t)pix * 4);
@@ -384,8 +384,6 @@ int svr_batch_arrays(const svr_batch_plan* p, const void* ws, const float** rgbs
                      const uint32_t** ndup, const uint32_t** sorted_vals) {
   if (!p || !ws) return SVR_ERR_SHAPE;
   BatchPtrs q = ptrs(p, const_cast<void*>(ws));
-  const bool odd = (sort_passes(p->key_bits) & 1) != 0;
-  (void)odd;
   if (rgbs) *rgbs = q.rgbs;
   if (drgbs) *drgbs = q.drgbs;
   if (ranges) *ranges = reinterpret_cast<const uint64_t*>(q.ranges);
@@ -429,21 +427,28 @@ int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, 
   group_segments_kernel<<<1, 64, 0, stream>>>(p->gt, P, q.scan, (uint32_t)p->cap, segs);
   cudaMemsetAsync(q.ranges, 0, (size_t)p->total_tiles * sizeof(uint2), stream);
   if (p->cap > 0) {
-    const bool odd = (sort_passes(p->key_bits) & 1) != 0;
-    uint64_t* k0 = odd ? q.ka : q.kb;
-    uint32_t* v0 = odd ? q.va : q.vb;
-    uint64_t* k1 = odd ? q.kb : q.ka;
-    uint32_t* v1 = odd ? q.vb : q.va;
+    // Two-level sort: LSD radix passes over the tile bits only put every
+    // tile's instances together in generation order (ending in ka/va), then
+    // one CTA per tile sorts its segment by the rank bits into kb/vb.  The
+    // result is the order of one stable sort by the full key.
+    const bool odd = (sort_passes(p->key_bits - p->rank_bits) & 1) != 0;
+    uint64_t* k0 = odd ? q.kb : q.ka;
+    uint32_t* v0 = odd ? q.vb : q.va;
+    uint64_t* k1 = odd ? q.ka : q.kb;
+    uint32_t* v1 = odd ? q.va : q.vb;
     duplicate_batch_kernel<<<grid, 256, 0, stream>>>(p->vt, P, octree_paths, q.bbox, q.quad, q.ndup, q.scan,
                                                      p->rank_bits, k0, v0, (uint32_t)p->cap, q.header + 1);
     for (int g = 0; g < p->gt.n; ++g) {
       launch_radix_sort(k0, v0, k1, v1, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, p->key_bits, q.sort_tmp,
-                        stream);
+                        stream, p->rank_bits);
       const uint32_t g_tiles = (g + 1 < p->gt.n ? p->gt.tile_base[g + 1] : (uint32_t)p->total_tiles) -
                                p->gt.tile_base[g];
-      launch_tile_ranges(q.kb, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, p->rank_bits, p->gt.tile_base[g],
+      launch_tile_ranges(q.ka, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, p->rank_bits, p->gt.tile_base[g],
                          g_tiles, q.ranges, stream);
     }
+    // the radix histograms in sort_tmp are dead here; the segment sort reuses it
+    launch_tile_segment_sort(q.ranges, (int)p->total_tiles, q.ka, q.va, q.kb, q.vb, p->rank_bits, p->cap,
+                             q.sort_tmp, stream);
   }
   return check_last();
 }

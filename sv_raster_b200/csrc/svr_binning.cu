@@ -17,44 +17,11 @@
 #include "svr_common.cuh"
 #include "svr_views.cuh"
 #include "svr_kernels.h"
+#include "svr_block.cuh"
 
 #include <mutex>
 
 namespace svr {
-
-// --------------------------------------------------------------------------
-// Block-wide helpers
-// --------------------------------------------------------------------------
-
-// Exclusive scan of one 32-bit value per thread over a CTA of NT threads.
-template <int NT, typename T>
-__device__ __forceinline__ T block_exclusive_scan(T x, T* s_warp /*[NT/32]*/, T& total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  T inc = x;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    T y = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += y;
-  }
-  if (lane == 31) s_warp[warp] = inc;
-  __syncthreads();
-  if (warp == 0) {
-    T w = (lane < NT / 32) ? s_warp[lane] : T(0);
-    T winc = w;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      T y = __shfl_up_sync(0xffffffffu, winc, o);
-      if (lane >= o) winc += y;
-    }
-    if (lane < NT / 32) s_warp[lane] = winc - w;  // exclusive warp offsets
-    if (lane == NT / 32 - 1) s_warp[NT / 32] = winc;
-  }
-  __syncthreads();
-  T res = s_warp[warp] + inc - x;
-  total = s_warp[NT / 32];
-  __syncthreads();
-  return res;
-}
 
 // --------------------------------------------------------------------------
 // Inclusive scan of uint32 counts (three phases, no inter-CTA waiting)
@@ -238,11 +205,6 @@ size_t sort_temp_bytes(size_t cap) {
 
 int sort_passes(int key_bits) { return (key_bits + 7) / 8; }
 
-__device__ __forceinline__ uint32_t lanemask_lt() {
-  uint32_t m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
 
 __global__ void __launch_bounds__(kSortThreads)
 radix_upsweep_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ d_start,
@@ -403,12 +365,13 @@ void ensure_sort_attributes() {
 }
 
 // Sorts the `*d_n` pairs starting at element `*d_start` (both read on the
-// device; d_start may be null for 0) of (k0, v0), using (k1, v1) as the
-// ping-pong buffer; `cap` bounds the count and sizes the grid.  Returns 0 if
-// the result is in (k0, v0), 1 if in (k1, v1).
+// device; d_start may be null for 0) of (k0, v0) by key bits [lo_bit,
+// key_bits), using (k1, v1) as the ping-pong buffer; `cap` bounds the count
+// and sizes the grid.  Returns 0 if the result is in (k0, v0), 1 if in (k1, v1).
 int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, const uint32_t* d_start,
-                      const uint32_t* d_n, uint32_t cap, int key_bits, void* temp, cudaStream_t stream) {
-  const int passes = sort_passes(key_bits);
+                      const uint32_t* d_n, uint32_t cap, int key_bits, void* temp, cudaStream_t stream,
+                      int lo_bit) {
+  const int passes = sort_passes(key_bits - lo_bit);
   if (cap == 0 || passes == 0) return 0;
   const int nb = sort_blocks(cap);
   uint32_t* hist = reinterpret_cast<uint32_t*>(temp);
@@ -417,7 +380,7 @@ int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, co
   ensure_sort_attributes();
   uint64_t* kin = k0; uint32_t* vin = v0; uint64_t* kout = k1; uint32_t* vout = v1;
   for (int p = 0; p < passes; ++p) {
-    const int shift = 8 * p;
+    const int shift = lo_bit + 8 * p;
     radix_upsweep_kernel<<<nb, kSortThreads, 0, stream>>>(kin, d_start, d_n, cap, shift, hist, nb);
     radix_scan_rows_kernel<<<kRadix, 1024, 0, stream>>>(hist, nb, digit_total);
     radix_downsweep_kernel<<<nb, kSortThreads, smem, stream>>>(kin, vin, kout, vout, d_start, d_n, cap, shift,

@@ -91,14 +91,17 @@ struct BinningLayout {
   size_t bytes;
 };
 
-BinningLayout binning_layout(void* buf, size_t n) {
+// The sort temp (last) serves the tile-bit radix passes and then the
+// per-tile segment sort, so its size depends on the tile count; the stages
+// after binning only use the key/value arrays and pass n_tiles = 0.
+BinningLayout binning_layout(void* buf, size_t n, int n_tiles) {
   Carver c(buf);
   BinningLayout b;
   b.keys_a = c.take<uint64_t>(n);
   b.keys_b = c.take<uint64_t>(n);
   b.vals_a = c.take<uint32_t>(n);
   b.vals_b = c.take<uint32_t>(n);
-  b.sort_temp = c.take<char>(sort_temp_bytes(n));
+  b.sort_temp = c.take<char>(std::max(sort_temp_bytes(n), n_tiles > 0 ? seg_sort_temp_bytes(n, n_tiles) : 0));
   b.bytes = c.size();
   return b;
 }
@@ -177,9 +180,8 @@ size_t svr_image_buffer_bytes(int width, int height) {
   return (width <= 0 || height <= 0) ? 0 : image_layout(nullptr, width, height).bytes;
 }
 size_t svr_binning_buffer_bytes(int64_t n, int width, int height) {
-  (void)width;
-  (void)height;
-  return n < 0 ? 0 : binning_layout(nullptr, (size_t)n).bytes;
+  if (n < 0 || width <= 0 || height <= 0) return 0;
+  return binning_layout(nullptr, (size_t)n, tiles_x(width) * tiles_y(height)).bytes;
 }
 
 const uint32_t* svr_geom_count_ptr(const void* geom) { return static_cast<const uint32_t*>(geom); }
@@ -223,7 +225,7 @@ static int fwd_prepare(const svr_camera* cam, int n_samp, int64_t P, int64_t num
   c.im = image_layout(image_buffer, W, H);
   if (!image_buffer || image_bytes < c.im.bytes) return SVR_ERR_CAPACITY;
   c.n = (size_t)num_rendered;
-  c.bl = binning_layout(binning_buffer, c.n);
+  c.bl = binning_layout(binning_buffer, c.n, tiles_x(W) * tiles_y(H));
   if (c.n > 0 && (!binning_buffer || binning_bytes < c.bl.bytes)) return SVR_ERR_CAPACITY;
   c.key_bits = plain_key_bits(W, H);
   if (c.key_bits > 64) return SVR_ERR_KEYBITS;
@@ -246,17 +248,24 @@ int svr_rasterize_binning(const svr_camera* cam, int64_t P, int64_t num_rendered
   const ViewParams& vp = c.vt.v[0];
   cudaMemsetAsync(c.im.ranges, 0, (size_t)vp.grid_x * vp.grid_y * sizeof(uint2), stream);
   if (c.n > 0) {
-    // Duplicate into the buffer that leaves the sorted result in (keys_b, vals_b).
-    const bool odd = (sort_passes(c.key_bits) & 1) != 0;
-    uint64_t* k0 = odd ? c.bl.keys_a : c.bl.keys_b;
-    uint32_t* v0 = odd ? c.bl.vals_a : c.bl.vals_b;
-    uint64_t* k1 = odd ? c.bl.keys_b : c.bl.keys_a;
-    uint32_t* v1 = odd ? c.bl.vals_b : c.bl.vals_a;
+    // Two-level sort (same order as one stable sort by the full key): radix
+    // passes over the tile bits leave each tile's instances together, in
+    // generation order, in (keys_a, vals_a); the per-tile segment sort by the
+    // rank bits then writes the final order to (keys_b, vals_b).
+    const bool odd = (sort_passes(c.key_bits - kRankBits) & 1) != 0;
+    uint64_t* k0 = odd ? c.bl.keys_b : c.bl.keys_a;
+    uint32_t* v0 = odd ? c.bl.vals_b : c.bl.vals_a;
+    uint64_t* k1 = odd ? c.bl.keys_a : c.bl.keys_b;
+    uint32_t* v1 = odd ? c.bl.vals_a : c.bl.vals_b;
+    const int n_tiles = vp.grid_x * vp.grid_y;
     launch_duplicate(c.vt, (int)P, octree_paths, c.g.bbox, c.g.quad, c.g.ndup, c.g.scan, k0, v0, (uint32_t)c.n,
                      c.g.header + 1, stream);
-    launch_radix_sort(k0, v0, k1, v1, nullptr, c.g.header, (uint32_t)c.n, c.key_bits, c.bl.sort_temp, stream);
-    launch_tile_ranges(c.bl.keys_b, nullptr, c.g.header, (uint32_t)c.n, kRankBits, 0u,
-                       (uint32_t)(vp.grid_x * vp.grid_y), c.im.ranges, stream);
+    launch_radix_sort(k0, v0, k1, v1, nullptr, c.g.header, (uint32_t)c.n, c.key_bits, c.bl.sort_temp, stream,
+                      kRankBits);
+    launch_tile_ranges(c.bl.keys_a, nullptr, c.g.header, (uint32_t)c.n, kRankBits, 0u, (uint32_t)n_tiles,
+                       c.im.ranges, stream);
+    launch_tile_segment_sort(c.im.ranges, n_tiles, c.bl.keys_a, c.bl.vals_a, c.bl.keys_b, c.bl.vals_b, kRankBits,
+                             c.n, c.bl.sort_temp, stream);
   }
   return check_launch(debug, stream);
 }
@@ -319,7 +328,7 @@ int svr_rasterize_backward(const svr_camera* cam, int n_samp, int64_t P, int64_t
   const int W = cam->width, H = cam->height;
   GeomLayout g = geom_layout(const_cast<void*>(geom_buffer), P);
   ImageLayout im = image_layout(const_cast<void*>(image_buffer), W, H);
-  BinningLayout bl = binning_layout(const_cast<void*>(binning_buffer), (size_t)num_rendered);
+  BinningLayout bl = binning_layout(const_cast<void*>(binning_buffer), (size_t)num_rendered, 0);
   const ViewParams vp = make_view(*cam);
   VoxelArrays va{g.bbox, vox_centers, vox_lengths, geos, nullptr, rgbs};
   BwdTileIn in{out_T, im.n_contrib, dL_dcolor, need_depth ? dL_ddepth : nullptr,
@@ -350,7 +359,7 @@ int svr_binning_sorted(const void* binning_buffer, int64_t num_rendered, int wid
   (void)width;
   (void)height;
   if (!binning_buffer || num_rendered < 0) return SVR_ERR_SHAPE;
-  BinningLayout bl = binning_layout(const_cast<void*>(binning_buffer), (size_t)num_rendered);
+  BinningLayout bl = binning_layout(const_cast<void*>(binning_buffer), (size_t)num_rendered, 0);
   if (keys) *keys = bl.keys_b;
   if (vals) *vals = bl.vals_b;
   return SVR_OK;

@@ -30,7 +30,17 @@ size_t sort_temp_bytes(size_t cap);
 void ensure_sort_attributes();
 int sort_passes(int key_bits);
 int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, const uint32_t* d_start,
-                      const uint32_t* d_n, uint32_t cap, int key_bits, void* temp, cudaStream_t stream);
+                      const uint32_t* d_n, uint32_t cap, int key_bits, void* temp, cudaStream_t stream,
+                      int lo_bit = 0);
+// Stable sort of every tile's segment [ranges[t].x, ranges[t].y) by the key
+// bits below `rank_bits`, from (ka, va) into (kb, vb) (svr_segsort.cu).
+// Sorts every tile's segment [ranges[t].x, ranges[t].y) of (ka, va) by key
+// bits [0, rank_bits), stably, into the same positions of (kb, vb); ka/va are
+// clobbered.  `cap` bounds the total instance count; temp holds
+// seg_sort_temp_bytes(cap, n_tiles) bytes.
+size_t seg_sort_temp_bytes(size_t cap, int n_tiles);
+void launch_tile_segment_sort(const uint2* ranges, int n_tiles, uint64_t* ka, uint32_t* va, uint64_t* kb,
+                              uint32_t* vb, int rank_bits, size_t cap, void* temp, cudaStream_t stream);
 void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_start, const uint32_t* d_n, uint32_t cap,
                         int rank_bits, uint32_t tile_base, uint32_t n_tiles, uint2* ranges, cudaStream_t stream);
 

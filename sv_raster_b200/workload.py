@@ -157,9 +157,9 @@ class PlainWorkload:
         n = 0
         for cam, _, _ in self.cams:
             T_ = math.ceil(cam.width / 16) * math.ceil(cam.height / 16)
-            passes = math.ceil((48 + int(T_).bit_length()) / 8)
-            # preprocess 1 + scan 3 + duplicate 1 + sort 3/pass + ranges 1 + fwd 1 + bwd 1 + sh 2
-            n += 1 + 3 + 1 + 3 * passes + 1 + 1 + 1 + 2
+            passes = math.ceil(int(T_).bit_length() / 8)  # radix passes over the tile bits only
+            # preprocess 1 + scan 3 + duplicate 1 + sort 3/pass + ranges 1 + segment sort 4 + fwd 1 + bwd 1 + sh 2
+            n += 1 + 3 + 1 + 3 * passes + 1 + 4 + 1 + 1 + 2
         return n
 
     def kernel_stats(self):
@@ -361,10 +361,11 @@ class BatchedWorkload:
 
     def launches_per_step(self):
         T_ = max(self.raster.n_tiles, 1)
-        passes = math.ceil((3 * self.sc.max_level + 3 + int(T_).bit_length()) / 8)
+        passes = math.ceil(int(T_).bit_length() / 8)  # radix passes over the tile bits only
         g = self.raster.n_groups
-        # project 1 + scan 3 + segments 1 + duplicate 1 + (sort 3/pass + ranges 1) per group + fwd 1 + bwd 1 + sh 1
-        return 1 + 3 + 1 + 1 + g * (3 * passes + 1) + 1 + 1 + 1
+        # project 1 + scan 3 + segments 1 + duplicate 1 + (sort 3/pass + ranges 1) per group
+        # + segment sort 4 (plan, small, chunk, merge) + fwd 1 + bwd 1 + sh 1
+        return 1 + 3 + 1 + 1 + g * (3 * passes + 1) + 4 + 1 + 1 + 1
 
     def kernel_stats(self):
         torch.cuda.synchronize()

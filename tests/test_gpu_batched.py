@@ -95,6 +95,42 @@ def test_batched_forward_equals_plain(c1, max_key_bits, monkeypatch):
         tile0 += nt
 
 
+def test_large_tile_segments_match_plain_sort():
+    """Low-resolution views put up to ~20k instances in one 16x16 tile, so the
+    per-tile segment sort takes its streamed (larger than shared memory) path;
+    every tile list must still equal the plain path's full-key radix sort."""
+    import dataclasses
+    sc = synthetic.config_scene("c1")
+    cams = [synthetic.make_camera(16, 16, 70.0, (0.3, -0.4, 3.2)), synthetic.make_camera(48, 40, 60.0, (0.0, 2.0, 2.5)),
+            synthetic.make_camera(64, 64, 90.0, (2.2, 0.5, -1.8))]
+    C = SceneTensors(dataclasses.replace(sc, cameras=cams))
+    r = BatchedRasterizer([DevCam(c) for c in cams], C.octpath, C.centers, C.lengths, max_level=sc.max_level)
+    r.fit_capacity(C.sh0, C.shs, 3)
+    r.prepare(C.sh0, C.shs, 3)
+    color, T = r.render(C.geos)
+    torch.cuda.synchronize()
+    assert r.header()[1] == 0
+    arr = r.arrays()
+    cols = r.split_color(color)
+    tile0, biggest = 0, 0
+    for k in range(len(cams)):
+        p = _plain_view(C, k, C.sh0, C.shs, C.geos)
+        assert torch.equal(cols[k], p["color"]), f"view {k}: colour differs"
+        cam = p["cam"]
+        pr, _, _ = mC.unpack_ImageState(cam.width, cam.height, p["img"])
+        _, pv = mC.unpack_sorted_list(p["binning"], p["R"], cam.width, cam.height)
+        nt = pr.shape[0] * pr.shape[1]
+        pr2 = pr.view(-1, 2)
+        br2 = arr["ranges"][tile0:tile0 + nt].view(-1, 2)
+        assert torch.equal(br2[:, 1] - br2[:, 0], pr2[:, 1] - pr2[:, 0])
+        for t in range(nt):
+            a0, a1, b0 = int(pr2[t, 0]), int(pr2[t, 1]), int(br2[t, 0])
+            biggest = max(biggest, a1 - a0)
+            assert torch.equal(arr["sorted_vals"][b0:b0 + a1 - a0], pv[a0:a1]), f"view {k} tile {t}"
+        tile0 += nt
+    assert biggest > 4096, biggest  # the streamed segment path ran
+
+
 def test_batched_backward_equals_plain_sum(c1):
     r, _ = _raster(c1)
     r.fit_capacity(c1.sh0, c1.shs, 3)
