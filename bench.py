@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--views", type=int, default=None, help="use only the first N views")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg (profiling runs)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="batched mode: default launch parameters instead of the autotuner's choice")
     ap.add_argument("--train", action="store_true",
                     help="training-step workload (fwd + bwd + fused Adam, graph-captured) vs the plain fp32 form")
     ap.add_argument("--plain-steps", type=int, default=10, help="steps of the plain form in --train mode")
@@ -156,7 +158,8 @@ def main():
     sc = scene_for(args, rank, world)
     if args.train:
         return run_train(args, sc, dev, world, rank)
-    wl = workload.PlainWorkload(sc, dev) if args.mode == "plain" else workload.BatchedWorkload(sc, dev)
+    wl = workload.PlainWorkload(sc, dev) if args.mode == "plain" else \
+        workload.BatchedWorkload(sc, dev, tune=not args.no_tune)
     n_views = len(sc.cameras)
 
     for _ in range(args.warmup):
@@ -232,6 +235,7 @@ def main():
                                    f"{sc.cameras[0].width}x{sc.cameras[0].height}, SH3, fwd+recompute bwd",
                        "mode": args.mode, "l2": "inputs larger than L2 (scene arrays > 126 MB)",
                        "instances_per_view": wl.instances_per_view()},
+            "autotuned": getattr(wl, "tuned", None),
             "render_fps": round(1000.0 / kstats["fwd_ms_per_view"], 2) if kstats.get("fwd_ms_per_view") else None,
             "rays_per_s": round(sum(c.width * c.height for c in sc.cameras) * world / (ms_total / args.steps * 1e-3),
                                 1),

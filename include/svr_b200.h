@@ -209,9 +209,31 @@ int svr_read_error(uint32_t* device_word, uint32_t* host_value, void* stream);
  * total instance count is at svr_batch_count_ptr.  Every voxel's octree level
  * must be <= max_level (checked on the device: SVR_DEVERR_LEVEL, 0x10). */
 typedef struct svr_batch_plan svr_batch_plan;
+/* tile_size: compositing tiles of 8x8, 16x16 (the reference's) or 32x32
+ * pixels.  Images, T and per-view gradients are the same for every tile size
+ * (a pixel sees the same instances in the same order); the instance count,
+ * tile lists and contributor indices are those of the chosen tiling. */
 int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_t capacity, int n_samp_per_vox,
-                          int max_level, svr_batch_plan** plan, size_t* workspace_bytes);
+                          int max_level, int tile_size, svr_batch_plan** plan, size_t* workspace_bytes);
 void svr_batch_plan_destroy(svr_batch_plan* plan);
+/* Compositing schedule of svr_batch_render / svr_batch_backward: both are
+ * persistent launches that take (view, tile) items from a device counter.
+ * order_flags bit 0 (forward) / bit 1 (backward), both set by default, rank
+ * the tiles largest first (by instance count, eighth-octave buckets) before
+ * the launch; a clear bit keeps tile order.  The ctas_per_sm caps (0 = as
+ * many as fit, the default) bound the resident CTAs per SM.  Results do not
+ * depend on the schedule (gradients only up to the order of floating-point
+ * additions). */
+int svr_batch_plan_set_schedule(svr_batch_plan* plan, int order_flags, int fwd_ctas_per_sm, int bwd_ctas_per_sm);
+/* Segment-size buckets of the per-tile segment sort in svr_batch_prepare:
+ * tiles of at most small_n (256, 512 or 1024) instances are sorted by one
+ * small CTA each, longer ones in runs of `chunk` (2048 or 4096) instances
+ * merged afterwards.  Defaults 512 / 4096; the order is the same for all. */
+int svr_batch_plan_set_sort_buckets(svr_batch_plan* plan, int small_n, int chunk);
+/* Records staged into shared memory per round by the compositing kernels:
+ * 128, 256 (default) or 512 with 16x16 tiles, 64 with 8x8, 256 with 32x32. */
+int svr_batch_plan_set_staging(svr_batch_plan* plan, int records);
+int svr_batch_plan_tile_size(const svr_batch_plan* plan);
 int64_t svr_batch_plan_pixels(const svr_batch_plan* plan);
 int64_t svr_batch_plan_tiles(const svr_batch_plan* plan);
 int svr_batch_plan_groups(const svr_batch_plan* plan);
@@ -227,11 +249,11 @@ int svr_batch_arrays(const svr_batch_plan* plan, const void* workspace, const fl
 int svr_batch_prepare(svr_batch_plan* plan, void* workspace, const int64_t* octree_paths, const float* vox_centers,
                       const float* vox_lengths, const void* sh0, const void* shs, int sh_bf16, int sh_degree, int M,
                       void* stream);
-/* Compositing of every (view, tile) in one launch; geos fp32 or bf16 [P,8].
+/* Compositing of every (view, tile) in one persistent launch; geos fp32 or bf16 [P,8].
  * out_color / out_T caller-zeroed. */
 int svr_batch_render(svr_batch_plan* plan, void* workspace, const float* vox_centers, const float* vox_lengths,
                      const void* geos, int geos_bf16, float* out_color, float* out_T, void* stream);
-/* Recompute-backward of every (view, tile) in one launch: dL_dgeos [P,8] and
+/* Recompute-backward of every (view, tile) in one persistent launch: dL_dgeos [P,8] and
  * subdiv [P] summed over views (caller-zeroed); per-view dL/drgb kept in the
  * workspace for svr_batch_sh_backward. */
 int svr_batch_backward(svr_batch_plan* plan, void* workspace, const float* vox_centers, const float* vox_lengths,

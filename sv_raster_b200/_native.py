@@ -74,9 +74,13 @@ _SIGS = {
     "svr_gather_grid_params_bw": (c_int, [c_int, c_i64, c_p, c_p, c_p, c_p, c_p]),
     "svr_read_error": (c_int, [c_p, ctypes.POINTER(ctypes.c_uint32), c_p]),
     "svr_total_variation_bw": (c_int, [c_p, c_p, c_f, c_p, c_int, c_int, c_i64, c_int, c_p, c_p, c_p]),
-    "svr_batch_plan_create": (c_int, [c_int, ctypes.POINTER(Camera), c_i64, c_i64, c_int, c_int,
+    "svr_batch_plan_create": (c_int, [c_int, ctypes.POINTER(Camera), c_i64, c_i64, c_int, c_int, c_int,
                                       ctypes.POINTER(c_p), ctypes.POINTER(c_sz)]),
     "svr_batch_plan_destroy": (None, [c_p]),
+    "svr_batch_plan_set_schedule": (c_int, [c_p, c_int, c_int, c_int]),
+    "svr_batch_plan_set_sort_buckets": (c_int, [c_p, c_int, c_int]),
+    "svr_batch_plan_set_staging": (c_int, [c_p, c_int]),
+    "svr_batch_plan_tile_size": (c_int, [c_p]),
     "svr_batch_plan_pixels": (c_i64, [c_p]),
     "svr_batch_plan_tiles": (c_i64, [c_p]),
     "svr_batch_plan_groups": (c_int, [c_p]),

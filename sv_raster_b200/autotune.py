@@ -1,0 +1,174 @@
+"""Autotuner for the batched rasterizer's launch parameters.
+
+The parameters it chooses change only how the work is scheduled, never the
+results (images and contributor counts are bit-identical across choices;
+gradients agree up to the order of floating-point additions):
+
+* ``fwd`` / ``bwd`` -- compositing schedule of the persistent forward and
+  backward launches: tiles largest first or in tile order, and the cap on
+  resident CTAs per SM (``BatchedRasterizer.set_schedule``).
+* ``sort`` -- segment-size buckets of the per-tile segment sort: the largest
+  segment sorted by one small CTA and the chunk length of the chunked sort
+  (``BatchedRasterizer.set_sort_buckets``).
+* ``tile`` -- compositing tile size of the batched path (8, 16 or 32 pixels)
+  with the voxel-staging depth (records staged into shared memory per round)
+  (``BatchedRasterizer.set_tile_size``; the tile size changes the binning, so
+  it is tuned with the full step).
+
+Each stage is timed on the caller's own scene and cameras with CUDA events
+(median of ``reps`` launches after warm-up), one stage at a time, and the
+fastest candidate is kept.  Results are cached in a JSON file keyed by the
+GPU, the scene size, the camera sizes and the storage dtypes
+(``SVR_AUTOTUNE_CACHE`` overrides the path; ``cache=False`` skips it).
+"""
+import json
+import os
+
+import torch
+
+DEFAULT_SPACE = {
+    "tile": [(16, 256), (8, 64), (32, 256), (16, 128), (16, 512)],
+    "sort": [(512, 4096), (256, 4096), (1024, 4096), (512, 2048)],
+    "fwd": [(True, 0), (False, 0), (True, 4), (True, 3)],
+    "bwd": [(True, 0), (False, 0), (True, 3), (True, 2)],
+}
+
+
+def cache_path():
+    return os.environ.get("SVR_AUTOTUNE_CACHE") or os.path.join(
+        os.path.expanduser("~"), ".cache", "sv_raster_b200", "autotune.json")
+
+
+def _load_cache(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store_cache(path, data):
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+
+
+def cache_key(raster, geos, sh0):
+    dev = raster.dev
+    name = torch.cuda.get_device_name(dev) if dev.type == "cuda" else "cpu"
+    sizes = ",".join(f"{w}x{h}" for h, w in raster.sizes)
+    return f"{name}|P={raster.P}|views={sizes}|ns={raster.n_samp}|geo={geos.dtype}|sh={sh0.dtype}"
+
+
+def time_ms(fn, reps=5, warmup=2, stream=None):
+    """Median device time of fn() in ms (CUDA events on the current stream)."""
+    st = stream or torch.cuda.current_stream()
+    for _ in range(warmup):
+        fn()
+    times = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    times.sort()
+    return times[len(times) // 2]
+
+
+def apply(raster, choice):
+    """Apply a tuned choice dict (keys of DEFAULT_SPACE) to a rasterizer."""
+    if "tile" in choice:
+        ts, sb = choice["tile"]
+        raster.set_tile_size(int(ts), int(sb))
+    if "sort" in choice:
+        raster.set_sort_buckets(*[int(x) for x in choice["sort"]])
+    f = choice.get("fwd", (True, 0))
+    b = choice.get("bwd", (True, 0))
+    raster.set_schedule(fwd_ordered=bool(f[0]), bwd_ordered=bool(b[0]), fwd_ctas_per_sm=int(f[1]),
+                        bwd_ctas_per_sm=int(b[1]))
+
+
+def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup=2, cache=True, timer=time_ms):
+    """Choose the batched rasterizer's launch parameters for this scene.
+
+    Returns ``dict(choice=..., timings=..., cached=bool)`` and leaves the
+    choice applied to ``raster``.  ``timer(fn, reps, warmup)`` times a stage
+    (replaceable for tests).  Stages are tuned in order: tile size (full
+    step), sort buckets (prepare), forward schedule (render), backward
+    schedule (backward), each with the previous choices applied.
+    """
+    space = dict(DEFAULT_SPACE if space is None else space)
+    key = cache_key(raster, geos, sh0)
+    path = cache_path()
+    if cache:
+        hit = _load_cache(path).get(key)
+        if hit is not None:
+            choice = {k: (tuple(v) if isinstance(v, list) else v) for k, v in hit["choice"].items()}
+            apply(raster, choice)
+            raster.fit_capacity(sh0, shs, sh_degree)
+            return dict(choice=choice, timings=hit.get("timings", {}), cached=True)
+
+    M = 1 + shs.shape[1]
+    choice = {"tile": DEFAULT_SPACE["tile"][0], "sort": DEFAULT_SPACE["sort"][0], "fwd": DEFAULT_SPACE["fwd"][0],
+              "bwd": DEFAULT_SPACE["bwd"][0]}
+    timings = {}
+    gen = torch.Generator(device=raster.dev)
+    gen.manual_seed(0)
+    state = {}
+
+    def upstream():
+        # a fixed, seeded upstream gradient of the images (values do not matter for timing)
+        if "dC" not in state or state["dC"].numel() != 3 * raster.n_pixels:
+            state["dC"] = torch.rand(3 * raster.n_pixels, device=raster.dev, generator=gen) * 1e-6
+            state["dT"] = torch.zeros(raster.n_pixels, device=raster.dev)
+        return state["dC"], state["dT"]
+
+    def step():
+        raster.prepare(sh0, shs, sh_degree)
+        render()
+        backward()
+
+    def prepare():
+        raster.prepare(sh0, shs, sh_degree)
+
+    def render():
+        state["out"] = raster.render(geos, *state.get("out", (None, None)))
+
+    def backward():
+        dC, dT = upstream()
+        state["grads"] = raster.backward(geos, state["out"][1], dC, dT, sh_degree, M, state.get("grads"))
+
+    stages = [("tile", step), ("sort", prepare), ("fwd", render), ("bwd", backward)]
+    for name, fn in stages:
+        cands = space.get(name)
+        if not cands:
+            continue
+        res = []
+        for cand in cands:
+            apply(raster, dict(choice, **{name: cand}))
+            if name == "tile":
+                raster.fit_capacity(sh0, shs, sh_degree)
+            if name in ("fwd", "bwd"):
+                raster.prepare(sh0, shs, sh_degree)
+                render()
+            t = timer(fn, reps, warmup)
+            res.append((t, cand))
+        timings[name] = [[c if not isinstance(c, tuple) else list(c), round(t, 4)] for t, c in res]
+        choice[name] = min(res, key=lambda x: x[0])[1]
+        apply(raster, choice)
+        if name == "tile":
+            raster.fit_capacity(sh0, shs, sh_degree)
+    if cache:
+        data = _load_cache(path)
+        data[key] = dict(choice={k: (list(v) if isinstance(v, tuple) else v) for k, v in choice.items()},
+                         timings=timings)
+        _store_cache(path, data)
+    return dict(choice=choice, timings=timings, cached=False)

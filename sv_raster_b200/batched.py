@@ -28,7 +28,7 @@ class BatchedRasterizer:
     """
 
     def __init__(self, cameras, octree_paths, vox_centers, vox_lengths, max_level=16, n_samp_per_vox=1,
-                 bg_color=0.0, capacity=None, headroom=1.25):
+                 bg_color=0.0, capacity=None, headroom=1.25, tile_size=16):
         self.dev = vox_centers.device
         self.cams = list(cameras)
         self.octree_paths = octree_paths.reshape(-1).contiguous()
@@ -50,6 +50,10 @@ class BatchedRasterizer:
         for h, w in self.sizes:
             self.pix_offsets.append(self.pix_offsets[-1] + h * w)
         self.plan = None
+        self.tile_size = int(tile_size)
+        self.staging = 64 if self.tile_size == 8 else 256
+        self.schedule = (3, 0, 0)
+        self.sort_buckets = (512, 4096)
         self._make_plan(0 if capacity is None else int(capacity))
         self.capacity_auto = capacity is None
 
@@ -62,13 +66,49 @@ class BatchedRasterizer:
         plan = ctypes.c_void_p()
         nbytes = ctypes.c_size_t()
         check(L.svr_batch_plan_create(len(self.cams), self._c_cams, self.P, capacity, self.n_samp, self.max_level,
-                                      ctypes.byref(plan), ctypes.byref(nbytes)), "batch_plan_create")
+                                      self.tile_size, ctypes.byref(plan), ctypes.byref(nbytes)), "batch_plan_create")
         self.plan = plan
         self.capacity = capacity
         self.ws = torch.empty(nbytes.value, dtype=torch.uint8, device=self.dev)
         self.n_pixels = int(L.svr_batch_plan_pixels(plan))
         self.n_tiles = int(L.svr_batch_plan_tiles(plan))
         self.n_groups = int(L.svr_batch_plan_groups(plan))
+        check(L.svr_batch_plan_set_schedule(plan, *self.schedule), "batch_plan_set_schedule")
+        check(L.svr_batch_plan_set_sort_buckets(plan, *self.sort_buckets), "batch_plan_set_sort_buckets")
+        check(L.svr_batch_plan_set_staging(plan, self.staging), "batch_plan_set_staging")
+
+    def set_tile_size(self, tile_size, staging=None):
+        """Compositing tile size (8, 16 or 32 pixels) and records staged per
+        round (default 64 / 256 / 256).  A new tile size re-plans (the
+        workspace and instance capacity change; call fit_capacity again)."""
+        tile_size = int(tile_size)
+        staging = int(staging) if staging is not None else (64 if tile_size == 8 else 256)
+        if tile_size != self.tile_size:
+            self.tile_size = tile_size
+            self.staging = staging
+            self._make_plan(self.capacity)
+        else:
+            self.set_staging(staging)
+
+    def set_staging(self, records):
+        """Records staged into shared memory per round (see svr_batch_plan_set_staging)."""
+        check(lib().svr_batch_plan_set_staging(self.plan, int(records)), "batch_plan_set_staging")
+        self.staging = int(records)
+
+    def set_sort_buckets(self, small_n=512, chunk=4096):
+        """Segment-size buckets of the per-tile segment sort (small_n in
+        256/512/1024, chunk in 2048/4096); the sorted order is the same for all."""
+        self.sort_buckets = (int(small_n), int(chunk))
+        check(lib().svr_batch_plan_set_sort_buckets(self.plan, *self.sort_buckets), "batch_plan_set_sort_buckets")
+
+    def set_schedule(self, fwd_ordered=True, bwd_ordered=True, fwd_ctas_per_sm=0, bwd_ctas_per_sm=0):
+        """Compositing schedule: per stage, tiles largest first (``*_ordered``)
+        or in tile order, and caps on the resident CTAs per SM of the
+        persistent forward / backward launches (0 = as many as fit).  Results
+        do not depend on it."""
+        self.schedule = (int(bool(fwd_ordered)) | (int(bool(bwd_ordered)) << 1), int(fwd_ctas_per_sm),
+                         int(bwd_ctas_per_sm))
+        check(lib().svr_batch_plan_set_schedule(self.plan, *self.schedule), "batch_plan_set_schedule")
 
     def __del__(self):
         try:

@@ -108,7 +108,7 @@ duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const int
   const uint32_t wend = min(end, cap);
   uint32_t off = end - n;
   int tx0, ty0, tx1, ty1;
-  bbox_tile_rect(bboxes[o], vp.grid_x, vp.grid_y, tx0, ty0, tx1, ty1);
+  bbox_tile_rect(bboxes[o], vp.grid_x, vp.grid_y, vp.tile_shift, tx0, ty0, tx1, ty1);
   const uint64_t path = (uint64_t)octpaths[idx];
   const int low = (rank_bits == kRankBits) ? 0 : kRankBits - (rank_bits - 3);  // 3*(16-L)
   if (low > 0 && (path & ((1ull << low) - 1ull)) != 0ull) atomicOr(err, SVR_DEVERR_LEVEL);
@@ -182,6 +182,25 @@ sh_bw_batch_kernel(const __grid_constant__ ViewTable views, int P, int M, const 
   }
 }
 
+// Work-order key of every tile for the persistent compositing launches:
+// one 8-bit digit, 255 minus an eighth-octave bucket of the tile's cost
+// (instances in [range.x, end), end = tile_last when given), so a stable
+// sort by it lists the tiles largest first and, within a bucket, in tile
+// order.  Thread 0 also stores the tile count the sort reads.
+__global__ void tile_order_keys_kernel(const uint2* __restrict__ ranges, const uint32_t* __restrict__ tile_last,
+                                       uint32_t n_tiles, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                       uint32_t* __restrict__ d_n) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) *d_n = n_tiles;
+  if (t >= n_tiles) return;
+  const uint2 r = ranges[t];
+  const uint32_t end = tile_last ? tile_last[t] : r.y;
+  const uint32_t cost = end > r.x ? end - r.x : 0u;
+  const uint32_t bucket = min(255u, (uint32_t)(log2f((float)cost + 1.f) * 7.9f));
+  keys[t] = 255u - bucket;
+  vals[t] = t;
+}
+
 inline int bit_width_u64(uint64_t n) {
   int b = 0;
   while (b < 64 && (n >> b)) ++b;
@@ -203,9 +222,17 @@ struct svr_batch_plan {
   int rank_bits;
   int key_bits;  // widest group key (all groups sorted with this many passes)
   int64_t total_tiles, total_pixels;
+  // compositing schedule (svr_batch_plan_set_schedule)
+  int order_flags;        // bit 0: forward tiles largest first, bit 1: backward (else tile order)
+  int fwd_ctas_per_sm;    // resident CTAs per SM of the persistent launches (0 = as many as fit)
+  int bwd_ctas_per_sm;
+  int seg_small_n, seg_chunk;  // segment-sort buckets (svr_batch_plan_set_sort_buckets)
+  int tile_size;               // compositing tile size (8, 16 or 32), fixed at creation
+  int stage;                   // records staged per round (svr_batch_plan_set_staging)
   // workspace layout (byte offsets)
   size_t o_header, o_ndup, o_scan, o_bbox, o_quad, o_scan_tmp, o_rgbs, o_drgbs;
   size_t o_ka, o_kb, o_va, o_vb, o_sort_tmp, o_ranges, o_tile_last, o_ncontrib;
+  size_t o_okey, o_oval, o_order_fwd, o_order_bwd, o_order_tmp;
   size_t bytes;
 };
 
@@ -226,6 +253,11 @@ struct BatchPtrs {
   uint2* ranges;
   uint32_t* tile_last;
   uint32_t* ncontrib;
+  uint64_t* okey;       // [2][T] order sort keys
+  uint32_t* oval;       // [T] order sort input values
+  uint32_t* order_fwd;  // [T]
+  uint32_t* order_bwd;  // [T]
+  void* order_tmp;
 };
 
 BatchPtrs ptrs(const svr_batch_plan* p, void* ws) {
@@ -247,10 +279,26 @@ BatchPtrs ptrs(const svr_batch_plan* p, void* ws) {
   q.ranges = reinterpret_cast<uint2*>(b + p->o_ranges);
   q.tile_last = reinterpret_cast<uint32_t*>(b + p->o_tile_last);
   q.ncontrib = reinterpret_cast<uint32_t*>(b + p->o_ncontrib);
+  q.okey = reinterpret_cast<uint64_t*>(b + p->o_okey);
+  q.oval = reinterpret_cast<uint32_t*>(b + p->o_oval);
+  q.order_fwd = reinterpret_cast<uint32_t*>(b + p->o_order_fwd);
+  q.order_bwd = reinterpret_cast<uint32_t*>(b + p->o_order_bwd);
+  q.order_tmp = b + p->o_order_tmp;
   return q;
 }
 
-constexpr int kHeaderWords = 16 + 2 * kMaxViews;  // [0] count, [1] error, [16..] group segments
+// Header words: [0] instance count, [1] error word, [2] forward work counter,
+// [3] backward work counter, [4] tile count read by the order sort,
+// [16..] group segments.
+constexpr int kHeaderWords = 16 + 2 * kMaxViews;
+
+// Longest-first work order of all tiles into `order` (see tile_order_keys_kernel).
+void build_tile_order(const svr_batch_plan* p, const BatchPtrs& q, const uint32_t* tile_last, uint32_t* order,
+                      cudaStream_t stream) {
+  const uint32_t T = (uint32_t)p->total_tiles;
+  tile_order_keys_kernel<<<(T + 255) / 256, 256, 0, stream>>>(q.ranges, tile_last, T, q.okey, q.oval, q.header + 4);
+  launch_radix_sort(q.okey, q.oval, q.okey + T, order, nullptr, q.header + 4, T, 8, q.order_tmp, stream);
+}
 
 inline int check_last() { return cudaGetLastError() == cudaSuccess ? SVR_OK : SVR_ERR_CUDA; }
 
@@ -259,13 +307,17 @@ inline int check_last() { return cudaGetLastError() == cudaSuccess ? SVR_OK : SV
 extern "C" {
 
 int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_t capacity, int n_samp_per_vox,
-                          int max_level, svr_batch_plan** out, size_t* workspace_bytes) {
+                          int max_level, int tile_size, svr_batch_plan** out, size_t* workspace_bytes) {
   if (!out || !workspace_bytes || !cams || n_views < 1 || n_views > kMaxViews || P < 1 ||
       P >= (1ll << kVoxIdBits) || capacity < 0 || capacity > 0xffffffffll || n_samp_per_vox < 1 ||
-      n_samp_per_vox > kMaxSamples || max_level < 1 || max_level > kMaxLevels)
+      n_samp_per_vox > kMaxSamples || max_level < 1 || max_level > kMaxLevels ||
+      !(tile_size == 8 || tile_size == 16 || tile_size == 32))
     return SVR_ERR_SHAPE;
+  const int tile_shift = tile_size == 8 ? 3 : (tile_size == 16 ? 4 : 5);
   svr_batch_plan* p = new svr_batch_plan();
   memset(&p->vt, 0, sizeof(p->vt));
+  p->tile_size = tile_size;
+  p->stage = tile_size == 8 ? 64 : 256;
   p->V = n_views;
   p->P = P;
   p->cap = (size_t)capacity;
@@ -282,8 +334,9 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
     ViewParams& vp = p->vt.v[v];
     vp.W = c.width;
     vp.H = c.height;
-    vp.grid_x = (c.width + kTileX - 1) / kTileX;
-    vp.grid_y = (c.height + kTileY - 1) / kTileY;
+    vp.grid_x = (c.width + tile_size - 1) / tile_size;
+    vp.grid_y = (c.height + tile_size - 1) / tile_size;
+    vp.tile_shift = tile_shift;
     vp.tanfovx = c.tanfovx;
     vp.tanfovy = c.tanfovy;
     vp.cx = c.cx;
@@ -360,7 +413,20 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->o_ranges = take((size_t)tiles * 8);
   p->o_tile_last = take((size_t)tiles * 4);
   p->o_ncontrib = take((size_t)pix * 4);
+  p->o_okey = take((size_t)tiles * 16);
+  p->o_oval = take((size_t)tiles * 4);
+  p->o_order_fwd = take((size_t)tiles * 4);
+  p->o_order_bwd = take((size_t)tiles * 4);
+  p->o_order_tmp = take(sort_temp_bytes((size_t)tiles));
   p->bytes = align_up(off) + kAlign;
+  p->order_flags = 3;
+  p->fwd_ctas_per_sm = 0;
+  p->bwd_ctas_per_sm = 0;
+  p->seg_small_n = 512;
+  p->seg_chunk = 4096;
+  ensure_segsort_attributes();
+  ensure_fwd_batch_attributes();
+  ensure_bwd_batch_attributes();
   ensure_sort_attributes();
   *out = p;
   *workspace_bytes = p->bytes;
@@ -368,6 +434,31 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
 }
 
 void svr_batch_plan_destroy(svr_batch_plan* plan) { delete plan; }
+
+int svr_batch_plan_set_schedule(svr_batch_plan* p, int order_flags, int fwd_ctas_per_sm, int bwd_ctas_per_sm) {
+  if (!p || order_flags < 0 || order_flags > 3 || fwd_ctas_per_sm < 0 || bwd_ctas_per_sm < 0 ||
+      fwd_ctas_per_sm > 32 || bwd_ctas_per_sm > 32)
+    return SVR_ERR_SHAPE;
+  p->order_flags = order_flags;
+  p->fwd_ctas_per_sm = fwd_ctas_per_sm;
+  p->bwd_ctas_per_sm = bwd_ctas_per_sm;
+  return SVR_OK;
+}
+int svr_batch_plan_set_staging(svr_batch_plan* p, int stage) {
+  if (!p || !batch_tile_supported(p->tile_size, stage)) return SVR_ERR_SHAPE;
+  p->stage = stage;
+  return SVR_OK;
+}
+
+int svr_batch_plan_tile_size(const svr_batch_plan* p) { return p ? p->tile_size : 0; }
+
+int svr_batch_plan_set_sort_buckets(svr_batch_plan* p, int small_n, int chunk) {
+  if (!p || !seg_buckets_supported(small_n, chunk)) return SVR_ERR_SHAPE;
+  p->seg_small_n = small_n;
+  p->seg_chunk = chunk;
+  return SVR_OK;
+}
+
 int64_t svr_batch_plan_pixels(const svr_batch_plan* p) { return p ? p->total_pixels : 0; }
 int64_t svr_batch_plan_tiles(const svr_batch_plan* p) { return p ? p->total_tiles : 0; }
 int svr_batch_plan_groups(const svr_batch_plan* p) { return p ? p->gt.n : 0; }
@@ -448,7 +539,7 @@ int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, 
     }
     // the radix histograms in sort_tmp are dead here; the segment sort reuses it
     launch_tile_segment_sort(q.ranges, (int)p->total_tiles, q.ka, q.va, q.kb, q.vb, p->rank_bits, p->cap,
-                             q.sort_tmp, stream);
+                             q.sort_tmp, stream, p->seg_small_n, p->seg_chunk);
   }
   return check_last();
 }
@@ -462,8 +553,11 @@ int svr_batch_render(svr_batch_plan* p, void* ws, const float* vox_centers, cons
   VoxelArrays va{q.bbox, vox_centers, vox_lengths, geos_bf16 ? nullptr : (const float*)geos,
                  geos_bf16 ? (const __nv_bfloat16*)geos : nullptr, q.rgbs};
   FwdTileOut out{q.tile_last, q.ncontrib, out_color, nullptr, nullptr, out_T, nullptr};
+  const bool ordered = (p->order_flags & 1) != 0;
+  if (ordered) build_tile_order(p, q, nullptr, q.order_fwd, stream);
   launch_render_fwd_batch(p->vt, (int)p->total_tiles, q.ranges, p->cap > 0 ? q.vb : nullptr, va, (int)p->P,
-                          (size_t)p->P * 3, out, p->n_samp, false, false, false, false, stream);
+                          (size_t)p->P * 3, out, p->n_samp, p->tile_size, p->stage,
+                          ordered ? q.order_fwd : nullptr, q.header + 2, p->fwd_ctas_per_sm, stream);
   return check_last();
 }
 
@@ -480,8 +574,11 @@ int svr_batch_backward(svr_batch_plan* p, void* ws, const float* vox_centers, co
                  geos_bf16 ? (const __nv_bfloat16*)geos : nullptr, q.rgbs};
   BwdTileIn in{out_T, q.ncontrib, dL_dcolor, nullptr, nullptr, dL_dT, nullptr, nullptr, 0.f, 0.f, 0.f};
   BwdTileOut out{dL_dgeos, q.drgbs, subdiv, q.header + 1};
+  const bool ordered = (p->order_flags & 2) != 0;
+  if (ordered) build_tile_order(p, q, q.tile_last, q.order_bwd, stream);
   launch_render_bwd_batch(p->vt, (int)p->total_tiles, q.ranges, q.tile_last, p->cap > 0 ? q.vb : nullptr, va,
-                          (int)p->P, (size_t)p->P * 3, in, out, p->n_samp, false, false, false, stream);
+                          (int)p->P, (size_t)p->P * 3, in, out, p->n_samp, p->tile_size, p->stage,
+                          ordered ? q.order_bwd : nullptr, q.header + 3, p->bwd_ctas_per_sm, stream);
   return check_last();
 }
 

@@ -157,7 +157,7 @@ duplicate_kernel(const __grid_constant__ ViewTable views, int P,
     return;
   }
   int tx0, ty0, tx1, ty1;
-  bbox_tile_rect(bboxes[o], vp.grid_x, vp.grid_y, tx0, ty0, tx1, ty1);
+  bbox_tile_rect(bboxes[o], vp.grid_x, vp.grid_y, vp.tile_shift, tx0, ty0, tx1, ty1);
   const uint64_t path = (uint64_t)octpaths[idx];
   const uint32_t qb = quads[o];
   for (uint32_t q = 0; q < 8; ++q) {

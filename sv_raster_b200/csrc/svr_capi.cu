@@ -122,6 +122,7 @@ ViewParams make_view(const svr_camera& cam) {
   v.H = cam.height;
   v.grid_x = tiles_x(cam.width);
   v.grid_y = tiles_y(cam.height);
+  v.tile_shift = kTileShift;
   v.tanfovx = cam.tanfovx;
   v.tanfovy = cam.tanfovy;
   v.cx = cam.cx;

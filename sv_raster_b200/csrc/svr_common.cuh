@@ -16,10 +16,11 @@
 namespace svr {
 
 // Tile geometry of the parity path (config.h:14-15).  Contributor indices and
-// tile lists are only comparable with the reference at 16x16 tiles.
+// tile lists are only comparable with the reference at 16x16 tiles; the
+// batched path may use 8x8 or 32x32 tiles (ViewParams::tile_shift).
 constexpr int kTileX = 16;
 constexpr int kTileY = 16;
-constexpr int kTilePixels = kTileX * kTileY;
+constexpr int kTileShift = 4;
 
 constexpr int kMaxLevels = 16;                    // config.h:16
 constexpr float kMaxAlpha = 0.99999f;             // config.h:17
@@ -61,13 +62,13 @@ __device__ __forceinline__ uint32_t bb_xmax(uint2 b) { return b.y >> 16; }
 __device__ __forceinline__ uint32_t bb_ymax(uint2 b) { return b.y & 0xFFFFu; }
 
 // Tile rectangle covered by a packed bbox, clamped to the tile grid
-// (auxiliary.h:86-100).
-__device__ __forceinline__ void bbox_tile_rect(uint2 bb, int grid_x, int grid_y,
+// (auxiliary.h:86-100), for square tiles of 1 << shift pixels.
+__device__ __forceinline__ void bbox_tile_rect(uint2 bb, int grid_x, int grid_y, int shift,
                                                int& tx0, int& ty0, int& tx1, int& ty1) {
-  tx0 = max(0, min(grid_x - 1, (int)(bb_xmin(bb) / kTileX)));
-  ty0 = max(0, min(grid_y - 1, (int)(bb_ymin(bb) / kTileY)));
-  tx1 = max(0, min(grid_x - 1, (int)(bb_xmax(bb) / kTileX)));
-  ty1 = max(0, min(grid_y - 1, (int)(bb_ymax(bb) / kTileY)));
+  tx0 = max(0, min(grid_x - 1, (int)(bb_xmin(bb) >> shift)));
+  ty0 = max(0, min(grid_y - 1, (int)(bb_ymin(bb) >> shift)));
+  tx1 = max(0, min(grid_x - 1, (int)(bb_xmax(bb) >> shift)));
+  ty1 = max(0, min(grid_y - 1, (int)(bb_ymax(bb) >> shift)));
 }
 
 __device__ __forceinline__ bool pixel_in_bbox(uint32_t px, uint32_t py, uint2 bb) {
@@ -172,12 +173,5 @@ __device__ __forceinline__ float2 ray_box(float cx, float cy, float cz, float le
   return make_float2(fmaxf(fmaxf(nx, ny), nz), fminf(fminf(fx, fy), fz));
 }
 
-// Pixel placement inside a 16x16 tile: each warp owns an 8x4 micro-tile
-// (forward.cu:77-92).
-__device__ __forceinline__ void tile_pixel(int tid, int& lx, int& ly) {
-  const int warp = tid >> 5, lane = tid & 31;
-  lx = (warp & 1) * 8 + (lane & 7);
-  ly = (warp >> 1) * 4 + (lane >> 3);
-}
 
 }  // namespace svr

@@ -38,9 +38,14 @@ int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, co
 // bits [0, rank_bits), stably, into the same positions of (kb, vb); ka/va are
 // clobbered.  `cap` bounds the total instance count; temp holds
 // seg_sort_temp_bytes(cap, n_tiles) bytes.
+// small_n / chunk are the segment-size buckets (256|512|1024 and 2048|4096;
+// other values fall back to 512 / 4096).
 size_t seg_sort_temp_bytes(size_t cap, int n_tiles);
+bool seg_buckets_supported(int small_n, int chunk);
+void ensure_segsort_attributes();
 void launch_tile_segment_sort(const uint2* ranges, int n_tiles, uint64_t* ka, uint32_t* va, uint64_t* kb,
-                              uint32_t* vb, int rank_bits, size_t cap, void* temp, cudaStream_t stream);
+                              uint32_t* vb, int rank_bits, size_t cap, void* temp, cudaStream_t stream,
+                              int small_n = 512, int chunk = 4096);
 void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_start, const uint32_t* d_n, uint32_t cap,
                         int rank_bits, uint32_t tile_base, uint32_t n_tiles, uint2* ranges, cudaStream_t stream);
 
@@ -48,17 +53,28 @@ void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_start, const uin
 void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t* vals, const VoxelArrays& va,
                        const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
                        cudaStream_t stream);
+// Multi-view forms (no depth / distortion / normal outputs): persistent
+// grids taking tiles from `counter` (zeroed here) in the order of `order`
+// (identity when null); ctas_per_sm caps the resident CTAs per SM (0 = as
+// many as fit).  (tile, stage) must satisfy batch_tile_supported.
+bool batch_tile_supported(int tile, int stage);
+void ensure_fwd_batch_attributes();
+void ensure_bwd_batch_attributes();
 void launch_render_fwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* vals, const VoxelArrays& va, int P, size_t rgb_view_stride,
-                             const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
-                             cudaStream_t stream);
+                             const FwdTileOut& out, int ns, int tile, int stage, const uint32_t* order,
+                             uint32_t* counter, int ctas_per_sm, cudaStream_t stream);
 void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t* tile_last, const uint32_t* vals,
                        const VoxelArrays& va, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
                        bool dist, bool normal, cudaStream_t stream);
 void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
-                             size_t rgb_view_stride, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
-                             bool dist, bool normal, cudaStream_t stream);
+                             size_t rgb_view_stride, const BwdTileIn& in, const BwdTileOut& out, int ns, int tile,
+                             int stage, const uint32_t* order, uint32_t* counter, int ctas_per_sm,
+                             cudaStream_t stream);
+// Grid of a persistent launch: resident CTAs of `kernel` on this device
+// (capped at ctas_per_sm per SM when > 0), at most n_items.
+int persistent_grid(const void* kernel, int threads, size_t dyn_smem, int n_items, int ctas_per_sm);
 
 // svr_sh_adam.cu
 void launch_sh_eval(int deg, int n_idx, int P, int M, const int64_t* idx, const float* centers, const float* cam_pos,

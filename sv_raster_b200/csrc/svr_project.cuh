@@ -54,7 +54,7 @@ __device__ __forceinline__ Projection project_voxel(const ViewParams& vp, const 
   pr.bbox.x = (((uint32_t)lrintf(bx0)) << 16) | ((uint32_t)lrintf(by0));
   pr.bbox.y = (((uint32_t)lrintf(bx1)) << 16) | ((uint32_t)lrintf(by1));
   int tx0, ty0, tx1, ty1;
-  bbox_tile_rect(pr.bbox, vp.grid_x, vp.grid_y, tx0, ty0, tx1, ty1);
+  bbox_tile_rect(pr.bbox, vp.grid_x, vp.grid_y, vp.tile_shift, tx0, ty0, tx1, ty1);
   pr.n = (uint32_t)((1 + ty1 - ty0) * (1 + tx1 - tx0)) * (uint32_t)__popc(qbits);
   pr.quads = qbits;
   return pr;

@@ -1,9 +1,10 @@
 // Per-tile compositing shared by the forward and backward kernels.
 //
-// A CTA of 256 threads owns one 16x16 pixel tile; each warp owns an 8x4
-// micro-tile (forward.cu:77-92).  Voxel instances of the tile's sorted list
-// are staged into shared memory in batches of kBatch records (structure of
-// arrays, vector loads where the layout allows), then every warp builds a
+// A CTA of TS*TS threads owns one TSxTS pixel tile (16x16 on the plain path,
+// as the reference); each warp owns an 8x4 micro-tile (forward.cu:77-92).
+// Voxel instances of the tile's sorted list are staged into shared memory in
+// batches of SB records (structure of arrays, vector loads where the layout
+// allows), then every warp builds a
 // ballot mask of the staged records whose packed bbox overlaps its 8x4
 // micro-tile and whose camera quadrant matches a ray quadrant present in the
 // warp.  Lanes walk only those records, in list order, so every pixel sees
@@ -18,12 +19,40 @@
 
 namespace svr {
 
-constexpr int kBatch = 256;              // records staged per round (one per thread)
-constexpr int kGroups = kBatch / 32;     // 32-record ballot groups per round
-// Resident CTAs per SM the compositing kernels are register-bounded for
-// (occupancy vs spills, chosen from -Xptxas -v and ncu measurements).
+// Tile geometry and staging depth of a compositing kernel: TS x TS pixel
+// tiles (TS = 8, 16 or 32), one thread per pixel, warps laid out row-major as
+// 8x4 micro-tiles, SB records staged per round.
+template <int TS_, int SB_>
+struct TileCfg {
+  static constexpr int TS = TS_;
+  static constexpr int NT = TS * TS;      // threads per CTA
+  static constexpr int NW = NT / 32;      // warps per CTA
+  static constexpr int MX = TS / 8;       // micro-tiles per tile row
+  static constexpr int SB = SB_;          // records staged per round
+  static constexpr int GROUPS = SB / 32;  // 32-record ballot groups per round
+  static_assert(TS == 8 || TS == 16 || TS == 32, "tile size");
+  static_assert(SB % 32 == 0 && SB >= 32, "staging depth");
+};
+using PlainTile = TileCfg<16, 256>;  // the reference's 16x16 tiles (config.h:14-15)
+
+// Resident CTAs per SM the compositing kernels are register-bounded for at
+// 256 threads (occupancy vs spills, chosen from -Xptxas -v and ncu
+// measurements); other CTA sizes keep the same threads per SM.
 constexpr int kFwdMinBlocks = 5;
 constexpr int kBwdMinBlocks = 4;
+template <class CFG>
+constexpr int fwd_min_blocks() { return CFG::NT >= 1024 ? 1 : kFwdMinBlocks * 256 / CFG::NT; }
+template <class CFG>
+constexpr int bwd_min_blocks() { return CFG::NT >= 1024 ? 1 : kBwdMinBlocks * 256 / CFG::NT; }
+
+// Pixel of thread `tid` inside its tile: warp w owns micro-tile
+// (w % MX, w / MX) of 8x4 pixels, lanes row-major inside it.
+template <class CFG>
+__device__ __forceinline__ void tile_pixel_of(int tid, int& lx, int& ly) {
+  const int warp = tid >> 5, lane = tid & 31;
+  lx = (warp % CFG::MX) * 8 + (lane & 7);
+  ly = (warp / CFG::MX) * 4 + (lane >> 3);
+}
 
 // Voxel attributes of one view as the kernels read them.
 struct VoxelArrays {
@@ -40,16 +69,18 @@ struct VoxelArrays {
 // instead of once per pixel: (c - o) -/+ l/2, c - l/2 and 1/l.  Each is the
 // same IEEE operation on the same operands as in the per-pixel form, so the
 // per-pixel results are unchanged bit for bit.
+template <int SB>
 struct StageSmem {
-  uint4 box[kBatch];          // xmin, xmax - xmin, ymin, (ymax - ymin) | quadrant << 16
-  float4 slab_lo[kBatch];     // (c - o) - l/2 (xyz), 1/l (w)
-  float4 slab_hi[kBatch];     // (c - o) + l/2 (xyz), l (w)
-  float4 corner[kBatch];      // c - l/2 (xyz), voxel id as int bits (w)
-  float4 geo[kBatch][2];      // 8 corner densities
-  float4 rgb[kBatch];         // rgb (xyz)
+  uint4 box[SB];          // xmin, xmax - xmin, ymin, (ymax - ymin) | quadrant << 16
+  float4 slab_lo[SB];     // (c - o) - l/2 (xyz), 1/l (w)
+  float4 slab_hi[SB];     // (c - o) + l/2 (xyz), l (w)
+  float4 corner[SB];      // c - l/2 (xyz), voxel id as int bits (w)
+  float4 geo[SB][2];      // 8 corner densities
+  float4 rgb[SB];         // rgb (xyz)
 };
 
-__device__ __forceinline__ void stage_record(StageSmem& s, int slot, uint32_t val, const VoxelArrays& va,
+template <int SB>
+__device__ __forceinline__ void stage_record(StageSmem<SB>& s, int slot, uint32_t val, const VoxelArrays& va,
                                              float ox, float oy, float oz) {
   const uint32_t vid = val_vox_id(val);
   const uint2 bb = va.bboxes[vid];
@@ -89,7 +120,8 @@ __device__ __forceinline__ float2 staged_ray_box(const float4& lo, const float4&
 
 // Does staged record `slot` possibly touch a pixel of this warp's 8x4
 // micro-tile with a matching ray quadrant?
-__device__ __forceinline__ bool record_hits_warp(const StageSmem& s, int slot, uint32_t wx0, uint32_t wy0,
+template <int SB>
+__device__ __forceinline__ bool record_hits_warp(const StageSmem<SB>& s, int slot, uint32_t wx0, uint32_t wy0,
                                                  uint32_t quad_mask) {
   const uint4 b = s.box[slot];
   return b.x <= wx0 + 7u && b.x + b.y >= wx0 && b.z <= wy0 + 3u && b.z + (b.w & 0xFFFFu) >= wy0 &&
@@ -99,13 +131,15 @@ __device__ __forceinline__ bool record_hits_warp(const StageSmem& s, int slot, u
 // The reference's per-pixel test: pixel inside the packed bbox and ray
 // quadrant equal to the instance's (forward.cu:186), as two unsigned range
 // checks on the staged (min, extent) form.
-__device__ __forceinline__ bool record_hits_pixel(const StageSmem& s, int j, uint32_t px, uint32_t py,
+template <int SB>
+__device__ __forceinline__ bool record_hits_pixel(const StageSmem<SB>& s, int j, uint32_t px, uint32_t py,
                                                   uint32_t quad) {
   const uint4 b = s.box[j];
   return (px - b.x) <= b.y && (py - b.z) <= (b.w & 0xFFFFu) && (b.w >> 16) == quad;
 }
 
-__device__ __forceinline__ void load_geo(const StageSmem& s, int j, float g[8]) {
+template <int SB>
+__device__ __forceinline__ void load_geo(const StageSmem<SB>& s, int j, float g[8]) {
   const float4 a = s.geo[j][0], b = s.geo[j][1];
   g[0] = a.x; g[1] = a.y; g[2] = a.z; g[3] = a.w;
   g[4] = b.x; g[5] = b.y; g[6] = b.z; g[7] = b.w;

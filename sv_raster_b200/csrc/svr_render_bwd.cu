@@ -1,5 +1,8 @@
-// Backward compositing kernels (plain one-view grid and the multi-view form)
-// and their template dispatch.
+// Backward compositing kernels and their template dispatch: the plain
+// one-view grid (16x16 tiles) and the multi-view persistent form (tile size
+// and staging depth chosen per plan).
+#include <mutex>
+
 #include "svr_kernels.h"
 #include "svr_render_bwd.cuh"
 
@@ -15,25 +18,29 @@ struct BwdArgs {
   BwdTileOut out;
 };
 
+template <class CFG>
 struct BwdSmem {
-  StageSmem s;
-  float grad[kBatch * kGradStride];
+  StageSmem<CFG::SB> s;
+  float grad[CFG::SB * kGradStride];
   float c2w[12];
+  uint32_t item;
 };
 
 template <int NS, bool DEPTH, bool DIST, bool NORMAL>
-__global__ void __launch_bounds__(kBatch, kBwdMinBlocks)
+__global__ void __launch_bounds__(PlainTile::NT, kBwdMinBlocks)
 render_bwd_kernel(const __grid_constant__ BwdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  BwdSmem& sm = *reinterpret_cast<BwdSmem*>(smem_raw);
+  BwdSmem<PlainTile>& sm = *reinterpret_cast<BwdSmem<PlainTile>*>(smem_raw);
   if (threadIdx.x < 12) sm.c2w[threadIdx.x] = a.vp.c2w[threadIdx.x];
   __syncthreads();
   const int tile_x = blockIdx.x, tile_y = blockIdx.y;
   const int tile = tile_y * a.vp.grid_x + tile_x;
-  render_tile_bwd<NS, DEPTH, DIST, NORMAL>(a.vp, sm.c2w, tile_x, tile_y, a.ranges[tile], a.tile_last[tile], a.vals,
-                                           a.va, a.in, a.out, sm.s, sm.grad);
+  render_tile_bwd<PlainTile, NS, DEPTH, DIST, NORMAL>(a.vp, sm.c2w, tile_x, tile_y, a.ranges[tile], a.tile_last[tile],
+                                                      a.vals, a.va, a.in, a.out, sm.s, sm.grad);
 }
 
+// Multi-view form: a persistent grid over all views' tiles, in the order of
+// `order` (see the forward's FwdBatchArgs).
 struct BwdBatchArgs {
   ViewTable views;
   int n_items;
@@ -45,46 +52,50 @@ struct BwdBatchArgs {
   size_t rgb_view_stride;
   BwdTileIn in;    // base pointers, offset per view
   BwdTileOut out;  // dL_drgbs offset per view by rgb_view_stride
+  const uint32_t* order;  // [n_items] work order, or nullptr
+  uint32_t* counter;      // work counter, zero at launch
 };
 
-template <int NS, bool DEPTH, bool DIST, bool NORMAL>
-__global__ void __launch_bounds__(kBatch, kBwdMinBlocks)
+template <class CFG, int NS>
+__global__ void __launch_bounds__(CFG::NT, bwd_min_blocks<CFG>())
 render_bwd_batch_kernel(const __grid_constant__ BwdBatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  BwdSmem& sm = *reinterpret_cast<BwdSmem*>(smem_raw);
-  const int item = blockIdx.x;
-  if (item >= a.n_items) return;
-  const int view = view_of_tile(a.views, item);
-  const ViewParams& vp = a.views.v[view];
-  if (threadIdx.x < 12) sm.c2w[threadIdx.x] = vp.c2w[threadIdx.x];
-  __syncthreads();
-  const int local = item - (int)vp.tile_base;
-  const int tile_x = local % vp.grid_x, tile_y = local / vp.grid_x;
-  VoxelArrays va = a.va;
-  va.bboxes = a.va.bboxes + (size_t)view * a.P;
-  va.rgbs = a.va.rgbs + (size_t)view * a.rgb_view_stride;
-  BwdTileIn in = a.in;
-  const size_t pb = vp.pix_base;
-  in.T = a.in.T + pb;
-  in.n_contrib = a.in.n_contrib + pb;
-  in.dL_dcolor = a.in.dL_dcolor + 3 * pb;
-  in.dL_dT = a.in.dL_dT + pb;
-  if (DEPTH) in.dL_ddepth = a.in.dL_ddepth + 3 * pb;
-  if (NORMAL) in.dL_dnormal = a.in.dL_dnormal + 3 * pb;
-  if (a.in.gt_color) in.gt_color = a.in.gt_color + 3 * pb;
-  if (a.in.out_depth) in.out_depth = a.in.out_depth + 3 * pb;
-  BwdTileOut o = a.out;
-  o.dL_drgbs = a.out.dL_drgbs + (size_t)view * a.rgb_view_stride;
-  render_tile_bwd<NS, DEPTH, DIST, NORMAL>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.tile_last[item], a.vals, va,
-                                           in, o, sm.s, sm.grad);
+  BwdSmem<CFG>& sm = *reinterpret_cast<BwdSmem<CFG>*>(smem_raw);
+  for (;;) {
+    if (threadIdx.x == 0) sm.item = atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const uint32_t k = sm.item;
+    if (k >= (uint32_t)a.n_items) break;
+    const int item = a.order ? (int)a.order[k] : (int)k;
+    const int view = view_of_tile(a.views, item);
+    const ViewParams& vp = a.views.v[view];
+    if (threadIdx.x < 12) sm.c2w[threadIdx.x] = vp.c2w[threadIdx.x];
+    __syncthreads();
+    const int local = item - (int)vp.tile_base;
+    const int tile_x = local % vp.grid_x, tile_y = local / vp.grid_x;
+    VoxelArrays va = a.va;
+    va.bboxes = a.va.bboxes + (size_t)view * a.P;
+    va.rgbs = a.va.rgbs + (size_t)view * a.rgb_view_stride;
+    BwdTileIn in = a.in;
+    const size_t pb = vp.pix_base;
+    in.T = a.in.T + pb;
+    in.n_contrib = a.in.n_contrib + pb;
+    in.dL_dcolor = a.in.dL_dcolor + 3 * pb;
+    in.dL_dT = a.in.dL_dT + pb;
+    BwdTileOut o = a.out;
+    o.dL_drgbs = a.out.dL_drgbs + (size_t)view * a.rgb_view_stride;
+    render_tile_bwd<CFG, NS, false, false, false>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.tile_last[item],
+                                                  a.vals, va, in, o, sm.s, sm.grad);
+    __syncthreads();  // shared state (item, camera, staging) is free for the next tile
+  }
 }
 
-static_assert(sizeof(BwdSmem) <= 48 * 1024, "backward staging must fit the default shared-memory limit");
+static_assert(sizeof(BwdSmem<PlainTile>) <= 48 * 1024, "plain backward staging must fit the default limit");
 
-#define SVR_BWD_CASE(KERNEL, NS_, D_, T_, N_)                                    \
-  if (ns == NS_ && depth == D_ && dist == T_ && normal == N_) {                  \
-    KERNEL<NS_, D_, T_, N_><<<grid, kBatch, sizeof(BwdSmem), stream>>>(ARGS);    \
-    return;                                                                      \
+#define SVR_BWD_CASE(KERNEL, NS_, D_, T_, N_)                                                     \
+  if (ns == NS_ && depth == D_ && dist == T_ && normal == N_) {                                   \
+    KERNEL<NS_, D_, T_, N_><<<grid, PlainTile::NT, sizeof(BwdSmem<PlainTile>), stream>>>(args);   \
+    return;                                                                                       \
   }
 #define SVR_BWD_CASES_NS(KERNEL, NS_)                                                            \
   SVR_BWD_CASE(KERNEL, NS_, false, false, false) SVR_BWD_CASE(KERNEL, NS_, false, false, true) \
@@ -98,22 +109,62 @@ void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t
                        const VoxelArrays& va, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
                        bool dist, bool normal, cudaStream_t stream) {
   BwdArgs args{vp, ranges, tile_last, vals, va, in, out};
-  dim3 grid(vp.grid_x, vp.grid_y);
-#define ARGS args
+  const dim3 grid(vp.grid_x, vp.grid_y);
   SVR_BWD_SWITCH(render_bwd_kernel)
-#undef ARGS
+}
+
+template <class CFG, int NS>
+static void set_bwd_batch_attr() {
+  cudaFuncSetAttribute(render_bwd_batch_kernel<CFG, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(BwdSmem<CFG>));
+}
+
+template <class CFG>
+static void set_bwd_batch_attrs() {
+  set_bwd_batch_attr<CFG, 1>();
+  set_bwd_batch_attr<CFG, 2>();
+  set_bwd_batch_attr<CFG, 3>();
+}
+
+void ensure_bwd_batch_attributes() {
+  static std::once_flag flags[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  std::call_once(flags[dev], [] {
+    set_bwd_batch_attrs<TileCfg<16, 128>>();
+    set_bwd_batch_attrs<TileCfg<16, 256>>();
+    set_bwd_batch_attrs<TileCfg<16, 512>>();
+    set_bwd_batch_attrs<TileCfg<8, 64>>();
+    set_bwd_batch_attrs<TileCfg<32, 256>>();
+  });
+}
+
+template <class CFG>
+static void launch_bwd_batch_cfg(const BwdBatchArgs& args, int ns, int ctas_per_sm, cudaStream_t stream) {
+  const size_t smem = sizeof(BwdSmem<CFG>);
+  auto go = [&](auto kfn) {
+    const int grid = persistent_grid((const void*)kfn, CFG::NT, smem, args.n_items, ctas_per_sm);
+    kfn<<<grid, CFG::NT, smem, stream>>>(args);
+  };
+  if (ns == 1) go(render_bwd_batch_kernel<CFG, 1>);
+  else if (ns == 2) go(render_bwd_batch_kernel<CFG, 2>);
+  else go(render_bwd_batch_kernel<CFG, 3>);
 }
 
 void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
-                             size_t rgb_view_stride, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
-                             bool dist, bool normal, cudaStream_t stream) {
+                             size_t rgb_view_stride, const BwdTileIn& in, const BwdTileOut& out, int ns, int tile,
+                             int stage, const uint32_t* order, uint32_t* counter, int ctas_per_sm,
+                             cudaStream_t stream) {
   if (n_items <= 0) return;
-  BwdBatchArgs args{views, n_items, ranges, tile_last, vals, va, P, rgb_view_stride, in, out};
-  dim3 grid(n_items);
-#define ARGS args
-  SVR_BWD_SWITCH(render_bwd_batch_kernel)
-#undef ARGS
+  ensure_bwd_batch_attributes();
+  cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
+  const BwdBatchArgs args{views, n_items, ranges, tile_last, vals, va, P, rgb_view_stride, in, out, order, counter};
+  if (tile == 8) launch_bwd_batch_cfg<TileCfg<8, 64>>(args, ns, ctas_per_sm, stream);
+  else if (tile == 32) launch_bwd_batch_cfg<TileCfg<32, 256>>(args, ns, ctas_per_sm, stream);
+  else if (stage == 128) launch_bwd_batch_cfg<TileCfg<16, 128>>(args, ns, ctas_per_sm, stream);
+  else if (stage == 512) launch_bwd_batch_cfg<TileCfg<16, 512>>(args, ns, ctas_per_sm, stream);
+  else launch_bwd_batch_cfg<TileCfg<16, 256>>(args, ns, ctas_per_sm, stream);
 }
 
 }  // namespace svr

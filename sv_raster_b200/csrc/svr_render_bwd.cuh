@@ -1,4 +1,4 @@
-// Backward compositing of one 16x16 tile: walks the tile's list back to
+// Backward compositing of one tile: walks the tile's list back to
 // front from tile_last, recovers transmittance by division and accumulates
 // per-voxel gradients.
 //
@@ -89,22 +89,23 @@ __device__ __forceinline__ int warp_reduce_scatter12(float v[12], int lane) {
   return ((lane & 1) == 0 && slot < 12) ? slot : -1;
 }
 
-template <int NS, bool DEPTH, bool DIST, bool NORMAL>
+template <class CFG, int NS, bool DEPTH, bool DIST, bool NORMAL>
 __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const float* __restrict__ c2w_s, int tile_x,
                                                 int tile_y, uint2 range_raw, uint32_t tile_last,
                                                 const uint32_t* __restrict__ vals, const VoxelArrays& va,
-                                                const BwdTileIn& in, const BwdTileOut& out, StageSmem& s,
-                                                float* s_grad /*[kBatch*kGradStride]*/) {
+                                                const BwdTileIn& in, const BwdTileOut& out, StageSmem<CFG::SB>& s,
+                                                float* s_grad /*[SB*kGradStride]*/) {
+  constexpr int SB = CFG::SB;
   const int W = vp.W, H = vp.H;
   const int tid = threadIdx.x, lane = tid & 31;
   int lx, ly;
-  tile_pixel(tid, lx, ly);
-  const uint32_t px = tile_x * kTileX + lx, py = tile_y * kTileY + ly;
+  tile_pixel_of<CFG>(tid, lx, ly);
+  const uint32_t px = tile_x * CFG::TS + lx, py = tile_y * CFG::TS + ly;
   const uint32_t pix_id = (uint32_t)W * py + px;
   const bool inside = px < (uint32_t)W && py < (uint32_t)H;
   const PixelRay ray = make_pixel_ray((float)px, (float)py, W, H, vp.tanfovx, vp.tanfovy, vp.cx, vp.cy, c2w_s);
   const int warp = tid >> 5;
-  const uint32_t wx0 = tile_x * kTileX + (warp & 1) * 8, wy0 = tile_y * kTileY + (warp >> 1) * 4;
+  const uint32_t wx0 = tile_x * CFG::TS + (warp % CFG::MX) * 8, wy0 = tile_y * CFG::TS + (warp / CFG::MX) * 4;
 
   // Range check (replaces the __trap at backward.cu:122-133).
   if (tile_last > range_raw.y || range_raw.x > tile_last) {
@@ -150,21 +151,22 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
     prefix_w = 1.f - T_final;
   }
 
-  for (int i = tid; i < kBatch * kGradStride; i += kBatch) s_grad[i] = 0.f;
+  for (int i = tid; i < SB * kGradStride; i += CFG::NT) s_grad[i] = 0.f;
   // Largest contributor count of this warp: records at or beyond it are skipped by every lane.
   const uint32_t warp_lc = __reduce_max_sync(0xffffffffu, last_contrib);
   const uint32_t quad_mask = __reduce_or_sync(0xffffffffu, inside ? (1u << ray.quad) : 0u);
 
-  const int rounds = (todo_total + kBatch - 1) / kBatch;
+  const int rounds = (todo_total + SB - 1) / SB;
   for (int r = 0; r < rounds; ++r) {
     __syncthreads();
-    const int base = r * kBatch;                     // records [base, base+n_here) from the back
-    const int n_here = min(kBatch, todo_total - base);
-    if (tid < n_here) stage_record(s, tid, vals[range.y - base - tid - 1], va, ray.ox, ray.oy, ray.oz);
+    const int base = r * SB;                     // records [base, base+n_here) from the back
+    const int n_here = min(SB, todo_total - base);
+    for (int i = tid; i < n_here; i += CFG::NT)
+      stage_record(s, i, vals[range.y - base - i - 1], va, ray.ox, ray.oy, ray.oz);
     __syncthreads();
 
     // Position (relative to range.x) of staged slot j is todo_total - base - j - 1.
-    for (int g = 0; g < kGroups && g * 32 < n_here; ++g) {
+    for (int g = 0; g < CFG::GROUPS && g * 32 < n_here; ++g) {
       const int slot = g * 32 + lane;
       const uint32_t pos = (uint32_t)(todo_total - base - slot - 1);
       const bool hit = slot < n_here && pos < warp_lc && record_hits_warp(s, slot, wx0, wy0, quad_mask);
@@ -359,13 +361,13 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
     }
     __syncthreads();
     // Flush this batch's accumulators: one set of reductions per (voxel, tile).
-    if (tid < n_here) {
-      float* acc = s_grad + tid * kGradStride;
+    for (int t = tid; t < n_here; t += CFG::NT) {
+      float* acc = s_grad + t * kGradStride;
       float gsum = 0.f;
 #pragma unroll
       for (int c = 0; c < 12; ++c) gsum += fabsf(acc[c]);
       if (gsum != 0.f) {
-        const uint32_t vid = (uint32_t)__float_as_int(s.corner[tid].w);
+        const uint32_t vid = (uint32_t)__float_as_int(s.corner[t].w);
 #pragma unroll
         for (int c = 0; c < 8; ++c) atomicAdd(out.dL_dgeos + 8 * (size_t)vid + c, acc[c]);
 #pragma unroll

@@ -1,10 +1,25 @@
-// Forward compositing kernels (plain one-view grid and the multi-view form,
-// one CTA per (view, tile) of every view in a single launch) and their
-// template dispatch.
+// Forward compositing kernels and their template dispatch: the plain
+// one-view grid (one CTA per 16x16 tile, the reference's layout) and the
+// multi-view form (one persistent launch over every (view, tile) of all
+// views, tile size and staging depth chosen per plan).
+#include <mutex>
+
 #include "svr_kernels.h"
 #include "svr_render_fwd.cuh"
 
 namespace svr {
+
+int persistent_grid(const void* kernel, int threads, size_t dyn_smem, int n_items, int ctas_per_sm) {
+  int dev = 0, sms = 1, per_sm = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, dyn_smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  if (ctas_per_sm > 0) per_sm = std::min(per_sm, ctas_per_sm);
+  const long long g = (long long)sms * per_sm;
+  return (int)std::max(1LL, std::min<long long>(g, (long long)n_items));
+}
 
 struct FwdArgs {
   ViewParams vp;
@@ -15,20 +30,25 @@ struct FwdArgs {
 };
 
 template <int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
-__global__ void __launch_bounds__(kBatch, kFwdMinBlocks)
+__global__ void __launch_bounds__(PlainTile::NT, kFwdMinBlocks)
 render_fwd_kernel(const __grid_constant__ FwdArgs a) {
-  __shared__ StageSmem s;
+  __shared__ StageSmem<PlainTile::SB> s;
   __shared__ float s_c2w[12];
-  __shared__ uint32_t s_red[kBatch / 32];
+  __shared__ uint32_t s_red[PlainTile::NW];
   if (threadIdx.x < 12) s_c2w[threadIdx.x] = a.vp.c2w[threadIdx.x];
   __syncthreads();
   const int tile_x = blockIdx.x, tile_y = blockIdx.y;
   const uint2 range = a.ranges[tile_y * a.vp.grid_x + tile_x];
-  render_tile_fwd<NS, DEPTH, DIST, NORMAL, MAXW>(a.vp, s_c2w, tile_x, tile_y, range, a.vals, a.va, a.out, s, s_red);
+  render_tile_fwd<PlainTile, NS, DEPTH, DIST, NORMAL, MAXW>(a.vp, s_c2w, tile_x, tile_y, range, a.vals, a.va, a.out,
+                                                            s, s_red);
 }
 
-// Multi-view form: one CTA per (view, tile) work item, items laid out view by
-// view.  Per-view arrays are addressed through the view's tile/pixel bases.
+// Multi-view form: a persistent grid over the (view, tile) work items of all
+// views, items laid out view by view.  CTAs take items from a device counter
+// in the order of `order` (largest tiles first when the caller ranks them by
+// cost; identity when null), so the heavy-tailed tile costs do not leave a
+// tail of late large tiles.  Per-view arrays are addressed through the view's
+// tile/pixel bases.
 struct FwdBatchArgs {
   ViewTable views;
   int n_items;                 // total tiles over all views
@@ -38,42 +58,54 @@ struct FwdBatchArgs {
   int P;
   size_t rgb_view_stride;      // elements between views in rgbs (0 = shared)
   FwdTileOut out;              // base pointers; offset per view
+  const uint32_t* order;       // [n_items] work order, or nullptr
+  uint32_t* counter;           // work counter, zero at launch
 };
 
-template <int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
-__global__ void __launch_bounds__(kBatch, kFwdMinBlocks)
+template <class CFG>
+struct FwdBatchSmem {
+  StageSmem<CFG::SB> s;
+  float c2w[12];
+  uint32_t red[CFG::NW];
+  uint32_t item;
+};
+
+template <class CFG, int NS>
+__global__ void __launch_bounds__(CFG::NT, fwd_min_blocks<CFG>())
 render_fwd_batch_kernel(const __grid_constant__ FwdBatchArgs a) {
-  __shared__ StageSmem s;
-  __shared__ float s_c2w[12];
-  __shared__ uint32_t s_red[kBatch / 32];
-  const int item = blockIdx.x;
-  if (item >= a.n_items) return;
-  const int view = view_of_tile(a.views, item);
-  const ViewParams& vp = a.views.v[view];
-  if (threadIdx.x < 12) s_c2w[threadIdx.x] = vp.c2w[threadIdx.x];
-  __syncthreads();
-  const int local = item - (int)vp.tile_base;
-  const int tile_x = local % vp.grid_x, tile_y = local / vp.grid_x;
-  const uint2 range = a.ranges[item];
-  VoxelArrays va = a.va;
-  va.bboxes = a.va.bboxes + (size_t)view * a.P;
-  va.rgbs = a.va.rgbs + (size_t)view * a.rgb_view_stride;
-  FwdTileOut o = a.out;
-  o.tile_last = a.out.tile_last + vp.tile_base;
-  o.n_contrib = a.out.n_contrib + vp.pix_base;
-  o.color = a.out.color + 3 * (size_t)vp.pix_base;
-  o.T = a.out.T + vp.pix_base;
-  if (DEPTH || DIST) o.depth = a.out.depth + 3 * (size_t)vp.pix_base;
-  if (NORMAL) o.normal = a.out.normal + 3 * (size_t)vp.pix_base;
-  if (MAXW) o.max_w = a.out.max_w + (size_t)view * a.P;
-  render_tile_fwd<NS, DEPTH, DIST, NORMAL, MAXW>(vp, s_c2w, tile_x, tile_y, range, a.vals, va, o, s, s_red);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FwdBatchSmem<CFG>& sm = *reinterpret_cast<FwdBatchSmem<CFG>*>(smem_raw);
+  for (;;) {
+    if (threadIdx.x == 0) sm.item = atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const uint32_t k = sm.item;
+    if (k >= (uint32_t)a.n_items) break;
+    const int item = a.order ? (int)a.order[k] : (int)k;
+    const int view = view_of_tile(a.views, item);
+    const ViewParams& vp = a.views.v[view];
+    if (threadIdx.x < 12) sm.c2w[threadIdx.x] = vp.c2w[threadIdx.x];
+    __syncthreads();
+    const int local = item - (int)vp.tile_base;
+    const int tile_x = local % vp.grid_x, tile_y = local / vp.grid_x;
+    VoxelArrays va = a.va;
+    va.bboxes = a.va.bboxes + (size_t)view * a.P;
+    va.rgbs = a.va.rgbs + (size_t)view * a.rgb_view_stride;
+    FwdTileOut o = a.out;
+    o.tile_last = a.out.tile_last + vp.tile_base;
+    o.n_contrib = a.out.n_contrib + vp.pix_base;
+    o.color = a.out.color + 3 * (size_t)vp.pix_base;
+    o.T = a.out.T + vp.pix_base;
+    render_tile_fwd<CFG, NS, false, false, false, false>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.vals, va, o,
+                                                         sm.s, sm.red);
+    __syncthreads();  // shared state (item, camera, staging) is free for the next tile
+  }
 }
 
 #define SVR_FWD_DISPATCH(KERNEL, GRID, STREAM, ...)                                                   \
   do {                                                                                                \
     const int _ns = ns;                                                                               \
     const bool _d = depth, _t = dist, _n = normal, _m = maxw;                                         \
-    auto _launch = [&](auto kfn) { kfn<<<GRID, kBatch, 0, STREAM>>>(__VA_ARGS__); };                  \
+    auto _launch = [&](auto kfn) { kfn<<<GRID, PlainTile::NT, 0, STREAM>>>(__VA_ARGS__); };           \
     (void)_launch;                                                                                    \
     SVR_FWD_SWITCH(KERNEL, _ns, _d, _t, _n, _m);                                                      \
   } while (0)
@@ -101,18 +133,67 @@ void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t
                        const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
                        cudaStream_t stream) {
   FwdArgs args{vp, ranges, vals, va, out};
-  dim3 grid(vp.grid_x, vp.grid_y);
+  const dim3 grid(vp.grid_x, vp.grid_y);
   SVR_FWD_DISPATCH(render_fwd_kernel, grid, stream, args);
+}
+
+// Batched tile configurations: (tile size, staging depth).
+bool batch_tile_supported(int tile, int stage) {
+  return (tile == 16 && (stage == 128 || stage == 256 || stage == 512)) || (tile == 8 && stage == 64) ||
+         (tile == 32 && stage == 256);
+}
+
+template <class CFG, int NS>
+static void set_fwd_batch_attr() {
+  cudaFuncSetAttribute(render_fwd_batch_kernel<CFG, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(FwdBatchSmem<CFG>));
+}
+
+template <class CFG>
+static void set_fwd_batch_attrs() {
+  set_fwd_batch_attr<CFG, 1>();
+  set_fwd_batch_attr<CFG, 2>();
+  set_fwd_batch_attr<CFG, 3>();
+}
+
+void ensure_fwd_batch_attributes() {
+  static std::once_flag flags[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  std::call_once(flags[dev], [] {
+    set_fwd_batch_attrs<TileCfg<16, 128>>();
+    set_fwd_batch_attrs<TileCfg<16, 256>>();
+    set_fwd_batch_attrs<TileCfg<16, 512>>();
+    set_fwd_batch_attrs<TileCfg<8, 64>>();
+    set_fwd_batch_attrs<TileCfg<32, 256>>();
+  });
+}
+
+template <class CFG>
+static void launch_fwd_batch_cfg(const FwdBatchArgs& args, int ns, int ctas_per_sm, cudaStream_t stream) {
+  const size_t smem = sizeof(FwdBatchSmem<CFG>);
+  auto go = [&](auto kfn) {
+    const int grid = persistent_grid((const void*)kfn, CFG::NT, smem, args.n_items, ctas_per_sm);
+    kfn<<<grid, CFG::NT, smem, stream>>>(args);
+  };
+  if (ns == 1) go(render_fwd_batch_kernel<CFG, 1>);
+  else if (ns == 2) go(render_fwd_batch_kernel<CFG, 2>);
+  else go(render_fwd_batch_kernel<CFG, 3>);
 }
 
 void launch_render_fwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* vals, const VoxelArrays& va, int P, size_t rgb_view_stride,
-                             const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
-                             cudaStream_t stream) {
+                             const FwdTileOut& out, int ns, int tile, int stage, const uint32_t* order,
+                             uint32_t* counter, int ctas_per_sm, cudaStream_t stream) {
   if (n_items <= 0) return;
-  FwdBatchArgs args{views, n_items, ranges, vals, va, P, rgb_view_stride, out};
-  dim3 grid(n_items);
-  SVR_FWD_DISPATCH(render_fwd_batch_kernel, grid, stream, args);
+  ensure_fwd_batch_attributes();
+  cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
+  const FwdBatchArgs args{views, n_items, ranges, vals, va, P, rgb_view_stride, out, order, counter};
+  if (tile == 8) launch_fwd_batch_cfg<TileCfg<8, 64>>(args, ns, ctas_per_sm, stream);
+  else if (tile == 32) launch_fwd_batch_cfg<TileCfg<32, 256>>(args, ns, ctas_per_sm, stream);
+  else if (stage == 128) launch_fwd_batch_cfg<TileCfg<16, 128>>(args, ns, ctas_per_sm, stream);
+  else if (stage == 512) launch_fwd_batch_cfg<TileCfg<16, 512>>(args, ns, ctas_per_sm, stream);
+  else launch_fwd_batch_cfg<TileCfg<16, 256>>(args, ns, ctas_per_sm, stream);
 }
 
 }  // namespace svr

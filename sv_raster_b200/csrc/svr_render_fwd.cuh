@@ -1,4 +1,4 @@
-// Forward compositing of one 16x16 tile: front-to-back alpha blending of the
+// Forward compositing of one tile: front-to-back alpha blending of the
 // tile's sorted voxel instances with trilinear density quadrature.
 //
 // Per-pixel arithmetic mirrors FORWARD::renderCUDA (forward.cu:39-392):
@@ -25,22 +25,23 @@ struct FwdTileOut {
   float* max_w;          // [P] or nullptr
 };
 
-template <int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
+template <class CFG, int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
 __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const float* __restrict__ c2w_s, int tile_x,
                                                 int tile_y, uint2 range, const uint32_t* __restrict__ vals,
-                                                const VoxelArrays& va, const FwdTileOut& out, StageSmem& s,
-                                                uint32_t* s_red) {
+                                                const VoxelArrays& va, const FwdTileOut& out,
+                                                StageSmem<CFG::SB>& s, uint32_t* s_red /*[CFG::NW]*/) {
+  constexpr int SB = CFG::SB;
   const int W = vp.W, H = vp.H;
   const int tid = threadIdx.x;
   const int tile_id = tile_y * vp.grid_x + tile_x;
   int lx, ly;
-  tile_pixel(tid, lx, ly);
-  const uint32_t px = tile_x * kTileX + lx, py = tile_y * kTileY + ly;
+  tile_pixel_of<CFG>(tid, lx, ly);
+  const uint32_t px = tile_x * CFG::TS + lx, py = tile_y * CFG::TS + ly;
   const uint32_t pix_id = (uint32_t)W * py + px;
   const bool inside = px < (uint32_t)W && py < (uint32_t)H;
   const PixelRay ray = make_pixel_ray((float)px, (float)py, W, H, vp.tanfovx, vp.tanfovy, vp.cx, vp.cy, c2w_s);
   const int warp = tid >> 5;
-  const uint32_t wx0 = tile_x * kTileX + (warp & 1) * 8, wy0 = tile_y * kTileY + (warp >> 1) * 4;
+  const uint32_t wx0 = tile_x * CFG::TS + (warp % CFG::MX) * 8, wy0 = tile_y * CFG::TS + (warp / CFG::MX) * 4;
 
   bool done = !inside;
   float T = 1.f;
@@ -52,18 +53,19 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
   uint32_t last_contrib = 0;
 
   const int todo_total = (int)(range.y - range.x);
-  const int rounds = (todo_total + kBatch - 1) / kBatch;
+  const int rounds = (todo_total + SB - 1) / SB;
   for (int r = 0; r < rounds; ++r) {
     // All pixels finished: stop (also the barrier that frees the staging buffer).
-    if (__syncthreads_count(done) == kBatch) break;
-    const int base = r * kBatch;
-    const int n_here = min(kBatch, todo_total - base);
-    if (tid < n_here) stage_record(s, tid, vals[range.x + base + tid], va, ray.ox, ray.oy, ray.oz);
+    if (__syncthreads_count(done) == CFG::NT) break;
+    const int base = r * SB;
+    const int n_here = min(SB, todo_total - base);
+    for (int i = tid; i < n_here; i += CFG::NT)
+      stage_record(s, i, vals[range.x + base + i], va, ray.ox, ray.oy, ray.oz);
     __syncthreads();
 
     const uint32_t quad_mask = __reduce_or_sync(0xffffffffu, done ? 0u : (1u << ray.quad));
     if (quad_mask == 0u) continue;  // whole warp finished
-    for (int g = 0; g < kGroups && g * 32 < n_here; ++g) {
+    for (int g = 0; g < CFG::GROUPS && g * 32 < n_here; ++g) {
       const int slot = g * 32 + (tid & 31);
       const bool hit = slot < n_here && record_hits_warp(s, slot, wx0, wy0, quad_mask);
       uint32_t m = __ballot_sync(0xffffffffu, hit);
@@ -211,7 +213,7 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
   if (tid == 0) {
     uint32_t m = 0;
 #pragma unroll
-    for (int w = 0; w < kBatch / 32; ++w) m = max(m, s_red[w]);
+    for (int w = 0; w < CFG::NW; ++w) m = max(m, s_red[w]);
     out.tile_last[tile_id] = range.x + m;
   }
 }

@@ -12,11 +12,11 @@
 // thousands and most of all instances), so the work is split by size:
 //
 //   plan    one thread per tile writes a work list: segments of at most
-//           kSmallN instances, and chunks of at most kChunk instances of the
-//           larger segments (chunk c of a segment starts at c * kChunk);
+//           small_n instances, and chunks of at most `chunk` instances of the
+//           larger segments (chunk c of a segment starts at c * chunk);
 //   small   one 128-thread CTA per small segment: LSD 8-bit passes in shared
 //           memory, result to (kb, vb);
-//   chunk   one 512-thread CTA per chunk: the same passes on up to kChunk
+//   chunk   one 512-thread CTA per chunk: the same passes on up to `chunk`
 //           items; a segment of one chunk is final (to kb, vb), otherwise the
 //           sorted run is written back in place (ka, va);
 //   merge   one CTA per run of a multi-run segment: an item's final place is
@@ -37,11 +37,18 @@
 
 namespace svr {
 
-constexpr int kSmallN = 512;     // largest segment handled by the small kernel
+// Segment-size buckets (chosen per plan; the defaults are 512 and 4096):
+// segments of at most small_n instances go to the small kernel, longer ones
+// are cut into runs of `chunk` instances.
 constexpr int kSmallThreads = 128;
-constexpr int kChunk = 4096;     // largest run sorted by one chunk CTA
 constexpr int kChunkThreads = 512;
 constexpr int kMergeThreads = 512;
+constexpr int kMinSmallN = 256;  // smallest supported small_n / chunk: they size the work lists
+constexpr int kMinChunk = 2048;
+
+bool seg_buckets_supported(int small_n, int chunk) {
+  return (small_n == 256 || small_n == 512 || small_n == 1024) && (chunk == 2048 || chunk == 4096);
+}
 
 // Shared memory of an LSD sort of up to CAP keys by NT threads.  The
 // payload moved with each key is its 16-bit index in the input; values are
@@ -147,22 +154,26 @@ struct SegLists {
   uint2* small;  // (start, n)
   uint4* chunk;  // (chunk start, chunk n, segment start, segment n)
   uint32_t small_cap, chunk_cap;
+  uint32_t small_n, chunk_n;  // bucket limits of this launch
 };
 
 inline size_t seg_align(size_t x) { return (x + 255) / 256 * 256; }
 
+// Chunk-list capacity for the smallest supported buckets (an upper bound for all).
 inline uint32_t seg_chunk_cap(size_t cap, int n_tiles) {
-  const size_t big_tiles = std::min<size_t>((size_t)n_tiles, cap / (kSmallN + 1));
-  return (uint32_t)(cap / kChunk + big_tiles + 1);
+  const size_t big_tiles = std::min<size_t>((size_t)n_tiles, cap / (kMinSmallN + 1));
+  return (uint32_t)(cap / kMinChunk + big_tiles + 1);
 }
 
 size_t seg_sort_temp_bytes(size_t cap, int n_tiles) {
   return 256 + seg_align((size_t)n_tiles * sizeof(uint2)) + (size_t)seg_chunk_cap(cap, n_tiles) * sizeof(uint4);
 }
 
-static SegLists seg_lists(void* temp, size_t cap, int n_tiles) {
+static SegLists seg_lists(void* temp, size_t cap, int n_tiles, int small_n, int chunk) {
   char* b = static_cast<char*>(temp);
   SegLists L;
+  L.small_n = (uint32_t)small_n;
+  L.chunk_n = (uint32_t)chunk;
   L.counters = reinterpret_cast<uint32_t*>(b);
   L.small = reinterpret_cast<uint2*>(b + 256);
   L.chunk = reinterpret_cast<uint4*>(b + 256 + seg_align((size_t)n_tiles * sizeof(uint2)));
@@ -181,8 +192,8 @@ seg_plan_kernel(const uint2* __restrict__ ranges, int n_tiles, SegLists L) {
     start = r.x;
     n = r.y - r.x;
   }
-  const bool small = n > 0 && n <= (uint32_t)kSmallN;
-  const uint32_t nch = n > (uint32_t)kSmallN ? (n + kChunk - 1) / kChunk : 0u;
+  const bool small = n > 0 && n <= L.small_n;
+  const uint32_t nch = n > L.small_n ? (n + L.chunk_n - 1) / L.chunk_n : 0u;
   // warp-aggregated reservations in both lists
   const uint32_t sball = __ballot_sync(0xffffffffu, small);
   uint32_t inc = nch;
@@ -205,14 +216,15 @@ seg_plan_kernel(const uint2* __restrict__ ranges, int n_tiles, SegLists L) {
   }
   for (uint32_t c = 0; c < nch; ++c) {
     const uint32_t e = cbase + inc - nch + c;
-    if (e < L.chunk_cap) L.chunk[e] = make_uint4(start + c * kChunk, min((uint32_t)kChunk, n - c * kChunk), start, n);
+    if (e < L.chunk_cap) L.chunk[e] = make_uint4(start + c * L.chunk_n, min(L.chunk_n, n - c * L.chunk_n), start, n);
   }
 }
 
+template <int SMALL_N>
 __global__ void __launch_bounds__(kSmallThreads)
 seg_small_kernel(SegLists L, const uint64_t* __restrict__ ka, const uint32_t* __restrict__ va,
                  uint64_t* __restrict__ kb, uint32_t* __restrict__ vb, int rank_bits) {
-  __shared__ SortSmem<kSmallThreads, kSmallN> sm;
+  __shared__ SortSmem<kSmallThreads, SMALL_N> sm;
   const uint32_t count = min(L.counters[0], L.small_cap);
   for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
     const uint2 s = L.small[e];
@@ -231,13 +243,16 @@ seg_small_kernel(SegLists L, const uint64_t* __restrict__ ka, const uint32_t* __
   }
 }
 
-using ChunkSmem = SortSmem<kChunkThreads, kChunk>;
+template <int CHUNK>
+using ChunkSmem = SortSmem<kChunkThreads, CHUNK>;
 
+template <int CHUNK>
 __global__ void __launch_bounds__(kChunkThreads, 2)
 seg_chunk_kernel(SegLists L, uint64_t* __restrict__ ka, uint32_t* __restrict__ va, uint64_t* __restrict__ kb,
                  uint32_t* __restrict__ vb, int rank_bits) {
+  constexpr int kChunk = CHUNK;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  ChunkSmem& sm = *reinterpret_cast<ChunkSmem*>(smem_raw);
+  ChunkSmem<CHUNK>& sm = *reinterpret_cast<ChunkSmem<CHUNK>*>(smem_raw);
   const uint32_t count = min(L.counters[1], L.chunk_cap);
   for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
     const uint4 c = L.chunk[e];
@@ -275,17 +290,20 @@ seg_chunk_kernel(SegLists L, uint64_t* __restrict__ ka, uint32_t* __restrict__ v
   }
 }
 
+template <int CHUNK>
 struct MergeSmem {
-  uint64_t own[kChunk];
-  uint64_t other[kChunk];
-  uint32_t cnt[kChunk];  // per own item: keys of the other runs ordered before it
+  uint64_t own[CHUNK];
+  uint64_t other[CHUNK];
+  uint32_t cnt[CHUNK];  // per own item: keys of the other runs ordered before it
 };
 
 // Merge-path co-ranking of run `own` (index r) against run `other` (index
 // s): thread t walks the merged order's outputs [t * per, (t + 1) * per) and,
 // for every own item it passes, adds the number of other-run keys before it.
 // On equal keys the earlier run comes first.
-__device__ __forceinline__ void corank_run(MergeSmem& sm, uint32_t n_own, uint32_t n_oth, bool own_first_on_tie) {
+template <int CHUNK>
+__device__ __forceinline__ void corank_run(MergeSmem<CHUNK>& sm, uint32_t n_own, uint32_t n_oth,
+                                           bool own_first_on_tie) {
   const uint32_t total = n_own + n_oth;
   const uint32_t per = (total + kMergeThreads - 1) / kMergeThreads;
   const uint32_t d0 = min(total, threadIdx.x * per), d1 = min(total, d0 + per);
@@ -311,11 +329,13 @@ __device__ __forceinline__ void corank_run(MergeSmem& sm, uint32_t n_own, uint32
   }
 }
 
+template <int CHUNK>
 __global__ void __launch_bounds__(kMergeThreads)
 seg_merge_kernel(SegLists L, const uint64_t* __restrict__ ka, const uint32_t* __restrict__ va,
                  uint64_t* __restrict__ kb, uint32_t* __restrict__ vb) {
+  constexpr int kChunk = CHUNK;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  MergeSmem& sm = *reinterpret_cast<MergeSmem*>(smem_raw);
+  MergeSmem<CHUNK>& sm = *reinterpret_cast<MergeSmem<CHUNK>*>(smem_raw);
   const uint32_t count = min(L.counters[1], L.chunk_cap);
   const int tid = threadIdx.x;
   for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
@@ -347,13 +367,19 @@ seg_merge_kernel(SegLists L, const uint64_t* __restrict__ ka, const uint32_t* __
   }
 }
 
-static void ensure_segsort_attributes() {
+void ensure_segsort_attributes() {
   static std::once_flag flags[64];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
   std::call_once(flags[dev], [] {
-    cudaFuncSetAttribute(seg_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ChunkSmem));
-    cudaFuncSetAttribute(seg_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MergeSmem));
+    cudaFuncSetAttribute(seg_chunk_kernel<2048>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(ChunkSmem<2048>));
+    cudaFuncSetAttribute(seg_chunk_kernel<4096>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(ChunkSmem<4096>));
+    cudaFuncSetAttribute(seg_merge_kernel<2048>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(MergeSmem<2048>));
+    cudaFuncSetAttribute(seg_merge_kernel<4096>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(MergeSmem<4096>));
   });
 }
 
@@ -364,20 +390,35 @@ static int sm_count() {
   return n > 0 ? n : 148;
 }
 
+template <int CHUNK>
+static void launch_chunk_and_merge(const SegLists& L, int sms, uint64_t* ka, uint32_t* va, uint64_t* kb,
+                                   uint32_t* vb, int rank_bits, cudaStream_t stream) {
+  const int chunk_grid = (int)std::min<int64_t>(L.chunk_cap, (int64_t)sms * 2);
+  seg_chunk_kernel<CHUNK><<<chunk_grid, kChunkThreads, sizeof(ChunkSmem<CHUNK>), stream>>>(L, ka, va, kb, vb,
+                                                                                          rank_bits);
+  const int merge_grid = (int)std::min<int64_t>(L.chunk_cap, (int64_t)sms * 2);
+  seg_merge_kernel<CHUNK><<<merge_grid, kMergeThreads, sizeof(MergeSmem<CHUNK>), stream>>>(L, ka, va, kb, vb);
+}
+
 void launch_tile_segment_sort(const uint2* ranges, int n_tiles, uint64_t* ka, uint32_t* va, uint64_t* kb,
-                              uint32_t* vb, int rank_bits, size_t cap, void* temp, cudaStream_t stream) {
+                              uint32_t* vb, int rank_bits, size_t cap, void* temp, cudaStream_t stream,
+                              int small_n, int chunk) {
   if (n_tiles <= 0 || cap == 0) return;
+  if (!seg_buckets_supported(small_n, chunk)) {
+    small_n = 512;
+    chunk = 4096;
+  }
   ensure_segsort_attributes();
-  const SegLists L = seg_lists(temp, cap, n_tiles);
+  const SegLists L = seg_lists(temp, cap, n_tiles, small_n, chunk);
   cudaMemsetAsync(L.counters, 0, 2 * sizeof(uint32_t), stream);
   seg_plan_kernel<<<(n_tiles + 255) / 256, 256, 0, stream>>>(ranges, n_tiles, L);
   const int sms = sm_count();
   const int small_grid = (int)std::min<int64_t>(n_tiles, (int64_t)sms * 12);
-  seg_small_kernel<<<small_grid, kSmallThreads, 0, stream>>>(L, ka, va, kb, vb, rank_bits);
-  const int chunk_grid = (int)std::min<int64_t>(L.chunk_cap, (int64_t)sms * 2);
-  seg_chunk_kernel<<<chunk_grid, kChunkThreads, sizeof(ChunkSmem), stream>>>(L, ka, va, kb, vb, rank_bits);
-  const int merge_grid = (int)std::min<int64_t>(L.chunk_cap, (int64_t)sms * 2);
-  seg_merge_kernel<<<merge_grid, kMergeThreads, sizeof(MergeSmem), stream>>>(L, ka, va, kb, vb);
+  if (small_n == 256) seg_small_kernel<256><<<small_grid, kSmallThreads, 0, stream>>>(L, ka, va, kb, vb, rank_bits);
+  else if (small_n == 1024) seg_small_kernel<1024><<<small_grid, kSmallThreads, 0, stream>>>(L, ka, va, kb, vb, rank_bits);
+  else seg_small_kernel<512><<<small_grid, kSmallThreads, 0, stream>>>(L, ka, va, kb, vb, rank_bits);
+  if (chunk == 2048) launch_chunk_and_merge<2048>(L, sms, ka, va, kb, vb, rank_bits, stream);
+  else launch_chunk_and_merge<4096>(L, sms, ka, va, kb, vb, rank_bits, stream);
 }
 
 }  // namespace svr

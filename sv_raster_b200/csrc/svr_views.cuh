@@ -9,7 +9,8 @@ constexpr int kMaxViews = 64;
 
 struct ViewParams {
   int W, H;              // image size in pixels
-  int grid_x, grid_y;    // tile grid (ceil(W/16), ceil(H/16))
+  int grid_x, grid_y;    // tile grid (ceil(W/ts), ceil(H/ts)), ts = 1 << tile_shift
+  int tile_shift;        // log2 of the tile size (4 on the plain path)
   float tanfovx, tanfovy;
   float cx, cy;          // principal point in pixels
   float focal_x, focal_y;  // 0.5*W/tanfovx, computed in float on the host (preprocess.cu:173-174)

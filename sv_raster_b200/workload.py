@@ -44,6 +44,14 @@ def _t(a, dev, dt=torch.float32):
     return torch.from_numpy(np.ascontiguousarray(a)).to(dev, dt)
 
 
+def tune_raster(raster, geos, sh0, shs):
+    """Autotune a batched rasterizer on this scene (see autotune.py); returns
+    the chosen launch parameters as a JSON-able dict."""
+    from .autotune import tune_batched
+    res = tune_batched(raster, geos, sh0, shs, 3)
+    return {k: (list(v) if isinstance(v, tuple) else v) for k, v in res["choice"].items()}
+
+
 class _Timer:
     """CUDA-event timing of one kernel stage on the launching stream."""
 
@@ -234,7 +242,7 @@ class BatchedWorkload:
     fp32 compositing / gradients, no host sync inside a step (the step is
     also captured as a CUDA graph)."""
 
-    def __init__(self, scene, dev, storage=torch.bfloat16, graph=True):
+    def __init__(self, scene, dev, storage=torch.bfloat16, graph=True, tune=True):
         from .batched import BatchedRasterizer
         self.sc = scene
         self.dev = dev
@@ -249,6 +257,10 @@ class BatchedWorkload:
         self.raster = BatchedRasterizer(self.cams, self.octpath, self.centers, self.lengths,
                                         max_level=scene.max_level)
         self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
+        self.tuned = None
+        if tune:
+            self.tuned = tune_raster(self.raster, self.geos, self.sh0, self.shs)
+            self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
         r = self.raster
         tg = [_t(t, dev).reshape(-1) for t in scene.targets]
         self.target = torch.cat([tg[i % len(tg)] for i in range(len(self.cams))])
@@ -363,9 +375,12 @@ class BatchedWorkload:
         T_ = max(self.raster.n_tiles, 1)
         passes = math.ceil(int(T_).bit_length() / 8)  # radix passes over the tile bits only
         g = self.raster.n_groups
+        order = self.raster.schedule[0]
         # project 1 + scan 3 + segments 1 + duplicate 1 + (sort 3/pass + ranges 1) per group
-        # + segment sort 4 (plan, small, chunk, merge) + fwd 1 + bwd 1 + sh 1
-        return 1 + 3 + 1 + 1 + g * (3 * passes + 1) + 4 + 1 + 1 + 1
+        # + segment sort 4 (plan, small, chunk, merge) + per ordered compositing stage a
+        # tile-order key kernel and one 3-kernel sort pass + fwd 1 + bwd 1 + sh 1
+        n_order = 4 * ((order & 1) + ((order >> 1) & 1))
+        return 1 + 3 + 1 + 1 + g * (3 * passes + 1) + 4 + n_order + 1 + 1 + 1
 
     def kernel_stats(self):
         torch.cuda.synchronize()
@@ -449,7 +464,7 @@ class BatchedTrainWorkload:
     capturable as one CUDA graph (the step count lives on the device)."""
 
     def __init__(self, scene, dev, storage=torch.bfloat16, lr_geo=0.025, lr_sh=0.01, betas=(0.1, 0.99),
-                 eps=1e-15):
+                 eps=1e-15, tune=True):
         from .batched import BatchedRasterizer
         self.sc, self.dev, self.P = scene, dev, scene.n_voxels
         self.octpath = _t(scene.octpath.reshape(-1, 1), dev, torch.int64)
@@ -462,6 +477,10 @@ class BatchedTrainWorkload:
         self.raster = BatchedRasterizer(self.cams, self.octpath, self.centers, self.lengths,
                                         max_level=scene.max_level)
         self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
+        self.tuned = None
+        if tune:
+            self.tuned = tune_raster(self.raster, self.geos, self.sh0, self.shs)
+            self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
         r = self.raster
         tg = [_t(t, dev).reshape(-1) for t in scene.targets]
         self.target = torch.cat([tg[i % len(tg)] for i in range(len(self.cams))])

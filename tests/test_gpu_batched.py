@@ -197,7 +197,7 @@ def test_graph_replay_equals_eager(c1):
     sc = synthetic.config_scene("c1")
     sc.targets = [np.random.default_rng(1).uniform(0, 1, (3, c.height, c.width)).astype(np.float32)
                   for c in sc.cameras]
-    wl = BatchedWorkload(sc, torch.device("cuda"), storage=torch.float32)
+    wl = BatchedWorkload(sc, torch.device("cuda"), storage=torch.float32, tune=False)
     wl._eager_step(False)
     torch.cuda.synchronize()
     c_eager, dgeo_eager = wl.color.clone(), wl.grads[0].clone()
@@ -242,7 +242,7 @@ def test_training_step_graph_matches_plain_form():
     sc.targets = [np.random.default_rng(3).uniform(0, 1, (3, c.height, c.width)).astype(np.float32)
                   for c in sc.cameras]
     dev = torch.device("cuda")
-    b = BatchedTrainWorkload(sc, dev, storage=torch.float32)
+    b = BatchedTrainWorkload(sc, dev, storage=torch.float32, tune=False)
     ms_b, lb = b.run(3)
     p = PlainTrainWorkload(sc, dev)
     ms_p, lp = p.run(3)
@@ -251,3 +251,67 @@ def test_training_step_graph_matches_plain_form():
         assert abs(x - y) / y < 1e-4
     assert rel_err(b.geos.float(), p.geos.detach()) < 1e-4
     assert rel_err(b.shs.float(), p.shs.detach()) < 1e-4
+
+
+def _render_and_grads(r, C, wC, wT):
+    r.fit_capacity(C.sh0, C.shs, 3)
+    r.prepare(C.sh0, C.shs, 3)
+    color, T = r.render(C.geos)
+    dgeo, sub, dsh0, dshs = r.backward(C.geos, T, wC, wT, 3, 16)
+    torch.cuda.synchronize()
+    total, err = r.header()
+    assert err == 0
+    return color.clone(), T.clone(), dgeo.clone(), sub.clone(), dsh0.clone(), dshs.clone(), total
+
+
+@pytest.mark.parametrize("tile,stage,order,ctas,buckets", [
+    (8, 64, (True, True), (0, 0), (512, 4096)),
+    (32, 256, (True, True), (0, 0), (512, 4096)),
+    (16, 128, (True, True), (0, 0), (256, 2048)),
+    (16, 512, (False, False), (0, 0), (1024, 4096)),
+    (16, 256, (False, True), (3, 2), (512, 2048)),
+])
+def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas, buckets):
+    """Every tile size, staging depth, compositing schedule and sort-bucket
+    setting the autotuner may pick renders bit-identical images and T (a pixel
+    sees the same instances in the same order) and the same gradients up to
+    the order of the atomic additions."""
+    g = torch.Generator(device="cuda").manual_seed(11)
+    r0, _ = _raster(c1)
+    n_pix = r0.n_pixels
+    wC = torch.randn(3 * n_pix, device="cuda", generator=g)
+    wT = torch.randn(n_pix, device="cuda", generator=g)
+    base = _render_and_grads(r0, c1, wC, wT)
+    r, _ = _raster(c1, tile_size=tile)
+    r.set_staging(stage)
+    r.set_schedule(fwd_ordered=order[0], bwd_ordered=order[1], fwd_ctas_per_sm=ctas[0], bwd_ctas_per_sm=ctas[1])
+    r.set_sort_buckets(*buckets)
+    got = _render_and_grads(r, c1, wC, wT)
+    assert torch.equal(got[0], base[0]), "colour differs"
+    assert torch.equal(got[1], base[1]), "T differs"
+    for a, b, name in zip(got[2:6], base[2:6], ("dL_dgeos", "subdiv", "dL_dsh0", "dL_dshs")):
+        assert rel_err(a, b) < 1e-5, name
+    if tile == 8:
+        assert got[6] > base[6]  # smaller tiles duplicate more instances
+    if tile == 32:
+        assert got[6] < base[6]
+
+
+def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
+    from sv_raster_b200.autotune import tune_batched
+    monkeypatch.setenv("SVR_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    g = torch.Generator(device="cuda").manual_seed(5)
+    r0, _ = _raster(c1)
+    wC = torch.randn(3 * r0.n_pixels, device="cuda", generator=g)
+    wT = torch.randn(r0.n_pixels, device="cuda", generator=g)
+    base = _render_and_grads(r0, c1, wC, wT)
+    r, _ = _raster(c1)
+    res = tune_batched(r, c1.geos, c1.sh0, c1.shs, 3, reps=2, warmup=1)
+    assert not res["cached"] and set(res["choice"]) == {"tile", "sort", "fwd", "bwd"}
+    got = _render_and_grads(r, c1, wC, wT)
+    assert torch.equal(got[0], base[0])
+    assert rel_err(got[2], base[2]) < 1e-5
+    r2, _ = _raster(c1)
+    res2 = tune_batched(r2, c1.geos, c1.sh0, c1.shs, 3)
+    assert res2["cached"] and res2["choice"] == res["choice"]
+    assert r2.tile_size == res["choice"]["tile"][0]
