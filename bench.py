@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg (profiling runs)")
     ap.add_argument("--no-tune", action="store_true",
                     help="batched mode: default launch parameters instead of the autotuner's choice")
+    ap.add_argument("--tile", default=None,
+                    help="batched mode: fixed compositing tile 'TS' or 'TS,SB' (8,64 | 16,128|256|512 | 32,256); "
+                         "no autotuning")
     ap.add_argument("--train", action="store_true",
                     help="training-step workload (fwd + bwd + fused Adam, graph-captured) vs the plain fp32 form")
     ap.add_argument("--plain-steps", type=int, default=10, help="steps of the plain form in --train mode")
@@ -158,8 +161,14 @@ def main():
     sc = scene_for(args, rank, world)
     if args.train:
         return run_train(args, sc, dev, world, rank)
-    wl = workload.PlainWorkload(sc, dev) if args.mode == "plain" else \
-        workload.BatchedWorkload(sc, dev, tune=not args.no_tune)
+    if args.mode == "plain":
+        wl = workload.PlainWorkload(sc, dev)
+    else:
+        tile = None
+        if args.tile:
+            parts = [int(x) for x in args.tile.split(",")]
+            tile = (parts[0], parts[1] if len(parts) > 1 else (64 if parts[0] == 8 else 256))
+        wl = workload.BatchedWorkload(sc, dev, tune=not (args.no_tune or tile), tile=tile)
     n_views = len(sc.cameras)
 
     for _ in range(args.warmup):
@@ -223,9 +232,12 @@ def main():
         traffic = None
         tf = os.path.join(ROOT, "profiles", "render_traffic.json")
         if os.path.exists(tf) and dom["name"] in ("render_fwd", "render_bwd"):
-            t = json.load(open(tf))
-            inst = wl.instances_per_view() * (n_views if args.mode == "batched" else 1)
-            traffic = round(t[dom["name"]]["dram_bytes"] / t["instances_per_launch"] * inst)
+            r = getattr(wl, "raster", None)
+            tkey = f"{r.tile_size},{r.staging}" if r is not None else "16,256"
+            t = json.load(open(tf))["tiles"].get(tkey)
+            if t is not None:
+                inst = wl.instances_per_view() * (n_views if args.mode == "batched" else 1)
+                traffic = round(t[dom["name"]]["dram_bytes"] / t["instances_per_launch"] * inst)
         line = {
             "metric": "fwd+bwd ms/view", "value": round(value, 4), "unit": "ms/view", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),

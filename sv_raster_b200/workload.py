@@ -49,7 +49,10 @@ def tune_raster(raster, geos, sh0, shs):
     the chosen launch parameters as a JSON-able dict."""
     from .autotune import tune_batched
     res = tune_batched(raster, geos, sh0, shs, 3)
-    return {k: (list(v) if isinstance(v, tuple) else v) for k, v in res["choice"].items()}
+    out = {k: (list(v) if isinstance(v, tuple) else v) for k, v in res["choice"].items()}
+    out["timings_ms"] = res["timings"]
+    out["cached"] = res["cached"]
+    return out
 
 
 class _Timer:
@@ -242,7 +245,7 @@ class BatchedWorkload:
     fp32 compositing / gradients, no host sync inside a step (the step is
     also captured as a CUDA graph)."""
 
-    def __init__(self, scene, dev, storage=torch.bfloat16, graph=True, tune=True):
+    def __init__(self, scene, dev, storage=torch.bfloat16, graph=True, tune=True, tile=None):
         from .batched import BatchedRasterizer
         self.sc = scene
         self.dev = dev
@@ -256,8 +259,11 @@ class BatchedWorkload:
         self.cams = [_DevCam(c, dev) for c in scene.cameras]
         self.raster = BatchedRasterizer(self.cams, self.octpath, self.centers, self.lengths,
                                         max_level=scene.max_level)
-        self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
         self.tuned = None
+        if tile is not None:
+            self.raster.set_tile_size(*tile)
+            self.tuned = {"tile": list(tile), "fixed": True}
+        self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
         if tune:
             self.tuned = tune_raster(self.raster, self.geos, self.sh0, self.shs)
             self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
