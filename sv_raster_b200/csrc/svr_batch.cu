@@ -45,34 +45,53 @@ struct GroupTable {
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
+// One thread per voxel, looping over the views: the voxel's centre, size and
+// SH coefficients are read once (the coefficients on its first visible view)
+// and kept in registers, so each view costs the projection arithmetic and
+// the per-(view, voxel) writes only.
 template <int DEG, typename TS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128)
 project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* __restrict__ centers,
                   const float* __restrict__ lengths, const TS* __restrict__ sh0, const TS* __restrict__ shs, int M,
                   uint32_t* __restrict__ ndup, uint2* __restrict__ bboxes, uint32_t* __restrict__ quads,
                   float* __restrict__ rgbs) {
-  const int view = blockIdx.y;
-  const ViewParams& vp = views.v[view];
-  __shared__ float s_m[24];
-  if (threadIdx.x < 12) s_m[threadIdx.x] = vp.w2c[threadIdx.x];
-  else if (threadIdx.x < 24) s_m[threadIdx.x] = vp.c2w[threadIdx.x - 12];
+  constexpr int NB = (DEG + 1) * (DEG + 1) - 1;  // rest coefficients per channel
+  __shared__ float s_m[kMaxViews][24];           // w2c (12) and c2w (12) of every view
+  for (int t = threadIdx.x; t < views.n * 24; t += blockDim.x) {
+    const int v = t / 24, k = t % 24;
+    s_m[v][k] = k < 12 ? views.v[v].w2c[k] : views.v[v].c2w[k - 12];
+  }
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
-  const size_t o = (size_t)view * P + i;
   const float cx = centers[3 * (size_t)i], cy = centers[3 * (size_t)i + 1], cz = centers[3 * (size_t)i + 2];
-  const Projection pr = project_voxel(vp, s_m, s_m + 12, cx, cy, cz, lengths[i]);
-  ndup[o] = pr.n;
-  bboxes[o] = pr.bbox;
-  quads[o] = pr.quads;
-  if (pr.n == 0) return;
-  // View-dependent colour of this visible voxel (sh_compute.cu:54-106).
-  float dx = cx - s_m[12 + 3], dy = cy - s_m[12 + 7], dz = cz - s_m[12 + 11];
-  const float rn = rnorm3df(dx, dy, dz);
-  dx = dx * rn; dy = dy * rn; dz = dz * rn;
-  const TS* sh = shs + (size_t)i * (M - 1) * 3;
+  const float len = lengths[i];
+  float c0[3];
+  float shr[NB > 0 ? NB * 3 : 1];
+  bool loaded = false;
+  for (int v = 0; v < views.n; ++v) {
+    const size_t o = (size_t)v * P + i;
+    const float* m = s_m[v];
+    const Projection pr = project_voxel(views.v[v], m, m + 12, cx, cy, cz, len);
+    ndup[o] = pr.n;
+    bboxes[o] = pr.bbox;
+    quads[o] = pr.quads;
+    if (pr.n == 0) continue;
+    if (!loaded) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) rgbs[3 * o + c] = sh_channel<DEG>(dx, dy, dz, ldf(sh0, 3 * (size_t)i + c), sh, c);
+      for (int c = 0; c < 3; ++c) c0[c] = ldf(sh0, 3 * (size_t)i + c);
+      const TS* sh = shs + (size_t)i * (M - 1) * 3;
+#pragma unroll
+      for (int k = 0; k < NB * 3; ++k) shr[k] = ldf(sh, k);
+      loaded = true;
+    }
+    // View-dependent colour of this visible voxel (sh_compute.cu:54-106).
+    float dx = cx - m[12 + 3], dy = cy - m[12 + 7], dz = cz - m[12 + 11];
+    const float rn = rnorm3df(dx, dy, dz);
+    dx = dx * rn; dy = dy * rn; dz = dz * rn;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) rgbs[3 * o + c] = sh_channel<DEG>(dx, dy, dz, c0[c], shr, c);
+  }
 }
 
 // Instance segment [start, start + count) of each sort group, clamped to the
@@ -88,6 +107,27 @@ __global__ void group_segments_kernel(const __grid_constant__ GroupTable gt, int
   segs[2 * g + 1] = end - start;
 }
 
+// Position of the k-th (0-based) set bit of m (k < popc(m)).
+__device__ __forceinline__ int nth_set_bit(uint32_t m, int k) {
+  int pos = 0;
+  int c = __popc(m & 0xFFFFu);
+  if (k >= c) { k -= c; pos += 16; m >>= 16; }
+  c = __popc(m & 0xFFu);
+  if (k >= c) { k -= c; pos += 8; m >>= 8; }
+  c = __popc(m & 0xFu);
+  if (k >= c) { k -= c; pos += 4; m >>= 4; }
+  c = __popc(m & 0x3u);
+  if (k >= c) { k -= c; pos += 2; m >>= 2; }
+  if (k >= (int)(m & 1u)) pos += 1;
+  return pos;
+}
+
+// Duplication with the stores of a warp coalesced.  The instances of the
+// warp's 32 consecutive (view, voxel) pairs form one contiguous run of the
+// scan; the warp walks that run 32 instances at a time, each lane decoding
+// its instance (owning voxel, then quadrant / tile row / tile column in the
+// plain path's generation order: quadrants ascending, tiles row-major,
+// forward.cu:540-562) and writing key and value at its own slot.
 __global__ void __launch_bounds__(256)
 duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const int64_t* __restrict__ octpaths,
                        const uint2* __restrict__ bboxes, const uint32_t* __restrict__ quads,
@@ -96,40 +136,65 @@ duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const int
                        uint32_t* __restrict__ err) {
   const int view = blockIdx.y;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= P) return;
-  const size_t o = (size_t)view * P + idx;
-  const uint32_t n = ndup[o];
-  if (n == 0) return;
+  const int lane = threadIdx.x & 31;
+  const bool valid = idx < P;
+  const size_t o = (size_t)view * P + (valid ? idx : 0);
   const ViewParams& vp = views.v[view];
-  const uint32_t end = scan[o];
-  // Past the capacity: flag it, and still write the instances that fit so
-  // that every slot below the capacity holds a valid key.
-  if (end > cap) atomicOr(err, SVR_DEVERR_CAPACITY);
-  const uint32_t wend = min(end, cap);
-  uint32_t off = end - n;
-  int tx0, ty0, tx1, ty1;
-  bbox_tile_rect(bboxes[o], vp.grid_x, vp.grid_y, vp.tile_shift, tx0, ty0, tx1, ty1);
-  const uint64_t path = (uint64_t)octpaths[idx];
+  const uint32_t n = valid ? ndup[o] : 0u;
+  const uint32_t end = valid ? scan[o] : 0u;
+  if (n > 0 && end > cap) atomicOr(err, SVR_DEVERR_CAPACITY);
+  int tx0 = 0, ty0 = 0, tx1 = 0, ty1 = 0;
+  uint64_t path = 0;
+  uint32_t qb = 0;
   const int low = (rank_bits == kRankBits) ? 0 : kRankBits - (rank_bits - 3);  // 3*(16-L)
-  if (low > 0 && (path & ((1ull << low) - 1ull)) != 0ull) atomicOr(err, SVR_DEVERR_LEVEL);
-  const uint32_t qb = quads[o];
-  for (uint32_t q = 0; q < 8; ++q) {
-    if (!(qb & (1u << q))) continue;
-    const uint64_t full = order_rank(path, q);
-    const uint64_t rank = (low == 0) ? full : (((full >> low) << 3) | q);
-    const uint32_t val = make_sort_val((uint32_t)idx, q);
-    for (int y = ty0; y <= ty1; ++y) {
-      for (int x = tx0; x <= tx1; ++x) {
-        const uint64_t tile = (uint64_t)(vp.sort_tile_off + (uint32_t)(y * vp.grid_x + x));
-        if (off < wend) {
-          keys[off] = (tile << rank_bits) | rank;
-          vals[off] = val;
-        }
-        ++off;
-      }
+  if (n > 0) {
+    bbox_tile_rect(bboxes[o], vp.grid_x, vp.grid_y, vp.tile_shift, tx0, ty0, tx1, ty1);
+    path = (uint64_t)octpaths[idx];
+    qb = quads[o];
+    if (low > 0 && (path & ((1ull << low) - 1ull)) != 0ull) atomicOr(err, SVR_DEVERR_LEVEL);
+    const uint32_t tiles = (uint32_t)((tx1 - tx0 + 1) * (ty1 - ty0 + 1));
+    if (tiles * (uint32_t)__popc(qb) != n) atomicOr(err, SVR_DEVERR_DUP_MISMATCH);
+  }
+  // exclusive scan of n over the warp; the run starts at the first lane's scan offset
+  uint32_t incl = n;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += t;
+  }
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  if (total == 0u) return;
+  const uint32_t off = incl - n;
+  const uint32_t run0 = __shfl_sync(0xffffffffu, end - n, 0) + 0u;  // lane 0's start (valid even if n == 0)
+  const uint32_t w = (uint32_t)(tx1 - tx0 + 1);
+  const uint32_t tiles = w * (uint32_t)(ty1 - ty0 + 1);
+  for (uint32_t cb = 0; cb < total; cb += 32) {
+    const uint32_t p = cb + lane;
+    // owning lane: the largest s with off_s <= p (offsets are non-decreasing)
+    int sl = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const uint32_t t = __shfl_sync(0xffffffffu, off, sl + step);
+      if (t <= p) sl += step;
+    }
+    const uint32_t k = p - __shfl_sync(0xffffffffu, off, sl);
+    const uint32_t s_tiles = __shfl_sync(0xffffffffu, tiles, sl);
+    const uint32_t s_w = __shfl_sync(0xffffffffu, w, sl);
+    const int s_tx0 = __shfl_sync(0xffffffffu, tx0, sl), s_ty0 = __shfl_sync(0xffffffffu, ty0, sl);
+    const uint32_t s_qb = __shfl_sync(0xffffffffu, qb, sl);
+    const uint64_t s_path = __shfl_sync(0xffffffffu, path, sl);
+    const uint32_t slot = run0 + p;
+    if (p < total && slot < cap) {
+      const uint32_t qi = k / s_tiles, rem = k - qi * s_tiles;
+      const uint32_t ty = (uint32_t)s_ty0 + rem / s_w, tx = (uint32_t)s_tx0 + rem % s_w;
+      const uint32_t q = (uint32_t)nth_set_bit(s_qb, (int)qi);
+      const uint64_t full = order_rank(s_path, q);
+      const uint64_t rank = (low == 0) ? full : (((full >> low) << 3) | q);
+      const uint64_t tile = (uint64_t)(vp.sort_tile_off + ty * (uint32_t)vp.grid_x + tx);
+      keys[slot] = (tile << rank_bits) | rank;
+      vals[slot] = make_sort_val((uint32_t)(blockIdx.x * blockDim.x + (threadIdx.x & ~31) + sl), q);
     }
   }
-  if (off != end) atomicOr(err, SVR_DEVERR_DUP_MISMATCH);
 }
 
 // dL/dSH of every voxel summed over views: sum_v basis(dir_v) * dL/drgb_v
@@ -496,16 +561,17 @@ int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, 
   const int P = (int)p->P;
   const size_t VP = (size_t)p->V * p->P;
   cudaMemsetAsync(q.header, 0, kHeaderWords * sizeof(uint32_t), stream);
-  dim3 grid((P + 255) / 256, p->V);
+  const dim3 pgrid((P + 127) / 128);
 #define SVR_PROJ(D)                                                                                           \
   if (sh_bf16)                                                                                                \
-    project_sh_kernel<D, __nv_bfloat16><<<grid, 256, 0, stream>>>(                                            \
+    project_sh_kernel<D, __nv_bfloat16><<<pgrid, 128, 0, stream>>>(                                           \
         p->vt, P, vox_centers, vox_lengths, (const __nv_bfloat16*)sh0, (const __nv_bfloat16*)shs, M, q.ndup, \
         q.bbox, q.quad, q.rgbs);                                                                              \
   else                                                                                                        \
-    project_sh_kernel<D, float><<<grid, 256, 0, stream>>>(p->vt, P, vox_centers, vox_lengths,                \
-                                                          (const float*)sh0, (const float*)shs, M, q.ndup,   \
-                                                          q.bbox, q.quad, q.rgbs);
+    project_sh_kernel<D, float><<<pgrid, 128, 0, stream>>>(p->vt, P, vox_centers, vox_lengths,               \
+                                                           (const float*)sh0, (const float*)shs, M, q.ndup,  \
+                                                           q.bbox, q.quad, q.rgbs);
+  const dim3 grid((P + 255) / 256, p->V);
   switch (sh_degree) {
     case 0: SVR_PROJ(0) break;
     case 1: SVR_PROJ(1) break;

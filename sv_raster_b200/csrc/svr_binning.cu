@@ -11,7 +11,7 @@
 // launched for a caller-given capacity, so the whole chain can be captured in
 // a CUDA graph without a host round trip.  The sort is a three-kernel-per-pass
 // LSD radix sort (upsweep histogram, per-digit row scan, stable downsweep)
-// with 8-bit digits and 2048-item CTA tiles; ranks within a CTA come from
+// with 8- to 10-bit digits and 2048-item CTA tiles; ranks within a CTA come from
 // warp __match_any_sync, which keeps it stable, so it reproduces the order of
 // any other stable sort of the same keys.
 #include "svr_common.cuh"
@@ -187,31 +187,47 @@ void launch_duplicate(const ViewTable& views, int P, const int64_t* octpaths, co
 }
 
 // --------------------------------------------------------------------------
-// LSD radix sort of (uint64 key, uint32 value) pairs
+// LSD radix sort of (uint64 key, uint32 value) pairs.  Digits are 8, 9 or 10
+// bits wide: a sort over n key bits takes ceil(n / 10) passes of equal width
+// (at least 8 bits), e.g. 2 passes of 9 bits for 18 bits instead of 3 of 8.
 // --------------------------------------------------------------------------
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortRounds = 8;                        // items per thread (registers: keep >= 3 CTAs/SM)
 constexpr int kSortTile = kSortThreads * kSortRounds;  // 2048
 constexpr int kWarpSpan = 32 * kSortRounds;            // 256 items per warp
-constexpr int kRadix = 256;
+constexpr int kMaxRadixBits = 10;
 
 static inline int sort_blocks(size_t cap) { return (int)((cap + kSortTile - 1) / kSortTile); }
 
 size_t sort_temp_bytes(size_t cap) {
   const size_t nb = (size_t)std::max(1, sort_blocks(cap));
-  return (nb * kRadix + kRadix) * sizeof(uint32_t) + 256;
+  const size_t radix = (size_t)1 << kMaxRadixBits;
+  return (nb * radix + radix) * sizeof(uint32_t) + 256;
 }
 
-int sort_passes(int key_bits) { return (key_bits + 7) / 8; }
+struct RadixPlan {
+  int passes;
+  int bits;  // digit width of every pass
+};
 
+static RadixPlan radix_plan(int nbits) {
+  if (nbits <= 0) return {0, 8};
+  const int passes = (nbits + kMaxRadixBits - 1) / kMaxRadixBits;
+  const int bits = std::max(8, (nbits + passes - 1) / passes);
+  return {passes, bits};
+}
 
+int sort_passes(int nbits) { return radix_plan(nbits).passes; }
+
+template <int RB>
 __global__ void __launch_bounds__(kSortThreads)
 radix_upsweep_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ d_start,
                      const uint32_t* __restrict__ d_n, uint32_t cap, int shift, uint32_t* __restrict__ hist,
                      int nblocks) {
-  __shared__ uint32_t s_hist[kSortWarps][kRadix];
-  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&s_hist[0][0])[i] = 0u;
+  constexpr int R = 1 << RB, DPT = R / kSortThreads;
+  __shared__ uint32_t s_hist[kSortWarps][R];
+  for (int i = threadIdx.x; i < kSortWarps * R; i += kSortThreads) (&s_hist[0][0])[i] = 0u;
   __syncthreads();
   const uint32_t n = min(*d_n, cap);
   if (d_start) keys += *d_start;
@@ -222,16 +238,20 @@ radix_upsweep_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restri
     for (int r = 0; r < kSortRounds; ++r) {
       const size_t i = start + (size_t)warp * kWarpSpan + r * 32 + lane;
       if (i < n) {
-        const uint32_t d = (uint32_t)(keys[i] >> shift) & 0xFFu;
+        const uint32_t d = (uint32_t)(keys[i] >> shift) & (R - 1u);
         atomicAdd(&s_hist[warp][d], 1u);
       }
     }
   }
   __syncthreads();
-  uint32_t s = 0;
 #pragma unroll
-  for (int w = 0; w < kSortWarps; ++w) s += s_hist[w][threadIdx.x];
-  hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = s;
+  for (int j = 0; j < DPT; ++j) {
+    const int d = threadIdx.x * DPT + j;
+    uint32_t s = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) s += s_hist[w][d];
+    hist[(size_t)d * nblocks + blockIdx.x] = s;
+  }
 }
 
 // One CTA per digit: exclusive scan of that digit's per-block counts (in
@@ -263,23 +283,27 @@ radix_scan_rows_kernel(uint32_t* __restrict__ hist, int nblocks, uint32_t* __res
   if (threadIdx.x == 0) digit_total[blockIdx.x] = running;
 }
 
+template <int RB>
 struct DownsweepSmem {
+  static constexpr int R = 1 << RB;
   uint64_t keys[kSortTile];
   uint32_t vals[kSortTile];
-  uint32_t warp_cnt[kSortWarps][kRadix];
-  uint32_t local_start[kRadix];
-  uint32_t global_start[kRadix];
+  uint32_t warp_cnt[kSortWarps][R];
+  uint32_t local_start[R];
+  uint32_t global_start[R];
   uint32_t scan_tmp[kSortThreads / 32 + 1];
 };
 
+template <int RB>
 __global__ void __launch_bounds__(kSortThreads, 3)
 radix_downsweep_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                        uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                        const uint32_t* __restrict__ d_start, const uint32_t* __restrict__ d_n, uint32_t cap, int shift,
                        const uint32_t* __restrict__ hist, const uint32_t* __restrict__ digit_total,
                        int nblocks) {
+  constexpr int R = 1 << RB, DPT = R / kSortThreads;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  DownsweepSmem& sm = *reinterpret_cast<DownsweepSmem*>(smem_raw);
+  DownsweepSmem<RB>& sm = *reinterpret_cast<DownsweepSmem<RB>*>(smem_raw);
   const uint32_t n = min(*d_n, cap);
   const size_t start = (size_t)blockIdx.x * kSortTile;
   if (start >= n) return;
@@ -289,11 +313,23 @@ radix_downsweep_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restr
   }
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  for (int i = tid; i < kSortWarps * kRadix; i += kSortThreads) (&sm.warp_cnt[0][0])[i] = 0u;
+  for (int i = tid; i < kSortWarps * R; i += kSortThreads) (&sm.warp_cnt[0][0])[i] = 0u;
   {
+    // thread t owns digits [t * DPT, (t + 1) * DPT)
+    uint32_t v[DPT], sum = 0;
+#pragma unroll
+    for (int j = 0; j < DPT; ++j) {
+      v[j] = digit_total[tid * DPT + j];
+      sum += v[j];
+    }
     uint32_t tot;
-    const uint32_t gbase = block_exclusive_scan<kSortThreads>(digit_total[tid], sm.scan_tmp, tot);
-    sm.global_start[tid] = gbase + hist[(size_t)tid * nblocks + blockIdx.x];
+    uint32_t gbase = block_exclusive_scan<kSortThreads>(sum, sm.scan_tmp, tot);
+#pragma unroll
+    for (int j = 0; j < DPT; ++j) {
+      const int d = tid * DPT + j;
+      sm.global_start[d] = gbase + hist[(size_t)d * nblocks + blockIdx.x];
+      gbase += v[j];
+    }
   }
   __syncthreads();
 
@@ -307,7 +343,7 @@ radix_downsweep_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restr
     const bool valid = i < n;
     k[r] = valid ? kin[i] : 0ull;
     v[r] = valid ? vin[i] : 0u;
-    const uint32_t d = valid ? ((uint32_t)(k[r] >> shift) & 0xFFu) : kRadix;
+    const uint32_t d = valid ? ((uint32_t)(k[r] >> shift) & (R - 1u)) : (uint32_t)R;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const uint32_t before = __popc(peers & lt);
     const uint32_t base = valid ? sm.warp_cnt[warp][d] : 0u;
@@ -319,22 +355,34 @@ radix_downsweep_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restr
   __syncthreads();
   {
     // Per digit: exclusive prefix over warps, then local start of the digit.
-    uint32_t run = 0;
+    uint32_t tot_d[DPT], sum = 0;
 #pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) {
-      const uint32_t c = sm.warp_cnt[w][tid];
-      sm.warp_cnt[w][tid] = run;
-      run += c;
+    for (int j = 0; j < DPT; ++j) {
+      const int d = tid * DPT + j;
+      uint32_t run = 0;
+#pragma unroll
+      for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = sm.warp_cnt[w][d];
+        sm.warp_cnt[w][d] = run;
+        run += c;
+      }
+      tot_d[j] = run;
+      sum += run;
     }
     uint32_t tot;
-    sm.local_start[tid] = block_exclusive_scan<kSortThreads>(run, sm.scan_tmp, tot);
+    uint32_t base = block_exclusive_scan<kSortThreads>(sum, sm.scan_tmp, tot);
+#pragma unroll
+    for (int j = 0; j < DPT; ++j) {
+      sm.local_start[tid * DPT + j] = base;
+      base += tot_d[j];
+    }
   }
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < kSortRounds; ++r) {
     const size_t i = start + (size_t)warp * kWarpSpan + r * 32 + lane;
     if (i < n) {
-      const uint32_t d = (uint32_t)(k[r] >> shift) & 0xFFu;
+      const uint32_t d = (uint32_t)(k[r] >> shift) & (R - 1u);
       const uint32_t pos = sm.local_start[d] + sm.warp_cnt[warp][d] + rk[r];
       sm.keys[pos] = k[r];
       sm.vals[pos] = v[r];
@@ -344,14 +392,14 @@ radix_downsweep_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restr
   const uint32_t tile_n = (uint32_t)min((size_t)kSortTile, (size_t)n - start);
   for (uint32_t p = tid; p < tile_n; p += kSortThreads) {
     const uint64_t key = sm.keys[p];
-    const uint32_t d = (uint32_t)(key >> shift) & 0xFFu;
+    const uint32_t d = (uint32_t)(key >> shift) & (R - 1u);
     const uint32_t g = sm.global_start[d] + (p - sm.local_start[d]);
     kout[g] = key;
     vout[g] = sm.vals[p];
   }
 }
 
-// Opt the downsweep kernel into >48 KB of dynamic shared memory, once per
+// Opt the downsweep kernels into >48 KB of dynamic shared memory, once per
 // device (a function attribute, so it must not be set inside graph capture
 // for the first time: plan creation and every plain call reach it first).
 void ensure_sort_attributes() {
@@ -359,9 +407,23 @@ void ensure_sort_attributes() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
   std::call_once(flags[dev], [] {
-    cudaFuncSetAttribute(radix_downsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(DownsweepSmem));
+    cudaFuncSetAttribute(radix_downsweep_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(DownsweepSmem<8>));
+    cudaFuncSetAttribute(radix_downsweep_kernel<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(DownsweepSmem<9>));
+    cudaFuncSetAttribute(radix_downsweep_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(DownsweepSmem<10>));
   });
+}
+
+template <int RB>
+static void radix_pass(const uint64_t* kin, const uint32_t* vin, uint64_t* kout, uint32_t* vout,
+                       const uint32_t* d_start, const uint32_t* d_n, uint32_t cap, int shift, uint32_t* hist,
+                       uint32_t* digit_total, int nb, cudaStream_t stream) {
+  radix_upsweep_kernel<RB><<<nb, kSortThreads, 0, stream>>>(kin, d_start, d_n, cap, shift, hist, nb);
+  radix_scan_rows_kernel<<<1 << RB, 1024, 0, stream>>>(hist, nb, digit_total);
+  radix_downsweep_kernel<RB><<<nb, kSortThreads, sizeof(DownsweepSmem<RB>), stream>>>(
+      kin, vin, kout, vout, d_start, d_n, cap, shift, hist, digit_total, nb);
 }
 
 // Sorts the `*d_n` pairs starting at element `*d_start` (both read on the
@@ -371,24 +433,22 @@ void ensure_sort_attributes() {
 int launch_radix_sort(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, const uint32_t* d_start,
                       const uint32_t* d_n, uint32_t cap, int key_bits, void* temp, cudaStream_t stream,
                       int lo_bit) {
-  const int passes = sort_passes(key_bits - lo_bit);
-  if (cap == 0 || passes == 0) return 0;
+  const RadixPlan rp = radix_plan(key_bits - lo_bit);
+  if (cap == 0 || rp.passes == 0) return 0;
   const int nb = sort_blocks(cap);
   uint32_t* hist = reinterpret_cast<uint32_t*>(temp);
-  uint32_t* digit_total = hist + (size_t)nb * kRadix;
-  const size_t smem = sizeof(DownsweepSmem);
+  uint32_t* digit_total = hist + (size_t)nb * (1u << rp.bits);
   ensure_sort_attributes();
   uint64_t* kin = k0; uint32_t* vin = v0; uint64_t* kout = k1; uint32_t* vout = v1;
-  for (int p = 0; p < passes; ++p) {
-    const int shift = lo_bit + 8 * p;
-    radix_upsweep_kernel<<<nb, kSortThreads, 0, stream>>>(kin, d_start, d_n, cap, shift, hist, nb);
-    radix_scan_rows_kernel<<<kRadix, 1024, 0, stream>>>(hist, nb, digit_total);
-    radix_downsweep_kernel<<<nb, kSortThreads, smem, stream>>>(kin, vin, kout, vout, d_start, d_n, cap, shift,
-                                                               hist, digit_total, nb);
+  for (int p = 0; p < rp.passes; ++p) {
+    const int shift = lo_bit + rp.bits * p;
+    if (rp.bits == 8) radix_pass<8>(kin, vin, kout, vout, d_start, d_n, cap, shift, hist, digit_total, nb, stream);
+    else if (rp.bits == 9) radix_pass<9>(kin, vin, kout, vout, d_start, d_n, cap, shift, hist, digit_total, nb, stream);
+    else radix_pass<10>(kin, vin, kout, vout, d_start, d_n, cap, shift, hist, digit_total, nb, stream);
     std::swap(kin, kout);
     std::swap(vin, vout);
   }
-  return passes & 1;
+  return rp.passes & 1;
 }
 
 // --------------------------------------------------------------------------
