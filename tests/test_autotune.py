@@ -57,7 +57,8 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
 
     geos = torch.zeros(r.P, 8)
     sh0, shs = torch.zeros(r.P, 3), torch.zeros(r.P, 15, 3)
-    res = autotune.tune_batched(r, geos, sh0, shs, 3, timer=timer)
+    space = dict(autotune.DEFAULT_SPACE, bwd=[(True, 0), (False, 0), (True, 3), (True, 2)])
+    res = autotune.tune_batched(r, geos, sh0, shs, 3, space=space, timer=timer)
     assert not res["cached"]
     assert res["choice"]["tile"] == (8, 64)
     assert res["choice"]["sort"] == (256, 4096)
