@@ -12,6 +12,9 @@ gradients agree up to the order of floating-point additions):
 * ``sort`` -- segment-size buckets of the per-tile segment sort: the largest
   segment sorted by one small CTA and the chunk length of the chunked sort
   (``BatchedRasterizer.set_sort_buckets``).
+* ``reduce`` -- backward gradient reduction threshold: records touched by at
+  most this many lanes of a warp add their gradients with shared-memory
+  atomics instead of a warp reduce-scatter (``set_reduction``).
 * ``tile`` -- compositing tile size of the batched path (8, 16 or 32 pixels)
   with the voxel-staging depth (records staged into shared memory per round)
   (``BatchedRasterizer.set_tile_size``; the tile size changes the binning, so
@@ -33,6 +36,7 @@ DEFAULT_SPACE = {
     "sort": [(512, 4096), (256, 4096), (1024, 4096), (512, 2048)],
     "fwd": [(True, 0), (False, 0)],
     "bwd": [(True, 0), (False, 0)],
+    "reduce": [1, 2, 4, 8],
 }
 
 
@@ -92,6 +96,8 @@ def apply(raster, choice):
         raster.set_tile_size(int(ts), int(sb))
     if "sort" in choice:
         raster.set_sort_buckets(*[int(x) for x in choice["sort"]])
+    if "reduce" in choice:
+        raster.set_reduction(int(choice["reduce"]))
     f = choice.get("fwd", (True, 0))
     b = choice.get("bwd", (True, 0))
     raster.set_schedule(fwd_ordered=bool(f[0]), bwd_ordered=bool(b[0]), fwd_ctas_per_sm=int(f[1]),
@@ -120,7 +126,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
 
     M = 1 + shs.shape[1]
     choice = {"tile": DEFAULT_SPACE["tile"][0], "sort": DEFAULT_SPACE["sort"][0], "fwd": DEFAULT_SPACE["fwd"][0],
-              "bwd": DEFAULT_SPACE["bwd"][0]}
+              "bwd": DEFAULT_SPACE["bwd"][0], "reduce": DEFAULT_SPACE["reduce"][0]}
     timings = {}
     gen = torch.Generator(device=raster.dev)
     gen.manual_seed(0)
@@ -148,7 +154,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
         dC, dT = upstream()
         state["grads"] = raster.backward(geos, state["out"][1], dC, dT, sh_degree, M, state.get("grads"))
 
-    stages = [("tile", step), ("sort", prepare), ("fwd", render), ("bwd", backward)]
+    stages = [("tile", step), ("sort", prepare), ("fwd", render), ("bwd", backward), ("reduce", backward)]
     for name, fn in stages:
         cands = space.get(name)
         if not cands:
@@ -158,7 +164,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
             apply(raster, dict(choice, **{name: cand}))
             if name == "tile":
                 raster.fit_capacity(sh0, shs, sh_degree)
-            if name in ("fwd", "bwd"):
+            if name in ("fwd", "bwd", "reduce"):
                 raster.prepare(sh0, shs, sh_degree)
                 render()
             t = timer(fn, reps, warmup)

@@ -54,6 +54,7 @@ class BatchedRasterizer:
         self.staging = 64 if self.tile_size == 8 else 256
         self.schedule = (3, 0, 0)
         self.sort_buckets = (512, 4096)
+        self.atomic_lanes = 1
         self._make_plan(0 if capacity is None else int(capacity))
         self.capacity_auto = capacity is None
 
@@ -76,6 +77,14 @@ class BatchedRasterizer:
         check(L.svr_batch_plan_set_schedule(plan, *self.schedule), "batch_plan_set_schedule")
         check(L.svr_batch_plan_set_sort_buckets(plan, *self.sort_buckets), "batch_plan_set_sort_buckets")
         check(L.svr_batch_plan_set_staging(plan, self.staging), "batch_plan_set_staging")
+        check(L.svr_batch_plan_set_reduction(plan, self.atomic_lanes), "batch_plan_set_reduction")
+
+    def set_reduction(self, atomic_lanes=1):
+        """Backward: records with at most ``atomic_lanes`` contributing lanes
+        in a warp add their gradients with shared atomics instead of the warp
+        reduce-scatter (only the order of additions changes)."""
+        check(lib().svr_batch_plan_set_reduction(self.plan, int(atomic_lanes)), "batch_plan_set_reduction")
+        self.atomic_lanes = int(atomic_lanes)
 
     def set_tile_size(self, tile_size, staging=None):
         """Compositing tile size (8, 16 or 32 pixels) and records staged per

@@ -199,51 +199,72 @@ duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const int
 
 // dL/dSH of every voxel summed over views: sum_v basis(dir_v) * dL/drgb_v
 // (sh_compute.cu:110-176 per view).  Views where the voxel got no gradient
-// are skipped.
+// are skipped.  Each CTA stages its voxels' 3 + 3*(M-1) outputs in shared
+// memory and stores them as contiguous rows (the per-voxel rows of dsh0 and
+// dshs are 12 B and 180 B long, too short for coalesced per-thread stores).
+constexpr int kShBwThreads = 128;
+
 template <int DEG>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kShBwThreads)
 sh_bw_batch_kernel(const __grid_constant__ ViewTable views, int P, int M, const float* __restrict__ centers,
                    const float* __restrict__ drgbs, float* __restrict__ dsh0, float* __restrict__ dshs) {
+  constexpr int NB = (DEG + 1) * (DEG + 1) - 1;
   __shared__ float s_pos[kMaxViews][3];
+  extern __shared__ __align__(16) float s_out[];  // [kShBwThreads][3 + 3 * (M - 1)] then written out
   for (int v = threadIdx.x; v < views.n; v += blockDim.x) {
     s_pos[v][0] = views.v[v].c2w[3];
     s_pos[v][1] = views.v[v].c2w[7];
     s_pos[v][2] = views.v[v].c2w[11];
   }
   __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P) return;
-  const float cx = centers[3 * (size_t)i], cy = centers[3 * (size_t)i + 1], cz = centers[3 * (size_t)i + 2];
+  const int rest = 3 * (M - 1);
+  const int i0 = blockIdx.x * kShBwThreads;
+  const int i = i0 + threadIdx.x;
   float a0[3] = {0.f, 0.f, 0.f};
-  float acc[15][3];
+  float acc[NB > 0 ? NB : 1][3];
 #pragma unroll
-  for (int k = 0; k < 15; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.f;
-  for (int v = 0; v < views.n; ++v) {
-    const float* g = drgbs + 3 * ((size_t)v * P + i);
-    const float g0 = g[0], g1 = g[1], g2 = g[2];
-    if (g0 == 0.f && g1 == 0.f && g2 == 0.f) continue;
-    float x = cx - s_pos[v][0], y = cy - s_pos[v][1], z = cz - s_pos[v][2];
-    const float rn = rnorm3df(x, y, z);
-    x = x * rn; y = y * rn; z = z * rn;
-    float basis[15];
-    sh_basis_rest<DEG>(x, y, z, basis);
-    a0[0] += kC0 * g0; a0[1] += kC0 * g1; a0[2] += kC0 * g2;
+  for (int k = 0; k < (NB > 0 ? NB : 1); ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.f;
+  if (i < P) {
+    const float cx = centers[3 * (size_t)i], cy = centers[3 * (size_t)i + 1], cz = centers[3 * (size_t)i + 2];
+    for (int v = 0; v < views.n; ++v) {
+      const float* g = drgbs + 3 * ((size_t)v * P + i);
+      const float g0 = g[0], g1 = g[1], g2 = g[2];
+      if (g0 == 0.f && g1 == 0.f && g2 == 0.f) continue;
+      float x = cx - s_pos[v][0], y = cy - s_pos[v][1], z = cz - s_pos[v][2];
+      const float rn = rnorm3df(x, y, z);
+      x = x * rn; y = y * rn; z = z * rn;
+      float basis[15];
+      sh_basis_rest<DEG>(x, y, z, basis);
+      a0[0] += kC0 * g0; a0[1] += kC0 * g1; a0[2] += kC0 * g2;
 #pragma unroll
-    for (int k = 0; k < (DEG + 1) * (DEG + 1) - 1; ++k) {
-      acc[k][0] += basis[k] * g0;
-      acc[k][1] += basis[k] * g1;
-      acc[k][2] += basis[k] * g2;
+      for (int k = 0; k < NB; ++k) {
+        acc[k][0] += basis[k] * g0;
+        acc[k][1] += basis[k] * g1;
+        acc[k][2] += basis[k] * g2;
+      }
     }
   }
-  dsh0[3 * (size_t)i + 0] = a0[0];
-  dsh0[3 * (size_t)i + 1] = a0[1];
-  dsh0[3 * (size_t)i + 2] = a0[2];
-  float* d = dshs + (size_t)i * (M - 1) * 3;
+  // stage: dsh0 rows first ([kShBwThreads][3]), then dshs rows ([kShBwThreads][rest])
+  float* s0 = s_out;
+  float* s1 = s_out + 3 * kShBwThreads;
+  const int t = threadIdx.x;
+  s0[3 * t + 0] = a0[0];
+  s0[3 * t + 1] = a0[1];
+  s0[3 * t + 2] = a0[2];
 #pragma unroll
-  for (int k = 0; k < (DEG + 1) * (DEG + 1) - 1; ++k) {
-    d[3 * k + 0] = acc[k][0];
-    d[3 * k + 1] = acc[k][1];
-    d[3 * k + 2] = acc[k][2];
+  for (int k = 0; k < NB; ++k) {
+    s1[t * rest + 3 * k + 0] = acc[k][0];
+    s1[t * rest + 3 * k + 1] = acc[k][1];
+    s1[t * rest + 3 * k + 2] = acc[k][2];
+  }
+  for (int k = 3 * NB; k < rest; ++k) s1[t * rest + k] = 0.f;  // coefficients above the degree
+  __syncthreads();
+  const int nv = min(kShBwThreads, P - i0);
+  float* o0 = dsh0 + 3 * (size_t)i0;
+  for (int e = t; e < 3 * nv; e += kShBwThreads) o0[e] = s0[e];
+  if (rest > 0) {
+    float* o1 = dshs + (size_t)rest * i0;
+    for (int e = t; e < rest * nv; e += kShBwThreads) o1[e] = s1[e];
   }
 }
 
@@ -294,6 +315,7 @@ struct svr_batch_plan {
   int seg_small_n, seg_chunk;  // segment-sort buckets (svr_batch_plan_set_sort_buckets)
   int tile_size;               // compositing tile size (8, 16 or 32), fixed at creation
   int stage;                   // records staged per round (svr_batch_plan_set_staging)
+  int atomic_lanes;            // backward reduction threshold (svr_batch_plan_set_reduction)
   // workspace layout (byte offsets)
   size_t o_header, o_ndup, o_scan, o_bbox, o_quad, o_scan_tmp, o_rgbs, o_drgbs;
   size_t o_ka, o_kb, o_va, o_vb, o_sort_tmp, o_ranges, o_tile_last, o_ncontrib;
@@ -489,6 +511,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->bwd_ctas_per_sm = 0;
   p->seg_small_n = 512;
   p->seg_chunk = 4096;
+  p->atomic_lanes = 1;
   ensure_segsort_attributes();
   ensure_fwd_batch_attributes();
   ensure_bwd_batch_attributes();
@@ -516,6 +539,12 @@ int svr_batch_plan_set_staging(svr_batch_plan* p, int stage) {
 }
 
 int svr_batch_plan_tile_size(const svr_batch_plan* p) { return p ? p->tile_size : 0; }
+
+int svr_batch_plan_set_reduction(svr_batch_plan* p, int atomic_lanes) {
+  if (!p || atomic_lanes < 1 || atomic_lanes > 32) return SVR_ERR_SHAPE;
+  p->atomic_lanes = atomic_lanes;
+  return SVR_OK;
+}
 
 int svr_batch_plan_set_sort_buckets(svr_batch_plan* p, int small_n, int chunk) {
   if (!p || !seg_buckets_supported(small_n, chunk)) return SVR_ERR_SHAPE;
@@ -638,7 +667,8 @@ int svr_batch_backward(svr_batch_plan* p, void* ws, const float* vox_centers, co
   cudaMemsetAsync(q.drgbs, 0, (size_t)p->V * p->P * 12, stream);
   VoxelArrays va{q.bbox, vox_centers, vox_lengths, geos_bf16 ? nullptr : (const float*)geos,
                  geos_bf16 ? (const __nv_bfloat16*)geos : nullptr, q.rgbs};
-  BwdTileIn in{out_T, q.ncontrib, dL_dcolor, nullptr, nullptr, dL_dT, nullptr, nullptr, 0.f, 0.f, 0.f};
+  BwdTileIn in{out_T, q.ncontrib, dL_dcolor, nullptr, nullptr, dL_dT, nullptr, nullptr, 0.f, 0.f, 0.f,
+               p->atomic_lanes};
   BwdTileOut out{dL_dgeos, q.drgbs, subdiv, q.header + 1};
   const bool ordered = (p->order_flags & 2) != 0;
   if (ordered) build_tile_order(p, q, q.tile_last, q.order_bwd, stream);
@@ -656,12 +686,14 @@ int svr_batch_sh_backward(svr_batch_plan* p, void* ws, const float* vox_centers,
     return SVR_ERR_SHAPE;
   BatchPtrs q = ptrs(p, ws);
   const int P = (int)p->P;
-  const int g = (P + 255) / 256;
+  const int g = (P + kShBwThreads - 1) / kShBwThreads;
+  const size_t smem = (size_t)kShBwThreads * (3 + 3 * (M - 1)) * sizeof(float);
+  if (smem > 48 * 1024) return SVR_ERR_SHAPE;  // M <= 32 coefficients per channel
   switch (sh_degree) {
-    case 0: sh_bw_batch_kernel<0><<<g, 256, 0, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
-    case 1: sh_bw_batch_kernel<1><<<g, 256, 0, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
-    case 2: sh_bw_batch_kernel<2><<<g, 256, 0, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
-    default: sh_bw_batch_kernel<3><<<g, 256, 0, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
+    case 0: sh_bw_batch_kernel<0><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
+    case 1: sh_bw_batch_kernel<1><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
+    case 2: sh_bw_batch_kernel<2><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
+    default: sh_bw_batch_kernel<3><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
   }
   return check_last();
 }

@@ -334,7 +334,7 @@ int svr_rasterize_backward(const svr_camera* cam, int n_samp, int64_t P, int64_t
   VoxelArrays va{g.bbox, vox_centers, vox_lengths, geos, nullptr, rgbs};
   BwdTileIn in{out_T, im.n_contrib, dL_dcolor, need_depth ? dL_ddepth : nullptr,
                need_normal ? dL_dnormal : nullptr, dL_dT, lambda_R_concen > 0 ? gt_color : nullptr,
-               need_dist ? out_depth : nullptr, lambda_R_concen, lambda_ascending, lambda_dist};
+               need_dist ? out_depth : nullptr, lambda_R_concen, lambda_ascending, lambda_dist, 1};
   BwdTileOut out{dL_dgeos, dL_drgbs, subdiv_p_bw, g.header + 1};
   launch_render_bwd(vp, im.ranges, im.tile_last, num_rendered > 0 ? bl.vals_b : nullptr, va, in, out, n_samp,
                     need_depth != 0, need_dist, need_normal != 0, stream);

@@ -26,6 +26,9 @@ struct BwdTileIn {
   const float* gt_color;   // [3,H,W] or nullptr
   const float* out_depth;  // [3,H,W] or nullptr (distortion prefix sums)
   float lambda_R_concen, lambda_ascending, lambda_dist;
+  // A record's gradients from at most this many lanes go straight into its
+  // shared accumulator with atomics; more lanes use the warp reduce-scatter.
+  int atomic_lanes;
 };
 
 struct BwdTileOut {
@@ -344,7 +347,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
         const uint32_t act_mask = __ballot_sync(0xffffffffu, contrib);
         if (act_mask == 0u) continue;
         float* acc = s_grad + j * kGradStride;
-        if (__popc(act_mask) == 1) {  // one lane: its values are the totals
+        if (__popc(act_mask) <= in.atomic_lanes) {  // few lanes: add their values directly
           if (contrib) {
 #pragma unroll
             for (int c = 0; c < 12; ++c) atomicAdd(acc + c, gp[c]);

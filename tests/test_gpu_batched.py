@@ -264,14 +264,14 @@ def _render_and_grads(r, C, wC, wT):
     return color.clone(), T.clone(), dgeo.clone(), sub.clone(), dsh0.clone(), dshs.clone(), total
 
 
-@pytest.mark.parametrize("tile,stage,order,ctas,buckets", [
-    (8, 64, (True, True), (0, 0), (512, 4096)),
-    (32, 256, (True, True), (0, 0), (512, 4096)),
-    (16, 128, (True, True), (0, 0), (256, 2048)),
-    (16, 512, (False, False), (0, 0), (1024, 4096)),
-    (16, 256, (False, True), (3, 2), (512, 2048)),
+@pytest.mark.parametrize("tile,stage,order,ctas,buckets,lanes", [
+    (8, 64, (True, True), (0, 0), (512, 4096), 4),
+    (32, 256, (True, True), (0, 0), (512, 4096), 1),
+    (16, 128, (True, True), (0, 0), (256, 2048), 8),
+    (16, 512, (False, False), (0, 0), (1024, 4096), 2),
+    (16, 256, (False, True), (3, 2), (512, 2048), 32),
 ])
-def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas, buckets):
+def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas, buckets, lanes):
     """Every tile size, staging depth, compositing schedule and sort-bucket
     setting the autotuner may pick renders bit-identical images and T (a pixel
     sees the same instances in the same order) and the same gradients up to
@@ -286,6 +286,7 @@ def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas,
     r.set_staging(stage)
     r.set_schedule(fwd_ordered=order[0], bwd_ordered=order[1], fwd_ctas_per_sm=ctas[0], bwd_ctas_per_sm=ctas[1])
     r.set_sort_buckets(*buckets)
+    r.set_reduction(lanes)
     got = _render_and_grads(r, c1, wC, wT)
     assert torch.equal(got[0], base[0]), "colour differs"
     assert torch.equal(got[1], base[1]), "T differs"
@@ -307,7 +308,7 @@ def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
     base = _render_and_grads(r0, c1, wC, wT)
     r, _ = _raster(c1)
     res = tune_batched(r, c1.geos, c1.sh0, c1.shs, 3, reps=2, warmup=1)
-    assert not res["cached"] and set(res["choice"]) == {"tile", "sort", "fwd", "bwd"}
+    assert not res["cached"] and set(res["choice"]) == {"tile", "sort", "fwd", "bwd", "reduce"}
     got = _render_and_grads(r, c1, wC, wT)
     assert torch.equal(got[0], base[0])
     assert rel_err(got[2], base[2]) < 1e-5
