@@ -104,7 +104,10 @@ int svr_rasterize_forward(const svr_camera* cam, int n_samp_per_vox, int need_de
 
 /* The two stages of svr_rasterize_forward, callable separately (same
  * arguments): duplication + sort + tile ranges (forward.cu:660-700), then the
- * compositing kernel alone (forward.cu:702-731). */
+ * compositing kernel alone (forward.cu:702-731).  The render stage also ranks
+ * the tiles by list length and stores that work order in the image buffer;
+ * its compositing launch and the backward's run the largest tiles first
+ * (results do not depend on the order). */
 int svr_rasterize_binning(const svr_camera* cam, int64_t P, int64_t num_rendered, const int64_t* octree_paths,
                           void* geom_buffer, void* binning_buffer, size_t binning_bytes, void* image_buffer,
                           size_t image_bytes, int debug, void* stream);

@@ -268,25 +268,6 @@ sh_bw_batch_kernel(const __grid_constant__ ViewTable views, int P, int M, const 
   }
 }
 
-// Work-order key of every tile for the persistent compositing launches:
-// one 8-bit digit, 255 minus an eighth-octave bucket of the tile's cost
-// (instances in [range.x, end), end = tile_last when given), so a stable
-// sort by it lists the tiles largest first and, within a bucket, in tile
-// order.  Thread 0 also stores the tile count the sort reads.
-__global__ void tile_order_keys_kernel(const uint2* __restrict__ ranges, const uint32_t* __restrict__ tile_last,
-                                       uint32_t n_tiles, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                                       uint32_t* __restrict__ d_n) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t == 0) *d_n = n_tiles;
-  if (t >= n_tiles) return;
-  const uint2 r = ranges[t];
-  const uint32_t end = tile_last ? tile_last[t] : r.y;
-  const uint32_t cost = end > r.x ? end - r.x : 0u;
-  const uint32_t bucket = min(255u, (uint32_t)(log2f((float)cost + 1.f) * 7.9f));
-  keys[t] = 255u - bucket;
-  vals[t] = t;
-}
-
 inline int bit_width_u64(uint64_t n) {
   int b = 0;
   while (b < 64 && (n >> b)) ++b;
@@ -379,12 +360,11 @@ BatchPtrs ptrs(const svr_batch_plan* p, void* ws) {
 // [16..] group segments.
 constexpr int kHeaderWords = 16 + 2 * kMaxViews;
 
-// Longest-first work order of all tiles into `order` (see tile_order_keys_kernel).
+// Longest-first work order of all tiles into `order` (see launch_tile_order).
 void build_tile_order(const svr_batch_plan* p, const BatchPtrs& q, const uint32_t* tile_last, uint32_t* order,
                       cudaStream_t stream) {
-  const uint32_t T = (uint32_t)p->total_tiles;
-  tile_order_keys_kernel<<<(T + 255) / 256, 256, 0, stream>>>(q.ranges, tile_last, T, q.okey, q.oval, q.header + 4);
-  launch_radix_sort(q.okey, q.oval, q.okey + T, order, nullptr, q.header + 4, T, 8, q.order_tmp, stream);
+  launch_tile_order(q.ranges, tile_last, (uint32_t)p->total_tiles, q.okey, q.oval, order, q.header + 4, q.order_tmp,
+                    stream);
 }
 
 inline int check_last() { return cudaGetLastError() == cudaSuccess ? SVR_OK : SVR_ERR_CUDA; }

@@ -488,4 +488,34 @@ void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_start, const uin
                                                            ranges);
 }
 
+// --------------------------------------------------------------------------
+// Tile work order for the compositing launches: tiles listed largest first
+// by their instance count (eighth-octave buckets, tile order within a
+// bucket).  Key = one 8-bit digit, 255 minus the bucket; a stable one-pass
+// radix sort gives the order.  Thread 0 also stores the tile count the sort
+// reads.
+// --------------------------------------------------------------------------
+__global__ void tile_order_keys_kernel(const uint2* __restrict__ ranges, const uint32_t* __restrict__ tile_last,
+                                       uint32_t n_tiles, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                       uint32_t* __restrict__ d_n) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) *d_n = n_tiles;
+  if (t >= n_tiles) return;
+  const uint2 r = ranges[t];
+  const uint32_t end = tile_last ? tile_last[t] : r.y;
+  const uint32_t cost = end > r.x ? end - r.x : 0u;
+  const uint32_t bucket = min(255u, (uint32_t)(log2f((float)cost + 1.f) * 7.9f));
+  keys[t] = 255u - bucket;
+  vals[t] = t;
+}
+
+size_t tile_order_temp_bytes(uint32_t n_tiles) { return sort_temp_bytes(n_tiles); }
+
+void launch_tile_order(const uint2* ranges, const uint32_t* tile_last, uint32_t n_tiles, uint64_t* keys,
+                       uint32_t* vals, uint32_t* order, uint32_t* d_n, void* temp, cudaStream_t stream) {
+  if (n_tiles == 0) return;
+  tile_order_keys_kernel<<<(n_tiles + 255) / 256, 256, 0, stream>>>(ranges, tile_last, n_tiles, keys, vals, d_n);
+  launch_radix_sort(keys, vals, keys + n_tiles, order, nullptr, d_n, n_tiles, 8, temp, stream);
+}
+
 }  // namespace svr

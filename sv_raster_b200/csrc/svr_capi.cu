@@ -59,11 +59,17 @@ GeomLayout geom_layout(void* buf, int64_t P) {
   return g;
 }
 
-// ---- image buffer: ranges | tile_last | n_contrib ----------------------------
+// ---- image buffer: ranges | tile_last | n_contrib | tile work orders ---------
 struct ImageLayout {
   uint2* ranges;
   uint32_t* tile_last;
   uint32_t* n_contrib;
+  uint32_t* order;      // [T] tiles largest first (by list length), written by the
+                        // render call, read by the forward and backward launches
+  uint64_t* okey;       // [2T] order sort keys
+  uint32_t* oval;       // [T]
+  uint32_t* ocount;     // tile count read by the order sort
+  void* otemp;          // tile_order_temp_bytes(T)
   size_t bytes;
 };
 
@@ -77,6 +83,11 @@ ImageLayout image_layout(void* buf, int W, int H) {
   im.ranges = c.take<uint2>(T);
   im.tile_last = c.take<uint32_t>(T);
   im.n_contrib = c.take<uint32_t>((size_t)W * H);
+  im.order = c.take<uint32_t>(T);
+  im.okey = c.take<uint64_t>(2 * T);
+  im.oval = c.take<uint32_t>(T);
+  im.ocount = c.take<uint32_t>(1);
+  im.otemp = c.take<char>(tile_order_temp_bytes((uint32_t)T));
   im.bytes = c.size();
   return im;
 }
@@ -289,8 +300,11 @@ int svr_rasterize_render(const svr_camera* cam, int n_samp, int need_depth, int 
   if (!aligned16(geos)) return SVR_ERR_ALIGN;
   VoxelArrays va{c.g.bbox, vox_centers, vox_lengths, geos, nullptr, rgbs};
   FwdTileOut out{c.im.tile_last, c.im.n_contrib, out_color, out_depth, out_normal, out_T, max_w};
+  const uint32_t n_tiles = (uint32_t)(c.vt.v[0].grid_x * c.vt.v[0].grid_y);
+  launch_tile_order(c.im.ranges, nullptr, n_tiles, c.im.okey, c.im.oval, c.im.order, c.im.ocount, c.im.otemp,
+                    stream);
   launch_render_fwd(c.vt.v[0], c.im.ranges, c.n > 0 ? c.bl.vals_b : nullptr, va, out, n_samp, need_depth != 0,
-                    need_distortion != 0, need_normal != 0, track_max_w != 0, stream);
+                    need_distortion != 0, need_normal != 0, track_max_w != 0, c.im.order, stream);
   return check_launch(debug, stream);
 }
 
@@ -336,8 +350,9 @@ int svr_rasterize_backward(const svr_camera* cam, int n_samp, int64_t P, int64_t
                need_normal ? dL_dnormal : nullptr, dL_dT, lambda_R_concen > 0 ? gt_color : nullptr,
                need_dist ? out_depth : nullptr, lambda_R_concen, lambda_ascending, lambda_dist, 1};
   BwdTileOut out{dL_dgeos, dL_drgbs, subdiv_p_bw, g.header + 1};
+  // the forward's tile order (read only: the image buffer is the forward's saved state)
   launch_render_bwd(vp, im.ranges, im.tile_last, num_rendered > 0 ? bl.vals_b : nullptr, va, in, out, n_samp,
-                    need_depth != 0, need_dist, need_normal != 0, stream);
+                    need_depth != 0, need_dist, need_normal != 0, im.order, stream);
   return check_launch(debug, stream);
 }
 

@@ -46,13 +46,22 @@ void ensure_segsort_attributes();
 void launch_tile_segment_sort(const uint2* ranges, int n_tiles, uint64_t* ka, uint32_t* va, uint64_t* kb,
                               uint32_t* vb, int rank_bits, size_t cap, void* temp, cudaStream_t stream,
                               int small_n = 512, int chunk = 4096);
+// Largest-first work order of n_tiles tiles by instance count (cost =
+// tile_last - start when tile_last is given, else the range length) into
+// order[n_tiles]; keys [2 * n_tiles] and vals [n_tiles] are scratch, d_n one
+// device word, temp tile_order_temp_bytes(n_tiles) bytes.
+size_t tile_order_temp_bytes(uint32_t n_tiles);
+void launch_tile_order(const uint2* ranges, const uint32_t* tile_last, uint32_t n_tiles, uint64_t* keys,
+                       uint32_t* vals, uint32_t* order, uint32_t* d_n, void* temp, cudaStream_t stream);
 void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_start, const uint32_t* d_n, uint32_t cap,
                         int rank_bits, uint32_t tile_base, uint32_t n_tiles, uint2* ranges, cudaStream_t stream);
 
 // svr_render_fwd.cu / svr_render_bwd.cu
+// Plain one-view launches: one CTA per 16x16 tile; CTA i renders tile
+// order[i] (largest tiles first) or tile i when order is null.
 void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t* vals, const VoxelArrays& va,
                        const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
-                       cudaStream_t stream);
+                       const uint32_t* order, cudaStream_t stream);
 // Multi-view forms (no depth / distortion / normal outputs): persistent
 // grids taking tiles from `counter` (zeroed here) in the order of `order`
 // (identity when null); ctas_per_sm caps the resident CTAs per SM (0 = as
@@ -66,7 +75,7 @@ void launch_render_fwd_batch(const ViewTable& views, int n_items, const uint2* r
                              uint32_t* counter, int ctas_per_sm, cudaStream_t stream);
 void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t* tile_last, const uint32_t* vals,
                        const VoxelArrays& va, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
-                       bool dist, bool normal, cudaStream_t stream);
+                       bool dist, bool normal, const uint32_t* order, cudaStream_t stream);
 void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
                              size_t rgb_view_stride, const BwdTileIn& in, const BwdTileOut& out, int ns, int tile,

@@ -16,6 +16,7 @@ struct BwdArgs {
   VoxelArrays va;
   BwdTileIn in;
   BwdTileOut out;
+  const uint32_t* order;  // CTA i renders tile order[i] (identity when null)
 };
 
 template <class CFG>
@@ -33,8 +34,8 @@ render_bwd_kernel(const __grid_constant__ BwdArgs a) {
   BwdSmem<PlainTile>& sm = *reinterpret_cast<BwdSmem<PlainTile>*>(smem_raw);
   if (threadIdx.x < 12) sm.c2w[threadIdx.x] = a.vp.c2w[threadIdx.x];
   __syncthreads();
-  const int tile_x = blockIdx.x, tile_y = blockIdx.y;
-  const int tile = tile_y * a.vp.grid_x + tile_x;
+  const int tile = a.order ? (int)a.order[blockIdx.x] : (int)blockIdx.x;
+  const int tile_x = tile % a.vp.grid_x, tile_y = tile / a.vp.grid_x;
   render_tile_bwd<PlainTile, NS, DEPTH, DIST, NORMAL>(a.vp, sm.c2w, tile_x, tile_y, a.ranges[tile], a.tile_last[tile],
                                                       a.vals, a.va, a.in, a.out, sm.s, sm.grad);
 }
@@ -107,9 +108,9 @@ static_assert(sizeof(BwdSmem<PlainTile>) <= 48 * 1024, "plain backward staging m
 
 void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t* tile_last, const uint32_t* vals,
                        const VoxelArrays& va, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
-                       bool dist, bool normal, cudaStream_t stream) {
-  BwdArgs args{vp, ranges, tile_last, vals, va, in, out};
-  const dim3 grid(vp.grid_x, vp.grid_y);
+                       bool dist, bool normal, const uint32_t* order, cudaStream_t stream) {
+  BwdArgs args{vp, ranges, tile_last, vals, va, in, out, order};
+  const dim3 grid(vp.grid_x * vp.grid_y);
   SVR_BWD_SWITCH(render_bwd_kernel)
 }
 

@@ -27,6 +27,7 @@ struct FwdArgs {
   const uint32_t* vals;
   VoxelArrays va;
   FwdTileOut out;
+  const uint32_t* order;  // CTA i renders tile order[i] (identity when null)
 };
 
 template <int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
@@ -37,8 +38,9 @@ render_fwd_kernel(const __grid_constant__ FwdArgs a) {
   __shared__ uint32_t s_red[PlainTile::NW];
   if (threadIdx.x < 12) s_c2w[threadIdx.x] = a.vp.c2w[threadIdx.x];
   __syncthreads();
-  const int tile_x = blockIdx.x, tile_y = blockIdx.y;
-  const uint2 range = a.ranges[tile_y * a.vp.grid_x + tile_x];
+  const int tile = a.order ? (int)a.order[blockIdx.x] : (int)blockIdx.x;
+  const int tile_x = tile % a.vp.grid_x, tile_y = tile / a.vp.grid_x;
+  const uint2 range = a.ranges[tile];
   render_tile_fwd<PlainTile, NS, DEPTH, DIST, NORMAL, MAXW>(a.vp, s_c2w, tile_x, tile_y, range, a.vals, a.va, a.out,
                                                             s, s_red);
 }
@@ -131,9 +133,9 @@ render_fwd_batch_kernel(const __grid_constant__ FwdBatchArgs a) {
 
 void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t* vals, const VoxelArrays& va,
                        const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
-                       cudaStream_t stream) {
-  FwdArgs args{vp, ranges, vals, va, out};
-  const dim3 grid(vp.grid_x, vp.grid_y);
+                       const uint32_t* order, cudaStream_t stream) {
+  FwdArgs args{vp, ranges, vals, va, out, order};
+  const dim3 grid(vp.grid_x * vp.grid_y);
   SVR_FWD_DISPATCH(render_fwd_kernel, grid, stream, args);
 }
 
