@@ -219,6 +219,12 @@ typedef struct svr_batch_plan svr_batch_plan;
 int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_t capacity, int n_samp_per_vox,
                           int max_level, int tile_size, svr_batch_plan** plan, size_t* workspace_bytes);
 void svr_batch_plan_destroy(svr_batch_plan* plan);
+/* The plan ranks every (voxel, quadrant) pair once, on the first
+ * svr_batch_prepare, from the octree paths it is given (one radix sort of 8P
+ * keys); instances are then keyed by that rank position.  The table is
+ * rebuilt when prepare sees a different octree_paths pointer or after this
+ * call (for paths changed in place). */
+int svr_batch_plan_invalidate_geometry(svr_batch_plan* plan);
 /* Compositing schedule of svr_batch_render / svr_batch_backward: both are
  * persistent launches that take (view, tile) items from a device counter.
  * order_flags bit 0 (forward) / bit 1 (backward), both set by default, rank

@@ -78,6 +78,7 @@ _SIGS = {
                                       ctypes.POINTER(c_p), ctypes.POINTER(c_sz)]),
     "svr_batch_plan_destroy": (None, [c_p]),
     "svr_batch_plan_set_schedule": (c_int, [c_p, c_int, c_int, c_int]),
+    "svr_batch_plan_invalidate_geometry": (c_int, [c_p]),
     "svr_batch_plan_set_sort_buckets": (c_int, [c_p, c_int, c_int]),
     "svr_batch_plan_set_staging": (c_int, [c_p, c_int]),
     "svr_batch_plan_tile_size": (c_int, [c_p]),

@@ -7,12 +7,16 @@
 // the results are those of the plain path:
 //   - projection is project_voxel (preprocess.cu:24-132 arithmetic), fused
 //     with the SH colour of each visible (voxel, view) (sh_compute.cu:54-106);
-//   - instances of all views share one flat array, view-major; views are
-//     grouped so that a group's [tile | Morton rank] key fits in 64 bits and
-//     each group is sorted as one segment.  Keys use a compressed rank: with
-//     every voxel at octree level <= L < 16, the rank's lowest 3*(16-L) bits
-//     are the quadrant repeated, so (rank >> 3*(16-L)) << 3 | quadrant orders
-//     instances exactly as the full 48-bit rank does;
+//   - instances of all views share one flat array, view-major, keyed
+//     [tile | rank position]: the position of the instance's (voxel,
+//     quadrant) pair in the ascending order of all 8P pairs' Morton ranks
+//     (ties by voxel, then quadrant: the reference's generation order).  The
+//     positions are view-independent, built once per plan by one radix sort,
+//     and order instances exactly as the 48-bit ranks do, in ceil(log2 8P)
+//     bits instead of 48.  The rank itself is compressed for the position
+//     sort: with every voxel at octree level <= L < 16 its lowest 3*(16-L)
+//     bits are the quadrant repeated, so (rank >> 3*(16-L)) << 3 | quadrant
+//     orders pairs exactly as the full rank does;
 //   - compositing / backward are the same per-tile device functions.
 #include <cstdlib>
 #include <cstring>
@@ -28,6 +32,11 @@
 #include "svr_sh.cuh"
 
 using namespace svr;
+
+namespace svr {
+// Instance keys: tile id above bit 32, rank position below.
+constexpr int kPosShift = 32;
+}  // namespace svr
 
 namespace {
 constexpr size_t kAlign = 256;
@@ -53,8 +62,9 @@ template <int DEG, typename TS>
 __global__ void __launch_bounds__(128)
 project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* __restrict__ centers,
                   const float* __restrict__ lengths, const TS* __restrict__ sh0, const TS* __restrict__ shs, int M,
-                  uint32_t* __restrict__ ndup, uint2* __restrict__ bboxes, uint32_t* __restrict__ quads,
-                  float* __restrict__ rgbs) {
+                  const int64_t* __restrict__ octpaths, int level_low_bits, uint32_t* __restrict__ ndup,
+                  uint2* __restrict__ bboxes, uint32_t* __restrict__ quads, float* __restrict__ rgbs,
+                  uint32_t* __restrict__ err) {
   constexpr int NB = (DEG + 1) * (DEG + 1) - 1;  // rest coefficients per channel
   __shared__ float s_m[kMaxViews][24];           // w2c (12) and c2w (12) of every view
   for (int t = threadIdx.x; t < views.n * 24; t += blockDim.x) {
@@ -64,6 +74,9 @@ project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* _
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
+  // voxels deeper than the plan's max level would break the compressed ranks
+  if (level_low_bits > 0 && ((uint64_t)octpaths[i] & ((1ull << level_low_bits) - 1ull)) != 0ull)
+    atomicOr(err, SVR_DEVERR_LEVEL);
   const float cx = centers[3 * (size_t)i], cy = centers[3 * (size_t)i + 1], cz = centers[3 * (size_t)i + 2];
   const float len = lengths[i];
   float c0[3];
@@ -129,9 +142,9 @@ __device__ __forceinline__ int nth_set_bit(uint32_t m, int k) {
 // plain path's generation order: quadrants ascending, tiles row-major,
 // forward.cu:540-562) and writing key and value at its own slot.
 __global__ void __launch_bounds__(256)
-duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const int64_t* __restrict__ octpaths,
+duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const uint32_t* __restrict__ rank_pos,
                        const uint2* __restrict__ bboxes, const uint32_t* __restrict__ quads,
-                       const uint32_t* __restrict__ ndup, const uint32_t* __restrict__ scan, int rank_bits,
+                       const uint32_t* __restrict__ ndup, const uint32_t* __restrict__ scan,
                        uint64_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t cap,
                        uint32_t* __restrict__ err) {
   const int view = blockIdx.y;
@@ -144,14 +157,10 @@ duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const int
   const uint32_t end = valid ? scan[o] : 0u;
   if (n > 0 && end > cap) atomicOr(err, SVR_DEVERR_CAPACITY);
   int tx0 = 0, ty0 = 0, tx1 = 0, ty1 = 0;
-  uint64_t path = 0;
   uint32_t qb = 0;
-  const int low = (rank_bits == kRankBits) ? 0 : kRankBits - (rank_bits - 3);  // 3*(16-L)
   if (n > 0) {
     bbox_tile_rect(bboxes[o], vp.grid_x, vp.grid_y, vp.tile_shift, tx0, ty0, tx1, ty1);
-    path = (uint64_t)octpaths[idx];
     qb = quads[o];
-    if (low > 0 && (path & ((1ull << low) - 1ull)) != 0ull) atomicOr(err, SVR_DEVERR_LEVEL);
     const uint32_t tiles = (uint32_t)((tx1 - tx0 + 1) * (ty1 - ty0 + 1));
     if (tiles * (uint32_t)__popc(qb) != n) atomicOr(err, SVR_DEVERR_DUP_MISMATCH);
   }
@@ -182,19 +191,41 @@ duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const int
     const uint32_t s_w = __shfl_sync(0xffffffffu, w, sl);
     const int s_tx0 = __shfl_sync(0xffffffffu, tx0, sl), s_ty0 = __shfl_sync(0xffffffffu, ty0, sl);
     const uint32_t s_qb = __shfl_sync(0xffffffffu, qb, sl);
-    const uint64_t s_path = __shfl_sync(0xffffffffu, path, sl);
     const uint32_t slot = run0 + p;
     if (p < total && slot < cap) {
       const uint32_t qi = k / s_tiles, rem = k - qi * s_tiles;
       const uint32_t ty = (uint32_t)s_ty0 + rem / s_w, tx = (uint32_t)s_tx0 + rem % s_w;
       const uint32_t q = (uint32_t)nth_set_bit(s_qb, (int)qi);
-      const uint64_t full = order_rank(s_path, q);
-      const uint64_t rank = (low == 0) ? full : (((full >> low) << 3) | q);
+      const uint32_t vid = (uint32_t)(blockIdx.x * blockDim.x + (threadIdx.x & ~31) + sl);
       const uint64_t tile = (uint64_t)(vp.sort_tile_off + ty * (uint32_t)vp.grid_x + tx);
-      keys[slot] = (tile << rank_bits) | rank;
-      vals[slot] = make_sort_val((uint32_t)(blockIdx.x * blockDim.x + (threadIdx.x & ~31) + sl), q);
+      keys[slot] = (tile << kPosShift) | rank_pos[8 * (size_t)vid + q];
+      vals[slot] = make_sort_val(vid, q);
     }
   }
+}
+
+// Rank-position table, step 1: the (compressed) Morton rank of every
+// (voxel, quadrant) pair, pair i = 8 * voxel + quadrant, and its index.
+// Thread 0 stores the pair count the sort reads.
+__global__ void rank_pos_keys_kernel(int P, const int64_t* __restrict__ octpaths, int rank_bits,
+                                     uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                     uint32_t* __restrict__ d_n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *d_n = (uint32_t)(8 * (size_t)P);
+  if (i >= 8 * (size_t)P) return;
+  const uint64_t path = (uint64_t)octpaths[i >> 3];
+  const uint32_t q = (uint32_t)(i & 7);
+  const int low = (rank_bits == kRankBits) ? 0 : kRankBits - (rank_bits - 3);  // 3*(16-L)
+  const uint64_t full = order_rank(path, q);
+  keys[i] = (low == 0) ? full : (((full >> low) << 3) | q);
+  vals[i] = (uint32_t)i;
+}
+
+// Step 2: after a stable sort of the keys, position k holds pair vals[k].
+__global__ void rank_pos_scatter_kernel(size_t n, const uint32_t* __restrict__ sorted_pairs,
+                                        uint32_t* __restrict__ rank_pos) {
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) rank_pos[sorted_pairs[k]] = (uint32_t)k;
 }
 
 // dL/dSH of every voxel summed over views: sum_v basis(dir_v) * dL/drgb_v
@@ -286,8 +317,11 @@ struct svr_batch_plan {
   int64_t P;
   size_t cap;
   int n_samp;
-  int rank_bits;
-  int key_bits;  // widest group key (all groups sorted with this many passes)
+  int rank_bits;  // compressed Morton rank width (position-table sort)
+  int pos_bits;   // bits of a rank position (ceil(log2(8P)))
+  int key_bits;   // widest group key (all groups sorted with this many passes)
+  bool pos_ready;                 // rank-position table built for pos_paths
+  const int64_t* pos_paths;
   int64_t total_tiles, total_pixels;
   // compositing schedule (svr_batch_plan_set_schedule)
   int order_flags;        // bit 0: forward tiles largest first, bit 1: backward (else tile order)
@@ -300,7 +334,7 @@ struct svr_batch_plan {
   // workspace layout (byte offsets)
   size_t o_header, o_ndup, o_scan, o_bbox, o_quad, o_scan_tmp, o_rgbs, o_drgbs;
   size_t o_ka, o_kb, o_va, o_vb, o_sort_tmp, o_ranges, o_tile_last, o_ncontrib;
-  size_t o_okey, o_oval, o_order_fwd, o_order_bwd, o_order_tmp;
+  size_t o_okey, o_oval, o_order_fwd, o_order_bwd, o_order_tmp, o_pos;
   size_t bytes;
 };
 
@@ -326,6 +360,7 @@ struct BatchPtrs {
   uint32_t* order_fwd;  // [T]
   uint32_t* order_bwd;  // [T]
   void* order_tmp;
+  uint32_t* rank_pos;   // [8P] position of (voxel, quadrant) in rank order
 };
 
 BatchPtrs ptrs(const svr_batch_plan* p, void* ws) {
@@ -352,12 +387,13 @@ BatchPtrs ptrs(const svr_batch_plan* p, void* ws) {
   q.order_fwd = reinterpret_cast<uint32_t*>(b + p->o_order_fwd);
   q.order_bwd = reinterpret_cast<uint32_t*>(b + p->o_order_bwd);
   q.order_tmp = b + p->o_order_tmp;
+  q.rank_pos = reinterpret_cast<uint32_t*>(b + p->o_pos);
   return q;
 }
 
 // Header words: [0] instance count, [1] error word, [2] forward work counter,
-// [3] backward work counter, [4] tile count read by the order sort,
-// [16..] group segments.
+// [3] backward work counter, [4] tile count read by the order sort, [5] pair
+// count read by the rank-position sort, [16..] group segments.
 constexpr int kHeaderWords = 16 + 2 * kMaxViews;
 
 // Longest-first work order of all tiles into `order` (see launch_tile_order).
@@ -390,6 +426,9 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->cap = (size_t)capacity;
   p->n_samp = n_samp_per_vox;
   p->rank_bits = (max_level >= kMaxLevels) ? kRankBits : 3 * max_level + 3;
+  p->pos_bits = bit_width_u64((uint64_t)(8 * P - 1));
+  p->pos_ready = false;
+  p->pos_paths = nullptr;
   p->vt.n = n_views;
   int64_t tiles = 0, pix = 0;
   for (int v = 0; v < n_views; ++v) {
@@ -440,7 +479,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
     int kb = 0;
     while (v < n_views) {
       const uint64_t t2 = gt_tiles + (uint64_t)p->vt.v[v].grid_x * p->vt.v[v].grid_y;
-      const int kb2 = p->rank_bits + bit_width_u64(t2);
+      const int kb2 = kPosShift + bit_width_u64(t2);
       if (kb2 > key_limit && gt_tiles > 0) break;
       if (kb2 > 64) {  // a single view does not fit
         delete p;
@@ -472,11 +511,13 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->o_scan_tmp = take(scan_temp_bytes(VP));
   p->o_rgbs = take(VP * 12);
   p->o_drgbs = take(VP * 12);
-  p->o_ka = take(p->cap * 8);
-  p->o_kb = take(p->cap * 8);
-  p->o_va = take(p->cap * 4);
-  p->o_vb = take(p->cap * 4);
-  p->o_sort_tmp = take(std::max(sort_temp_bytes(p->cap), seg_sort_temp_bytes(p->cap, (int)tiles)));
+  // the instance arrays also serve the one-time sort of the 8P rank keys
+  const size_t kv = std::max(p->cap, (size_t)(8 * P));
+  p->o_ka = take(kv * 8);
+  p->o_kb = take(kv * 8);
+  p->o_va = take(kv * 4);
+  p->o_vb = take(kv * 4);
+  p->o_sort_tmp = take(std::max(sort_temp_bytes(kv), seg_sort_temp_bytes(p->cap, (int)tiles)));
   p->o_ranges = take((size_t)tiles * 8);
   p->o_tile_last = take((size_t)tiles * 4);
   p->o_ncontrib = take((size_t)pix * 4);
@@ -485,6 +526,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->o_order_fwd = take((size_t)tiles * 4);
   p->o_order_bwd = take((size_t)tiles * 4);
   p->o_order_tmp = take(sort_temp_bytes((size_t)tiles));
+  p->o_pos = take((size_t)(8 * P) * 4);
   p->bytes = align_up(off) + kAlign;
   p->order_flags = 3;
   p->fwd_ctas_per_sm = 0;
@@ -502,6 +544,12 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
 }
 
 void svr_batch_plan_destroy(svr_batch_plan* plan) { delete plan; }
+
+int svr_batch_plan_invalidate_geometry(svr_batch_plan* p) {
+  if (!p) return SVR_ERR_SHAPE;
+  p->pos_ready = false;
+  return SVR_OK;
+}
 
 int svr_batch_plan_set_schedule(svr_batch_plan* p, int order_flags, int fwd_ctas_per_sm, int bwd_ctas_per_sm) {
   if (!p || order_flags < 0 || order_flags > 3 || fwd_ctas_per_sm < 0 || bwd_ctas_per_sm < 0 ||
@@ -571,15 +619,17 @@ int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, 
   const size_t VP = (size_t)p->V * p->P;
   cudaMemsetAsync(q.header, 0, kHeaderWords * sizeof(uint32_t), stream);
   const dim3 pgrid((P + 127) / 128);
+  const int level_low = (p->rank_bits == kRankBits) ? 0 : kRankBits - (p->rank_bits - 3);  // 3*(16-L)
 #define SVR_PROJ(D)                                                                                           \
   if (sh_bf16)                                                                                                \
     project_sh_kernel<D, __nv_bfloat16><<<pgrid, 128, 0, stream>>>(                                           \
-        p->vt, P, vox_centers, vox_lengths, (const __nv_bfloat16*)sh0, (const __nv_bfloat16*)shs, M, q.ndup, \
-        q.bbox, q.quad, q.rgbs);                                                                              \
+        p->vt, P, vox_centers, vox_lengths, (const __nv_bfloat16*)sh0, (const __nv_bfloat16*)shs, M,         \
+        octree_paths, level_low, q.ndup, q.bbox, q.quad, q.rgbs, q.header + 1);                               \
   else                                                                                                        \
     project_sh_kernel<D, float><<<pgrid, 128, 0, stream>>>(p->vt, P, vox_centers, vox_lengths,               \
-                                                           (const float*)sh0, (const float*)shs, M, q.ndup,  \
-                                                           q.bbox, q.quad, q.rgbs);
+                                                           (const float*)sh0, (const float*)shs, M,          \
+                                                           octree_paths, level_low, q.ndup, q.bbox, q.quad,  \
+                                                           q.rgbs, q.header + 1);
   const dim3 grid((P + 255) / 256, p->V);
   switch (sh_degree) {
     case 0: SVR_PROJ(0) break;
@@ -592,28 +642,40 @@ int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, 
   uint32_t* segs = q.header + 16;
   group_segments_kernel<<<1, 64, 0, stream>>>(p->gt, P, q.scan, (uint32_t)p->cap, segs);
   cudaMemsetAsync(q.ranges, 0, (size_t)p->total_tiles * sizeof(uint2), stream);
+  if (!p->pos_ready || p->pos_paths != octree_paths) {
+    // Rank positions of all (voxel, quadrant) pairs: one stable radix sort of
+    // the 8P compressed ranks in the (still free) instance arrays.
+    const size_t n8 = 8 * (size_t)P;
+    rank_pos_keys_kernel<<<(unsigned)((n8 + 255) / 256), 256, 0, stream>>>(P, octree_paths, p->rank_bits, q.ka, q.va,
+                                                                          q.header + 5);
+    const int in_b = launch_radix_sort(q.ka, q.va, q.kb, q.vb, nullptr, q.header + 5, (uint32_t)n8, p->rank_bits,
+                                       q.sort_tmp, stream);
+    rank_pos_scatter_kernel<<<(unsigned)((n8 + 255) / 256), 256, 0, stream>>>(n8, in_b ? q.vb : q.va, q.rank_pos);
+    p->pos_ready = true;
+    p->pos_paths = octree_paths;
+  }
   if (p->cap > 0) {
     // Two-level sort: LSD radix passes over the tile bits only put every
     // tile's instances together in generation order (ending in ka/va), then
-    // one CTA per tile sorts its segment by the rank bits into kb/vb.  The
-    // result is the order of one stable sort by the full key.
-    const bool odd = (sort_passes(p->key_bits - p->rank_bits) & 1) != 0;
+    // one CTA per tile sorts its segment by the rank-position bits into
+    // kb/vb.  The result is the order of one stable sort by the full key.
+    const bool odd = (sort_passes(p->key_bits - kPosShift) & 1) != 0;
     uint64_t* k0 = odd ? q.kb : q.ka;
     uint32_t* v0 = odd ? q.vb : q.va;
     uint64_t* k1 = odd ? q.ka : q.kb;
     uint32_t* v1 = odd ? q.va : q.vb;
-    duplicate_batch_kernel<<<grid, 256, 0, stream>>>(p->vt, P, octree_paths, q.bbox, q.quad, q.ndup, q.scan,
-                                                     p->rank_bits, k0, v0, (uint32_t)p->cap, q.header + 1);
+    duplicate_batch_kernel<<<grid, 256, 0, stream>>>(p->vt, P, q.rank_pos, q.bbox, q.quad, q.ndup, q.scan, k0, v0,
+                                                     (uint32_t)p->cap, q.header + 1);
     for (int g = 0; g < p->gt.n; ++g) {
       launch_radix_sort(k0, v0, k1, v1, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, p->key_bits, q.sort_tmp,
-                        stream, p->rank_bits);
+                        stream, kPosShift);
       const uint32_t g_tiles = (g + 1 < p->gt.n ? p->gt.tile_base[g + 1] : (uint32_t)p->total_tiles) -
                                p->gt.tile_base[g];
-      launch_tile_ranges(q.ka, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, p->rank_bits, p->gt.tile_base[g],
+      launch_tile_ranges(q.ka, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, kPosShift, p->gt.tile_base[g],
                          g_tiles, q.ranges, stream);
     }
     // the radix histograms in sort_tmp are dead here; the segment sort reuses it
-    launch_tile_segment_sort(q.ranges, (int)p->total_tiles, q.ka, q.va, q.kb, q.vb, p->rank_bits, p->cap,
+    launch_tile_segment_sort(q.ranges, (int)p->total_tiles, q.ka, q.va, q.kb, q.vb, p->pos_bits, p->cap,
                              q.sort_tmp, stream, p->seg_small_n, p->seg_chunk);
   }
   return check_last();

@@ -52,10 +52,11 @@ def _raster(C, max_level=None, views=(0, 1, 2), **kw):
     return r, cams
 
 
-@pytest.mark.parametrize("max_key_bits", [None, 35])
+@pytest.mark.parametrize("max_key_bits", [None, 40])
 def test_batched_forward_equals_plain(c1, max_key_bits, monkeypatch):
     if max_key_bits:
-        monkeypatch.setenv("SVR_MAX_KEY_BITS", str(max_key_bits))  # forces one sort group per view
+        # 32 position bits + 8 bits for one view's tiles: one sort group per view
+        monkeypatch.setenv("SVR_MAX_KEY_BITS", str(max_key_bits))
     r, _ = _raster(c1)
     if max_key_bits:
         assert r.n_groups == 3
