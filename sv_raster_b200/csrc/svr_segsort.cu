@@ -50,13 +50,16 @@ bool seg_buckets_supported(int small_n, int chunk) {
   return (small_n == 256 || small_n == 512 || small_n == 1024) && (chunk == 2048 || chunk == 4096);
 }
 
-// Shared memory of an LSD sort of up to CAP keys by NT threads.  The
-// payload moved with each key is its 16-bit index in the input; values are
-// gathered from global memory once, after the last pass.
-template <int NT, int CAP>
+// Shared memory of an LSD sort of up to CAP keys of type KT by NT threads.
+// The payload moved with each key is its 16-bit index in the input; values
+// are gathered from global memory once, after the last pass.  KT is uint32_t
+// when the sorted bits fit 32 (the batched path's rank positions; the tile
+// bits above them are the same for the whole segment and are put back on the
+// way out), uint64_t otherwise (the plain path's 48-bit ranks).
+template <int NT, int CAP, typename KT>
 struct SortSmem {
   static_assert(CAP <= 65536, "16-bit payload indices");
-  uint64_t k[2][CAP];
+  KT k[2][CAP];
   uint16_t idx[2][CAP];
   uint32_t wcnt[NT / 32][256];  // per-warp digit counts, then per-warp exclusive prefixes
   uint32_t dstart[256];         // exclusive digit starts
@@ -68,8 +71,8 @@ struct SortSmem {
 // buffer index (0 or 1) holding the result.  Warp w owns the contiguous items
 // [w * chunk, (w + 1) * chunk), so ranking warp by warp and digit by digit
 // keeps equal digits in input order.
-template <int NT, int CAP>
-__device__ int smem_lsd_sort(SortSmem<NT, CAP>& sm, int n, int rank_bits) {
+template <int NT, int CAP, typename KT>
+__device__ int smem_lsd_sort(SortSmem<NT, CAP, KT>& sm, int n, int rank_bits) {
   constexpr int NW = NT / 32;
   constexpr int R = CAP / NT;                   // rounds of 32 items per warp at most
   constexpr int DPT = NT >= 256 ? 1 : 256 / NT;  // digits owned per thread (consecutive)
@@ -220,53 +223,62 @@ seg_plan_kernel(const uint2* __restrict__ ranges, int n_tiles, SegLists L) {
   }
 }
 
-template <int SMALL_N>
+// Key bits above a KT key: kept from the segment's first key (they are the
+// same for the whole segment when KT is narrower than the key).
+template <typename KT>
+__device__ __forceinline__ uint64_t high_bits(uint64_t key) {
+  return sizeof(KT) == 8 ? 0ull : (key & 0xFFFFFFFF00000000ull);
+}
+
+template <int SMALL_N, typename KT>
 __global__ void __launch_bounds__(kSmallThreads)
 seg_small_kernel(SegLists L, const uint64_t* __restrict__ ka, const uint32_t* __restrict__ va,
                  uint64_t* __restrict__ kb, uint32_t* __restrict__ vb, int rank_bits) {
-  __shared__ SortSmem<kSmallThreads, SMALL_N> sm;
+  __shared__ SortSmem<kSmallThreads, SMALL_N, KT> sm;
   const uint32_t count = min(L.counters[0], L.small_cap);
   for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
     const uint2 s = L.small[e];
     const int n = (int)s.y;
+    const uint64_t hi = high_bits<KT>(ka[s.x]);
     __syncthreads();  // the previous segment's results have been read out
     for (int i = threadIdx.x; i < n; i += kSmallThreads) {
-      sm.k[0][i] = ka[s.x + i];
+      sm.k[0][i] = (KT)ka[s.x + i];
       sm.idx[0][i] = (uint16_t)i;
     }
     __syncthreads();
     const int cur = smem_lsd_sort(sm, n, rank_bits);
     for (int i = threadIdx.x; i < n; i += kSmallThreads) {
-      kb[s.x + i] = sm.k[cur][i];
+      kb[s.x + i] = hi | (uint64_t)sm.k[cur][i];
       vb[s.x + i] = va[s.x + sm.idx[cur][i]];
     }
   }
 }
 
-template <int CHUNK>
-using ChunkSmem = SortSmem<kChunkThreads, CHUNK>;
+template <int CHUNK, typename KT>
+using ChunkSmem = SortSmem<kChunkThreads, CHUNK, KT>;
 
-template <int CHUNK>
+template <int CHUNK, typename KT>
 __global__ void __launch_bounds__(kChunkThreads, 2)
 seg_chunk_kernel(SegLists L, uint64_t* __restrict__ ka, uint32_t* __restrict__ va, uint64_t* __restrict__ kb,
                  uint32_t* __restrict__ vb, int rank_bits) {
   constexpr int kChunk = CHUNK;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  ChunkSmem<CHUNK>& sm = *reinterpret_cast<ChunkSmem<CHUNK>*>(smem_raw);
+  ChunkSmem<CHUNK, KT>& sm = *reinterpret_cast<ChunkSmem<CHUNK, KT>*>(smem_raw);
   const uint32_t count = min(L.counters[1], L.chunk_cap);
   for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
     const uint4 c = L.chunk[e];
     const int n = (int)c.y;
+    const uint64_t hi = high_bits<KT>(ka[c.x]);
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += kChunkThreads) {
-      sm.k[0][i] = ka[c.x + i];
+      sm.k[0][i] = (KT)ka[c.x + i];
       sm.idx[0][i] = (uint16_t)i;
     }
     __syncthreads();
     const int cur = smem_lsd_sort(sm, n, rank_bits);
     if (c.w == c.y) {  // a single-chunk segment is final
       for (int i = threadIdx.x; i < n; i += kChunkThreads) {
-        kb[c.x + i] = sm.k[cur][i];
+        kb[c.x + i] = hi | (uint64_t)sm.k[cur][i];
         vb[c.x + i] = va[c.x + sm.idx[cur][i]];
       }
     } else {  // the sorted run goes back in place: gather every value before any is overwritten
@@ -282,7 +294,7 @@ seg_chunk_kernel(SegLists L, uint64_t* __restrict__ ka, uint32_t* __restrict__ v
       for (int j = 0; j < kPer; ++j) {
         const int i = threadIdx.x + j * kChunkThreads;
         if (i < n) {
-          ka[c.x + i] = sm.k[cur][i];
+          ka[c.x + i] = hi | (uint64_t)sm.k[cur][i];
           va[c.x + i] = vv[j];
         }
       }
@@ -290,10 +302,10 @@ seg_chunk_kernel(SegLists L, uint64_t* __restrict__ ka, uint32_t* __restrict__ v
   }
 }
 
-template <int CHUNK>
+template <int CHUNK, typename KT>
 struct MergeSmem {
-  uint64_t own[CHUNK];
-  uint64_t other[CHUNK];
+  KT own[CHUNK];
+  KT other[CHUNK];
   uint32_t cnt[CHUNK];  // per own item: keys of the other runs ordered before it
 };
 
@@ -301,15 +313,15 @@ struct MergeSmem {
 // s): thread t walks the merged order's outputs [t * per, (t + 1) * per) and,
 // for every own item it passes, adds the number of other-run keys before it.
 // On equal keys the earlier run comes first.
-template <int CHUNK>
-__device__ __forceinline__ void corank_run(MergeSmem<CHUNK>& sm, uint32_t n_own, uint32_t n_oth,
+template <int CHUNK, typename KT>
+__device__ __forceinline__ void corank_run(MergeSmem<CHUNK, KT>& sm, uint32_t n_own, uint32_t n_oth,
                                            bool own_first_on_tie) {
   const uint32_t total = n_own + n_oth;
   const uint32_t per = (total + kMergeThreads - 1) / kMergeThreads;
   const uint32_t d0 = min(total, threadIdx.x * per), d1 = min(total, d0 + per);
   if (d0 >= d1) return;
   // own[i] comes before other[j] in the merged order
-  auto own_before = [&](uint64_t a, uint64_t b) { return own_first_on_tie ? (a <= b) : (a < b); };
+  auto own_before = [&](KT a, KT b) { return own_first_on_tie ? (a <= b) : (a < b); };
   // i = number of own items among the first d0 outputs: the smallest i with
   // own[i] not before other[d0 - 1 - i]
   uint32_t lo = d0 > n_oth ? d0 - n_oth : 0u, hi = min(d0, n_own);
@@ -329,13 +341,13 @@ __device__ __forceinline__ void corank_run(MergeSmem<CHUNK>& sm, uint32_t n_own,
   }
 }
 
-template <int CHUNK>
+template <int CHUNK, typename KT>
 __global__ void __launch_bounds__(kMergeThreads)
 seg_merge_kernel(SegLists L, const uint64_t* __restrict__ ka, const uint32_t* __restrict__ va,
                  uint64_t* __restrict__ kb, uint32_t* __restrict__ vb) {
   constexpr int kChunk = CHUNK;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  MergeSmem<CHUNK>& sm = *reinterpret_cast<MergeSmem<CHUNK>*>(smem_raw);
+  MergeSmem<CHUNK, KT>& sm = *reinterpret_cast<MergeSmem<CHUNK, KT>*>(smem_raw);
   const uint32_t count = min(L.counters[1], L.chunk_cap);
   const int tid = threadIdx.x;
   for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
@@ -344,9 +356,10 @@ seg_merge_kernel(SegLists L, const uint64_t* __restrict__ ka, const uint32_t* __
     const uint32_t n = c.y, seg0 = c.z, seg_n = c.w;
     const uint32_t r = (c.x - seg0) / kChunk;
     const uint32_t runs = (seg_n + kChunk - 1) / kChunk;
+    const uint64_t hi = high_bits<KT>(ka[seg0]);
     __syncthreads();
     for (uint32_t i = tid; i < n; i += kMergeThreads) {
-      sm.own[i] = ka[c.x + i];
+      sm.own[i] = (KT)ka[c.x + i];
       sm.cnt[i] = 0u;
     }
     for (uint32_t s = 0; s < runs; ++s) {
@@ -354,17 +367,25 @@ seg_merge_kernel(SegLists L, const uint64_t* __restrict__ ka, const uint32_t* __
       const uint32_t s0 = seg0 + s * kChunk;
       const uint32_t ns = min((uint32_t)kChunk, seg_n - s * kChunk);
       __syncthreads();
-      for (uint32_t i = tid; i < ns; i += kMergeThreads) sm.other[i] = ka[s0 + i];
+      for (uint32_t i = tid; i < ns; i += kMergeThreads) sm.other[i] = (KT)ka[s0 + i];
       __syncthreads();
       corank_run(sm, n, ns, /*own_first_on_tie=*/r < s);
     }
     __syncthreads();
     for (uint32_t i = tid; i < n; i += kMergeThreads) {
       const uint32_t pos = i + sm.cnt[i];
-      kb[seg0 + pos] = sm.own[i];
+      kb[seg0 + pos] = hi | (uint64_t)sm.own[i];
       vb[seg0 + pos] = va[c.x + i];
     }
   }
+}
+
+template <int CHUNK, typename KT>
+static void set_chunk_merge_attrs() {
+  cudaFuncSetAttribute(seg_chunk_kernel<CHUNK, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(ChunkSmem<CHUNK, KT>));
+  cudaFuncSetAttribute(seg_merge_kernel<CHUNK, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(MergeSmem<CHUNK, KT>));
 }
 
 void ensure_segsort_attributes() {
@@ -372,14 +393,10 @@ void ensure_segsort_attributes() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
   std::call_once(flags[dev], [] {
-    cudaFuncSetAttribute(seg_chunk_kernel<2048>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(ChunkSmem<2048>));
-    cudaFuncSetAttribute(seg_chunk_kernel<4096>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(ChunkSmem<4096>));
-    cudaFuncSetAttribute(seg_merge_kernel<2048>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(MergeSmem<2048>));
-    cudaFuncSetAttribute(seg_merge_kernel<4096>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(MergeSmem<4096>));
+    set_chunk_merge_attrs<2048, uint64_t>();
+    set_chunk_merge_attrs<4096, uint64_t>();
+    set_chunk_merge_attrs<2048, uint32_t>();
+    set_chunk_merge_attrs<4096, uint32_t>();
   });
 }
 
@@ -390,14 +407,30 @@ static int sm_count() {
   return n > 0 ? n : 148;
 }
 
-template <int CHUNK>
+template <int CHUNK, typename KT>
 static void launch_chunk_and_merge(const SegLists& L, int sms, uint64_t* ka, uint32_t* va, uint64_t* kb,
                                    uint32_t* vb, int rank_bits, cudaStream_t stream) {
   const int chunk_grid = (int)std::min<int64_t>(L.chunk_cap, (int64_t)sms * 2);
-  seg_chunk_kernel<CHUNK><<<chunk_grid, kChunkThreads, sizeof(ChunkSmem<CHUNK>), stream>>>(L, ka, va, kb, vb,
-                                                                                          rank_bits);
+  seg_chunk_kernel<CHUNK, KT><<<chunk_grid, kChunkThreads, sizeof(ChunkSmem<CHUNK, KT>), stream>>>(L, ka, va, kb,
+                                                                                                  vb, rank_bits);
   const int merge_grid = (int)std::min<int64_t>(L.chunk_cap, (int64_t)sms * 2);
-  seg_merge_kernel<CHUNK><<<merge_grid, kMergeThreads, sizeof(MergeSmem<CHUNK>), stream>>>(L, ka, va, kb, vb);
+  seg_merge_kernel<CHUNK, KT><<<merge_grid, kMergeThreads, sizeof(MergeSmem<CHUNK, KT>), stream>>>(L, ka, va, kb,
+                                                                                                  vb);
+}
+
+template <typename KT>
+static void launch_segments(const SegLists& L, int n_tiles, int small_n, int chunk, uint64_t* ka, uint32_t* va,
+                            uint64_t* kb, uint32_t* vb, int rank_bits, cudaStream_t stream) {
+  const int sms = sm_count();
+  const int small_grid = (int)std::min<int64_t>(n_tiles, (int64_t)sms * 12);
+  if (small_n == 256)
+    seg_small_kernel<256, KT><<<small_grid, kSmallThreads, 0, stream>>>(L, ka, va, kb, vb, rank_bits);
+  else if (small_n == 1024)
+    seg_small_kernel<1024, KT><<<small_grid, kSmallThreads, 0, stream>>>(L, ka, va, kb, vb, rank_bits);
+  else
+    seg_small_kernel<512, KT><<<small_grid, kSmallThreads, 0, stream>>>(L, ka, va, kb, vb, rank_bits);
+  if (chunk == 2048) launch_chunk_and_merge<2048, KT>(L, sms, ka, va, kb, vb, rank_bits, stream);
+  else launch_chunk_and_merge<4096, KT>(L, sms, ka, va, kb, vb, rank_bits, stream);
 }
 
 void launch_tile_segment_sort(const uint2* ranges, int n_tiles, uint64_t* ka, uint32_t* va, uint64_t* kb,
@@ -412,13 +445,10 @@ void launch_tile_segment_sort(const uint2* ranges, int n_tiles, uint64_t* ka, ui
   const SegLists L = seg_lists(temp, cap, n_tiles, small_n, chunk);
   cudaMemsetAsync(L.counters, 0, 2 * sizeof(uint32_t), stream);
   seg_plan_kernel<<<(n_tiles + 255) / 256, 256, 0, stream>>>(ranges, n_tiles, L);
-  const int sms = sm_count();
-  const int small_grid = (int)std::min<int64_t>(n_tiles, (int64_t)sms * 12);
-  if (small_n == 256) seg_small_kernel<256><<<small_grid, kSmallThreads, 0, stream>>>(L, ka, va, kb, vb, rank_bits);
-  else if (small_n == 1024) seg_small_kernel<1024><<<small_grid, kSmallThreads, 0, stream>>>(L, ka, va, kb, vb, rank_bits);
-  else seg_small_kernel<512><<<small_grid, kSmallThreads, 0, stream>>>(L, ka, va, kb, vb, rank_bits);
-  if (chunk == 2048) launch_chunk_and_merge<2048>(L, sms, ka, va, kb, vb, rank_bits, stream);
-  else launch_chunk_and_merge<4096>(L, sms, ka, va, kb, vb, rank_bits, stream);
+  // keys whose sorted bits fit 32 are sorted as 32-bit words (the bits above
+  // are the segment's tile, the same for all its keys)
+  if (rank_bits <= 32) launch_segments<uint32_t>(L, n_tiles, small_n, chunk, ka, va, kb, vb, rank_bits, stream);
+  else launch_segments<uint64_t>(L, n_tiles, small_n, chunk, ka, va, kb, vb, rank_bits, stream);
 }
 
 }  // namespace svr
