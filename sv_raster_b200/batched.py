@@ -159,13 +159,11 @@ class BatchedRasterizer:
                                       M, self._stream()), "batch_prepare")
 
     def render(self, geos, out_color=None, out_T=None):
-        """Composite every view; returns flat (color [sum 3HW], T [sum HW])."""
+        """Composite every view; returns flat (color [sum 3HW], T [sum HW]).
+        Every pixel of every view is written, so the outputs need no clearing."""
         if out_color is None:
-            out_color = torch.zeros(3 * self.n_pixels, device=self.dev)
-            out_T = torch.zeros(self.n_pixels, device=self.dev)
-        else:
-            out_color.zero_()
-            out_T.zero_()
+            out_color = torch.empty(3 * self.n_pixels, device=self.dev)
+            out_T = torch.empty(self.n_pixels, device=self.dev)
         check(lib().svr_batch_render(self.plan, self._p(self.ws), self._p(self.centers), self._p(self.lengths),
                                      self._p(geos), int(geos.dtype == torch.bfloat16), self._p(out_color),
                                      self._p(out_T), self._stream()), "batch_render")
@@ -174,8 +172,9 @@ class BatchedRasterizer:
     def backward(self, geos, out_T, dL_dcolor, dL_dT, sh_degree, M, grads=None):
         """Returns (dL_dgeos [P,8], subdiv [P], dL_dsh0 [P,3], dL_dshs [P,M-1,3]) fp32."""
         if grads is None:
+            # dL_dgeos and subdiv accumulate; the SH gradients are overwritten
             grads = (torch.zeros(self.P, 8, device=self.dev), torch.zeros(self.P, device=self.dev),
-                     torch.zeros(self.P, 3, device=self.dev), torch.zeros(self.P, M - 1, 3, device=self.dev))
+                     torch.empty(self.P, 3, device=self.dev), torch.empty(self.P, M - 1, 3, device=self.dev))
         else:
             grads[0].zero_()
             grads[1].zero_()

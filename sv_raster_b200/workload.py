@@ -400,37 +400,54 @@ class BatchedWorkload:
     def e2e(self, steps, warmup):
         """Public autograd API (BatchedRender) with the targets and camera
         matrices copied from pinned host memory each step and the loss read
-        back; cameras are updated in place so the plan stays valid."""
+        back; cameras are updated in place so the plan stays valid.  The next
+        step's targets are uploaded on a copy stream while the current step
+        computes (double-buffered), as a training loop would prefetch them."""
         from .batched import BatchedRender
         dev = self.dev
         host_t = self.target.cpu().pin_memory()
         host_w2c = [torch.from_numpy(c.w2c).pin_memory() for c in self.sc.cameras]
         host_c2w = [torch.from_numpy(c.c2w).pin_memory() for c in self.sc.cameras]
-        tgt = torch.empty_like(self.target)
+        tgt = [torch.empty_like(self.target), torch.empty_like(self.target)]
         geos = self.geos.clone().requires_grad_(True)
         sh0 = self.sh0.clone().requires_grad_(True)
         shs = self.shs.clone().requires_grad_(True)
         h2d = host_t.numel() * 4 + len(self.cams) * 2 * 64
+        main = torch.cuda.current_stream(dev)
+        copy = torch.cuda.Stream(dev)
+        ready = [torch.cuda.Event(), torch.cuda.Event()]  # target buffer uploaded
+        free = [torch.cuda.Event(), torch.cuda.Event()]   # target buffer consumed by its step
 
-        def one_step():
-            tgt.copy_(host_t, non_blocking=True)
+        def upload(k):
+            with torch.cuda.stream(copy):
+                copy.wait_event(free[k % 2])
+                tgt[k % 2].copy_(host_t, non_blocking=True)
+                ready[k % 2].record(copy)
+
+        def one_step(k):
+            upload(k + 1)  # prefetch the next step's inputs behind this step's compute
+            main.wait_event(ready[k % 2])
             for c, a, b in zip(self.cams, host_w2c, host_c2w):
                 c.w2c.copy_(a, non_blocking=True)
                 c.c2w.copy_(b, non_blocking=True)
             color, T = BatchedRender.apply(self.raster, 3, geos, sh0, shs)
-            loss = (self.scale * 0.5 * (color - tgt) ** 2).sum()
+            loss = (self.scale * 0.5 * (color - tgt[k % 2]) ** 2).sum()
+            free[k % 2].record(main)
             loss.backward()
             return float(loss.detach().cpu())
 
-        for _ in range(warmup):
-            one_step()
+        for e in free:
+            e.record(main)
+        upload(0)
+        for k in range(warmup):
+            one_step(k)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        st = torch.cuda.current_stream(dev)
-        e0.record(st)
-        for _ in range(steps):
-            one_step()
-        e1.record(st)
+        e0.record(main)
+        for k in range(warmup, warmup + steps):
+            one_step(k)
+        main.wait_event(ready[(warmup + steps) % 2])  # every upload issued in the timed region has landed
+        e1.record(main)
         torch.cuda.synchronize()
         return dict(ms_total=e0.elapsed_time(e1), h2d=h2d, d2h=4)
 
