@@ -253,6 +253,9 @@ int64_t svr_batch_plan_tiles(const svr_batch_plan* plan);
 int svr_batch_plan_groups(const svr_batch_plan* plan);
 const uint32_t* svr_batch_count_ptr(const svr_batch_plan* plan, const void* workspace);
 uint32_t* svr_batch_error_ptr(const svr_batch_plan* plan, void* workspace);
+/* Packed pixel bbox of every (view, voxel) pair [V,P] (uint2 as uint64:
+ * .x = xmin << 16 | ymin, .y = xmax << 16 | ymax), valid after prepare. */
+const uint64_t* svr_batch_bbox_ptr(const svr_batch_plan* plan, const void* workspace);
 /* Device arrays inside a workspace: rgbs / dL_drgbs [V,P,3], ranges [T] (uint2
  * as uint64), tile_last [T], n_contrib [pixels], n_dup [V,P], sorted values. */
 int svr_batch_arrays(const svr_batch_plan* plan, const void* workspace, const float** rgbs, const float** drgbs,

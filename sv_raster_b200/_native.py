@@ -88,6 +88,7 @@ _SIGS = {
     "svr_batch_plan_groups": (c_int, [c_p]),
     "svr_batch_count_ptr": (c_p, [c_p, c_p]),
     "svr_batch_error_ptr": (c_p, [c_p, c_p]),
+    "svr_batch_bbox_ptr": (c_p, [c_p, c_p]),
     "svr_batch_arrays": (c_int, [c_p, c_p] + [ctypes.POINTER(c_p)] * 7),
     "svr_batch_prepare": (c_int, [c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_int, c_int, c_int, c_p]),
     "svr_batch_render": (c_int, [c_p, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_p]),

@@ -206,7 +206,9 @@ class BatchedRasterizer:
         off = [p.value - base for p in ptrs]
         VP = len(self.cams) * self.P
         ws = self.ws
+        ob = lib().svr_batch_bbox_ptr(self.plan, self._p(self.ws)) - base
         return dict(
+            bbox=ws[ob:ob + 8 * VP].view(torch.int32).view(len(self.cams), self.P, 2),
             rgbs=ws[off[0]:off[0] + 12 * VP].view(torch.float32).view(len(self.cams), self.P, 3),
             drgbs=ws[off[1]:off[1] + 12 * VP].view(torch.float32).view(len(self.cams), self.P, 3),
             ranges=ws[off[2]:off[2] + 8 * self.n_tiles].view(torch.int32).view(self.n_tiles, 2),

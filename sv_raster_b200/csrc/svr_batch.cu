@@ -588,6 +588,10 @@ int svr_batch_plan_groups(const svr_batch_plan* p) { return p ? p->gt.n : 0; }
 const uint32_t* svr_batch_count_ptr(const svr_batch_plan* p, const void* ws) {
   return reinterpret_cast<const uint32_t*>(static_cast<const char*>(ws) + p->o_header);
 }
+const uint64_t* svr_batch_bbox_ptr(const svr_batch_plan* p, const void* ws) {
+  return reinterpret_cast<const uint64_t*>(static_cast<const char*>(ws) + p->o_bbox);
+}
+
 uint32_t* svr_batch_error_ptr(const svr_batch_plan* p, void* ws) {
   return reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + p->o_header) + 1;
 }
