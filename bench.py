@@ -230,6 +230,7 @@ def main():
         # measured DRAM bytes per launch: committed ncu capture of the same
         # kernel on a smaller case, scaled by instances per launch
         traffic = None
+        issue = None
         tf = os.path.join(ROOT, "profiles", "render_traffic.json")
         if os.path.exists(tf) and dom["name"] in ("render_fwd", "render_bwd"):
             r = getattr(wl, "raster", None)
@@ -238,6 +239,11 @@ def main():
             if t is not None:
                 inst = wl.instances_per_view() * (n_views if args.mode == "batched" else 1)
                 traffic = round(t[dom["name"]]["dram_bytes"] / t["instances_per_launch"] * inst)
+                # the compositing kernels are bounded by instruction issue, not HBM
+                ipc = t[dom["name"]].get("ipc")
+                if ipc:
+                    issue = {"ipc": ipc, "peak_ipc": 4.0, "frac": round(ipc / 4.0, 3),
+                             "source": "profiles/render_traffic.json (committed ncu capture, small case)"}
         line = {
             "metric": "fwd+bwd ms/view", "value": round(value, 4), "unit": "ms/view", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
@@ -258,7 +264,7 @@ def main():
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": dom["bytes_per_launch"],
-                         "ms_per_launch": round(dom["ms_per_launch"], 4)},
+                         "ms_per_launch": round(dom["ms_per_launch"], 4), "issue": issue},
             "kernels": kstats["table"],
             "clocks": clocks,
         }
