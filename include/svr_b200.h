@@ -246,7 +246,7 @@ int svr_batch_plan_tile_size(const svr_batch_plan* plan);
 /* Backward gradient reduction inside a warp: a staged record's 12 gradient
  * values from at most atomic_lanes (1-32, default 1) contributing lanes are
  * added to its shared accumulator with atomics, from more lanes through a
- * 13-shuffle reduce-scatter.  Only the order of additions changes. */
+ * 16-shuffle reduce-scatter.  Only the order of additions changes. */
 int svr_batch_plan_set_reduction(svr_batch_plan* plan, int atomic_lanes);
 int64_t svr_batch_plan_pixels(const svr_batch_plan* plan);
 int64_t svr_batch_plan_tiles(const svr_batch_plan* plan);

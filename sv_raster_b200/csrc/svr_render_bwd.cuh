@@ -46,7 +46,7 @@ __device__ __forceinline__ float warp_sum(float x) {
   return x;
 }
 
-// Reduce-scatter of 12 per-lane values over the warp in 13 shuffles (the
+// Reduce-scatter of 12 per-lane values over the warp in 16 shuffles (the
 // values are padded to 16 slots): after five halving steps lane l holds in
 // v[0] the warp total of slot (l >> 1) & 15; returns that slot for the even
 // lane that should publish it (-1 otherwise or for a padding slot).
