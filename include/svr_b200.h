@@ -240,7 +240,8 @@ int svr_batch_plan_set_schedule(svr_batch_plan* plan, int order_flags, int fwd_c
  * merged afterwards.  Defaults 512 / 4096; the order is the same for all. */
 int svr_batch_plan_set_sort_buckets(svr_batch_plan* plan, int small_n, int chunk);
 /* Records staged into shared memory per round by the compositing kernels:
- * 128, 256 (default) or 512 with 16x16 tiles, 64 with 8x8, 256 with 32x32. */
+ * 128, 256 (default) or 512 with 16x16 tiles, 32, 64 (default) or 128 with
+ * 8x8, 256 with 32x32. */
 int svr_batch_plan_set_staging(svr_batch_plan* plan, int records);
 int svr_batch_plan_tile_size(const svr_batch_plan* plan);
 /* Backward gradient reduction inside a warp: a staged record's 12 gradient

@@ -32,7 +32,7 @@ import os
 import torch
 
 DEFAULT_SPACE = {
-    "tile": [(16, 256), (8, 64), (32, 256), (16, 128), (16, 512)],
+    "tile": [(16, 256), (8, 64), (8, 32), (8, 128), (16, 128), (16, 512), (32, 256)],
     "sort": [(512, 4096), (256, 4096), (1024, 4096), (512, 2048)],
     "fwd": [(True, 0), (False, 0)],
     "bwd": [(True, 0), (False, 0)],

@@ -135,7 +135,9 @@ void ensure_bwd_batch_attributes() {
     set_bwd_batch_attrs<TileCfg<16, 128>>();
     set_bwd_batch_attrs<TileCfg<16, 256>>();
     set_bwd_batch_attrs<TileCfg<16, 512>>();
+    set_bwd_batch_attrs<TileCfg<8, 32>>();
     set_bwd_batch_attrs<TileCfg<8, 64>>();
+    set_bwd_batch_attrs<TileCfg<8, 128>>();
     set_bwd_batch_attrs<TileCfg<32, 256>>();
   });
 }
@@ -161,7 +163,9 @@ void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* r
   ensure_bwd_batch_attributes();
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
   const BwdBatchArgs args{views, n_items, ranges, tile_last, vals, va, P, rgb_view_stride, in, out, order, counter};
-  if (tile == 8) launch_bwd_batch_cfg<TileCfg<8, 64>>(args, ns, ctas_per_sm, stream);
+  if (tile == 8 && stage == 32) launch_bwd_batch_cfg<TileCfg<8, 32>>(args, ns, ctas_per_sm, stream);
+  else if (tile == 8 && stage == 128) launch_bwd_batch_cfg<TileCfg<8, 128>>(args, ns, ctas_per_sm, stream);
+  else if (tile == 8) launch_bwd_batch_cfg<TileCfg<8, 64>>(args, ns, ctas_per_sm, stream);
   else if (tile == 32) launch_bwd_batch_cfg<TileCfg<32, 256>>(args, ns, ctas_per_sm, stream);
   else if (stage == 128) launch_bwd_batch_cfg<TileCfg<16, 128>>(args, ns, ctas_per_sm, stream);
   else if (stage == 512) launch_bwd_batch_cfg<TileCfg<16, 512>>(args, ns, ctas_per_sm, stream);

@@ -141,8 +141,8 @@ void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t
 
 // Batched tile configurations: (tile size, staging depth).
 bool batch_tile_supported(int tile, int stage) {
-  return (tile == 16 && (stage == 128 || stage == 256 || stage == 512)) || (tile == 8 && stage == 64) ||
-         (tile == 32 && stage == 256);
+  return (tile == 16 && (stage == 128 || stage == 256 || stage == 512)) ||
+         (tile == 8 && (stage == 32 || stage == 64 || stage == 128)) || (tile == 32 && stage == 256);
 }
 
 template <class CFG, int NS>
@@ -166,7 +166,9 @@ void ensure_fwd_batch_attributes() {
     set_fwd_batch_attrs<TileCfg<16, 128>>();
     set_fwd_batch_attrs<TileCfg<16, 256>>();
     set_fwd_batch_attrs<TileCfg<16, 512>>();
+    set_fwd_batch_attrs<TileCfg<8, 32>>();
     set_fwd_batch_attrs<TileCfg<8, 64>>();
+    set_fwd_batch_attrs<TileCfg<8, 128>>();
     set_fwd_batch_attrs<TileCfg<32, 256>>();
   });
 }
@@ -191,7 +193,9 @@ void launch_render_fwd_batch(const ViewTable& views, int n_items, const uint2* r
   ensure_fwd_batch_attributes();
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
   const FwdBatchArgs args{views, n_items, ranges, vals, va, P, rgb_view_stride, out, order, counter};
-  if (tile == 8) launch_fwd_batch_cfg<TileCfg<8, 64>>(args, ns, ctas_per_sm, stream);
+  if (tile == 8 && stage == 32) launch_fwd_batch_cfg<TileCfg<8, 32>>(args, ns, ctas_per_sm, stream);
+  else if (tile == 8 && stage == 128) launch_fwd_batch_cfg<TileCfg<8, 128>>(args, ns, ctas_per_sm, stream);
+  else if (tile == 8) launch_fwd_batch_cfg<TileCfg<8, 64>>(args, ns, ctas_per_sm, stream);
   else if (tile == 32) launch_fwd_batch_cfg<TileCfg<32, 256>>(args, ns, ctas_per_sm, stream);
   else if (stage == 128) launch_fwd_batch_cfg<TileCfg<16, 128>>(args, ns, ctas_per_sm, stream);
   else if (stage == 512) launch_fwd_batch_cfg<TileCfg<16, 512>>(args, ns, ctas_per_sm, stream);

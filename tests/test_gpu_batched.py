@@ -267,6 +267,8 @@ def _render_and_grads(r, C, wC, wT):
 
 @pytest.mark.parametrize("tile,stage,order,ctas,buckets,lanes", [
     (8, 64, (True, True), (0, 0), (512, 4096), 4),
+    (8, 32, (True, False), (0, 0), (256, 4096), 1),
+    (8, 128, (False, True), (0, 0), (1024, 2048), 2),
     (32, 256, (True, True), (0, 0), (512, 4096), 1),
     (16, 128, (True, True), (0, 0), (256, 2048), 8),
     (16, 512, (False, False), (0, 0), (1024, 4096), 2),
