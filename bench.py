@@ -160,7 +160,10 @@ def main():
     from sv_raster_b200 import workload
     sc = scene_for(args, rank, world)
     if args.train:
-        return run_train(args, sc, dev, world, rank)
+        rc = run_train(args, sc, dev, world, rank)
+        if world > 1:
+            dist.destroy_process_group()
+        return rc
     if args.mode == "plain":
         wl = workload.PlainWorkload(sc, dev)
     else:
@@ -287,20 +290,24 @@ def run_train(args, sc, dev, world, rank):
     torch.cuda.set_device(dev)
     torch.zeros(1, device=dev)
     torch.cuda.reset_peak_memory_stats()
-    wl = workload.BatchedTrainWorkload(sc, dev)
+    exchange = workload.GradientExchange() if world > 1 else None
+    wl = workload.BatchedTrainWorkload(sc, dev, exchange=exchange)
     wl.capture()
     peak_setup = torch.cuda.max_memory_allocated()  # includes the autotuner's trial plans
     torch.cuda.reset_peak_memory_stats()
     ms_b, loss_b = wl.run(args.steps)
+    ms_b = workload.max_over_ranks(ms_b, device=dev)
     peak_b = torch.cuda.max_memory_allocated()
     del wl
     torch.cuda.empty_cache()
-    torch.cuda.reset_peak_memory_stats()
-    wp = workload.PlainTrainWorkload(sc, dev)
-    ms_p, loss_p = wp.run(args.plain_steps)
-    peak_p = torch.cuda.max_memory_allocated()
-    n = min(len(loss_b), len(loss_p))
-    dev_rel = max(abs(a - b) / abs(b) for a, b in zip(loss_b[:n], loss_p[:n]))
+    ms_p = loss_p = peak_p = dev_rel = None
+    if world == 1:  # the plain per-view form is the single-GPU comparator
+        torch.cuda.reset_peak_memory_stats()
+        wp = workload.PlainTrainWorkload(sc, dev)
+        ms_p, loss_p = wp.run(args.plain_steps)
+        peak_p = torch.cuda.max_memory_allocated()
+        n = min(len(loss_b), len(loss_p))
+        dev_rel = max(abs(a - b) / abs(b) for a, b in zip(loss_b[:n], loss_p[:n]))
     if rank == 0:
         print(json.dumps({
             "metric": "training ms/step", "value": round(ms_b, 3), "unit": "ms/step", "higher_is_better": False,
@@ -308,14 +315,16 @@ def run_train(args, sc, dev, world, rank):
             "config": {"workload": f"{args.config}: {sc.n_voxels} voxels, {len(sc.cameras)} views per step "
                                    f"({sc.cameras[0].width}x{sc.cameras[0].height} ... mixed), fwd + recompute bwd "
                                    f"+ fused Adam, one CUDA graph per step"},
-            "plain_fp32": {"ms_per_step": round(ms_p, 3), "steps": args.plain_steps,
-                           "peak_hbm_gb": round(peak_p / 1e9, 2)},
-            "speedup_vs_plain": round(ms_p / ms_b, 3),
+            "scaling": "weak",
+            "exchange": "sum all-reduce of the flat gradient buffer per step (NCCL)" if world > 1 else None,
+            "plain_fp32": None if ms_p is None else {"ms_per_step": round(ms_p, 3), "steps": args.plain_steps,
+                                                     "peak_hbm_gb": round(peak_p / 1e9, 2)},
+            "speedup_vs_plain": None if ms_p is None else round(ms_p / ms_b, 3),
             "peak_hbm_gb": round(peak_b / 1e9, 2),
             "peak_hbm_gb_incl_setup": round(peak_setup / 1e9, 2),
             "loss_batched_bf16": [round(x, 6) for x in loss_b],
-            "loss_plain_fp32": [round(x, 6) for x in loss_p],
-            "loss_max_rel_dev_common_steps": round(dev_rel, 6)}), flush=True)
+            "loss_plain_fp32": None if loss_p is None else [round(x, 6) for x in loss_p],
+            "loss_max_rel_dev_common_steps": None if dev_rel is None else round(dev_rel, 6)}), flush=True)
     return 0
 
 

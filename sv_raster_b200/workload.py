@@ -480,14 +480,41 @@ class DeviceAdam:
             ctypes.c_void_p(torch.cuda.current_stream(self.params[0].device).cuda_stream)), "fused_adam_step_device")
 
 
+class GradientExchange:
+    """View-parallel training across ranks: every rank renders its own views
+    of the replicated scene, then one sum all-reduce of its flat gradient
+    buffer makes every rank's gradient the gradient of the mean loss over all
+    ranks' views, so the identical Adam update keeps the parameters
+    replicated.  The loss is averaged the same way (for reporting)."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.group = group
+        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+
+    def __call__(self, flat_grad, loss=None):
+        if self.world == 1:
+            return
+        self.dist.all_reduce(flat_grad, group=self.group)
+        flat_grad.mul_(1.0 / self.world)
+        if loss is not None:
+            self.dist.all_reduce(loss, group=self.group)
+            loss.mul_(1.0 / self.world)
+
+
 class BatchedTrainWorkload:
     """One training step over all views: batched projection + SH, binning,
     compositing, L2 loss, recompute backward, multi-view SH backward and a
     fused Adam update of densities and SH (bf16 storage, fp32 moments);
-    capturable as one CUDA graph (the step count lives on the device)."""
+    capturable as one CUDA graph (the step count lives on the device).
+
+    With ``exchange`` (a GradientExchange over several ranks) each rank
+    renders its own views and the step becomes: graph (forward + backward) ->
+    all-reduce of the flat gradient buffer -> graph (Adam)."""
 
     def __init__(self, scene, dev, storage=torch.bfloat16, lr_geo=0.025, lr_sh=0.01, betas=(0.1, 0.99),
-                 eps=1e-15, tune=True):
+                 eps=1e-15, tune=True, exchange=None):
         from .batched import BatchedRasterizer
         self.sc, self.dev, self.P = scene, dev, scene.n_voxels
         self.octpath = _t(scene.octpath.reshape(-1, 1), dev, torch.int64)
@@ -514,12 +541,17 @@ class BatchedTrainWorkload:
         self.dT = torch.zeros(r.n_pixels, device=dev)
         self.dC = torch.zeros_like(self.color)
         self.loss = torch.zeros((), device=dev)
-        self.grads = (torch.zeros(self.P, 8, device=dev), torch.zeros(self.P, device=dev),
-                      torch.zeros(self.P, 3, device=dev), torch.zeros(self.P, 15, 3, device=dev))
+        # one flat buffer for the exchanged gradients: densities, sh0, shs (then subdiv, not exchanged)
+        P = self.P
+        self.flat_grad = torch.zeros(P * (8 + 3 + 45), device=dev)
+        self.grads = (self.flat_grad[:8 * P].view(P, 8), torch.zeros(P, device=dev),
+                      self.flat_grad[8 * P:11 * P].view(P, 3), self.flat_grad[11 * P:].view(P, 15, 3))
         self.adam = DeviceAdam([self.geos, self.sh0, self.shs], [lr_geo, lr_sh, lr_sh], betas, eps)
+        self.exchange = exchange if (exchange is not None and exchange.world > 1) else None
         self.graph = None
+        self.graph_adam = None
 
-    def _step(self):
+    def _forward_backward(self):
         r = self.raster
         r.prepare(self.sh0, self.shs, 3)
         r.render(self.geos, self.color, self.T)
@@ -527,7 +559,13 @@ class BatchedTrainWorkload:
         torch.mul(self.scale, diff, out=self.dC)
         self.loss.copy_((self.dC * diff).sum() * 0.5)  # mean over views of MSE (scale = 2 / (N_v V))
         r.backward(self.geos, self.T, self.dC, self.dT, 3, 16, grads=self.grads)
+
+    def _adam(self):
         self.adam.step([self.grads[0], self.grads[2], self.grads[3]])
+
+    def _step(self):
+        self._forward_backward()
+        self._adam()
 
     def capture(self):
         s = torch.cuda.Stream(self.dev)
@@ -535,10 +573,27 @@ class BatchedTrainWorkload:
         with torch.cuda.stream(s):  # warm-up launches (sets kernel attributes, allocator pools)
             self._eager_probe()
         torch.cuda.current_stream(self.dev).wait_stream(s)
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            self._step()
-        self.graph = g
+        if self.exchange is None:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._step()
+            self.graph = g
+        else:
+            # the collective stays outside the graphs: forward + backward, then Adam
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._forward_backward()
+            ga = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(ga):
+                self._adam()
+            self.graph, self.graph_adam = g, ga
+
+    def replay(self):
+        """One training step from the captured graph(s)."""
+        self.graph.replay()
+        if self.exchange is not None:
+            self.exchange(self.flat_grad, self.loss)
+            self.graph_adam.replay()
 
     def _eager_probe(self):
         # one forward/backward without the optimizer update, so parameters are untouched
@@ -557,7 +612,7 @@ class BatchedTrainWorkload:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         for i in range(steps):
-            self.graph.replay()
+            self.replay()
             losses[i].copy_(self.loss)
         e1.record(st)
         torch.cuda.synchronize()
