@@ -301,6 +301,7 @@ int svr_rasterize_render(const svr_camera* cam, int n_samp, int need_depth, int 
   VoxelArrays va{c.g.bbox, vox_centers, vox_lengths, geos, nullptr, rgbs};
   FwdTileOut out{c.im.tile_last, c.im.n_contrib, out_color, out_depth, out_normal, out_T, max_w};
   const uint32_t n_tiles = (uint32_t)(c.vt.v[0].grid_x * c.vt.v[0].grid_y);
+  cudaMemsetAsync(c.im.tile_last, 0, n_tiles * sizeof(uint32_t), stream);  // combined by atomicMax
   launch_tile_order(c.im.ranges, nullptr, n_tiles, c.im.okey, c.im.oval, c.im.order, c.im.ocount, c.im.otemp,
                     stream);
   launch_render_fwd(c.vt.v[0], c.im.ranges, c.n > 0 ? c.bl.vals_b : nullptr, va, out, n_samp, need_depth != 0,

@@ -33,7 +33,10 @@ struct TileCfg {
   static_assert(TS == 8 || TS == 16 || TS == 32, "tile size");
   static_assert(SB % 32 == 0 && SB >= 32, "staging depth");
 };
-using PlainTile = TileCfg<16, 256>;  // the reference's 16x16 tiles (config.h:14-15)
+// The plain path keeps the reference's 16x16 tile lists (config.h:14-15)
+// and composites each with four 8x8 CTAs that share the list.
+using PlainTile = TileCfg<8, 64>;
+constexpr int kPlainSub = 4;  // 8x8 CTAs per 16x16 list
 
 // Resident CTAs per SM the compositing kernels are register-bounded for at
 // 256 threads (occupancy vs spills, chosen from -Xptxas -v and ncu

@@ -27,15 +27,17 @@ struct BwdSmem {
   uint32_t item;
 };
 
+// CTA b back-propagates quadrant b % 4 of the 16x16 list order[b / 4].
 template <int NS, bool DEPTH, bool DIST, bool NORMAL>
-__global__ void __launch_bounds__(PlainTile::NT, kBwdMinBlocks)
+__global__ void __launch_bounds__(PlainTile::NT, bwd_min_blocks<PlainTile>())
 render_bwd_kernel(const __grid_constant__ BwdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BwdSmem<PlainTile>& sm = *reinterpret_cast<BwdSmem<PlainTile>*>(smem_raw);
   if (threadIdx.x < 12) sm.c2w[threadIdx.x] = a.vp.c2w[threadIdx.x];
   __syncthreads();
-  const int tile = a.order ? (int)a.order[blockIdx.x] : (int)blockIdx.x;
-  const int tile_x = tile % a.vp.grid_x, tile_y = tile / a.vp.grid_x;
+  const int b = blockIdx.x / kPlainSub, sub = blockIdx.x % kPlainSub;
+  const int tile = a.order ? (int)a.order[b] : b;
+  const int tile_x = (tile % a.vp.grid_x) * 2 + (sub & 1), tile_y = (tile / a.vp.grid_x) * 2 + (sub >> 1);
   render_tile_bwd<PlainTile, NS, DEPTH, DIST, NORMAL>(a.vp, sm.c2w, tile_x, tile_y, a.ranges[tile], a.tile_last[tile],
                                                       a.vals, a.va, a.in, a.out, sm.s, sm.grad);
 }
@@ -110,7 +112,7 @@ void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t
                        const VoxelArrays& va, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
                        bool dist, bool normal, const uint32_t* order, cudaStream_t stream) {
   BwdArgs args{vp, ranges, tile_last, vals, va, in, out, order};
-  const dim3 grid(vp.grid_x * vp.grid_y);
+  const dim3 grid(vp.grid_x * vp.grid_y * kPlainSub);
   SVR_BWD_SWITCH(render_bwd_kernel)
 }
 

@@ -30,19 +30,22 @@ struct FwdArgs {
   const uint32_t* order;  // CTA i renders tile order[i] (identity when null)
 };
 
+// CTA b composites quadrant b % 4 of the 16x16 list order[b / 4] (the
+// caller zeroes tile_last; the four quadrants combine it with atomicMax).
 template <int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
-__global__ void __launch_bounds__(PlainTile::NT, kFwdMinBlocks)
+__global__ void __launch_bounds__(PlainTile::NT, fwd_min_blocks<PlainTile>())
 render_fwd_kernel(const __grid_constant__ FwdArgs a) {
   __shared__ StageSmem<PlainTile::SB> s;
   __shared__ float s_c2w[12];
   __shared__ uint32_t s_red[PlainTile::NW];
   if (threadIdx.x < 12) s_c2w[threadIdx.x] = a.vp.c2w[threadIdx.x];
   __syncthreads();
-  const int tile = a.order ? (int)a.order[blockIdx.x] : (int)blockIdx.x;
-  const int tile_x = tile % a.vp.grid_x, tile_y = tile / a.vp.grid_x;
+  const int b = blockIdx.x / kPlainSub, sub = blockIdx.x % kPlainSub;
+  const int tile = a.order ? (int)a.order[b] : b;
+  const int tile_x = (tile % a.vp.grid_x) * 2 + (sub & 1), tile_y = (tile / a.vp.grid_x) * 2 + (sub >> 1);
   const uint2 range = a.ranges[tile];
-  render_tile_fwd<PlainTile, NS, DEPTH, DIST, NORMAL, MAXW>(a.vp, s_c2w, tile_x, tile_y, range, a.vals, a.va, a.out,
-                                                            s, s_red);
+  render_tile_fwd<PlainTile, NS, DEPTH, DIST, NORMAL, MAXW, true>(a.vp, s_c2w, tile_x, tile_y, range, a.vals, a.va,
+                                                                  a.out, a.out.tile_last + tile, s, s_red);
 }
 
 // Multi-view form: a persistent grid over the (view, tile) work items of all
@@ -98,7 +101,7 @@ render_fwd_batch_kernel(const __grid_constant__ FwdBatchArgs a) {
     o.color = a.out.color + 3 * (size_t)vp.pix_base;
     o.T = a.out.T + vp.pix_base;
     render_tile_fwd<CFG, NS, false, false, false, false>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.vals, va, o,
-                                                         sm.s, sm.red);
+                                                         o.tile_last + local, sm.s, sm.red);
     __syncthreads();  // shared state (item, camera, staging) is free for the next tile
   }
 }
@@ -135,7 +138,7 @@ void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t
                        const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
                        const uint32_t* order, cudaStream_t stream) {
   FwdArgs args{vp, ranges, vals, va, out, order};
-  const dim3 grid(vp.grid_x * vp.grid_y);
+  const dim3 grid(vp.grid_x * vp.grid_y * kPlainSub);
   SVR_FWD_DISPATCH(render_fwd_kernel, grid, stream, args);
 }
 

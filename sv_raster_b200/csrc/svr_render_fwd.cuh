@@ -16,7 +16,7 @@
 namespace svr {
 
 struct FwdTileOut {
-  uint32_t* tile_last;   // [T] of this view
+  uint32_t* tile_last;   // [T] of this view (indexed by the callers)
   uint32_t* n_contrib;   // [H*W] of this view
   float* color;          // [3,H,W]
   float* depth;          // [3,H,W] or nullptr
@@ -25,15 +25,19 @@ struct FwdTileOut {
   float* max_w;          // [P] or nullptr
 };
 
-template <class CFG, int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW>
+// (tile_x, tile_y) index CFG::TS-sized tiles; `range` is the list the tile
+// walks (its own, or the list of an enclosing tile it shares with others);
+// `last_slot` receives range.x + the tile's largest contributor count, with
+// atomicMax when SHARED_LAST (several CTAs share one list and slot, which
+// then starts at 0).
+template <class CFG, int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW, bool SHARED_LAST = false>
 __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const float* __restrict__ c2w_s, int tile_x,
                                                 int tile_y, uint2 range, const uint32_t* __restrict__ vals,
-                                                const VoxelArrays& va, const FwdTileOut& out,
+                                                const VoxelArrays& va, const FwdTileOut& out, uint32_t* last_slot,
                                                 StageSmem<CFG::SB>& s, uint32_t* s_red /*[CFG::NW]*/) {
   constexpr int SB = CFG::SB;
   const int W = vp.W, H = vp.H;
   const int tid = threadIdx.x;
-  const int tile_id = tile_y * vp.grid_x + tile_x;
   int lx, ly;
   tile_pixel_of<CFG>(tid, lx, ly);
   const uint32_t px = tile_x * CFG::TS + lx, py = tile_y * CFG::TS + ly;
@@ -214,7 +218,8 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
     uint32_t m = 0;
 #pragma unroll
     for (int w = 0; w < CFG::NW; ++w) m = max(m, s_red[w]);
-    out.tile_last[tile_id] = range.x + m;
+    if (SHARED_LAST) atomicMax(last_slot, range.x + m);
+    else *last_slot = range.x + m;
   }
 }
 
