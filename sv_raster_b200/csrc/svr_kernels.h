@@ -57,8 +57,10 @@ void launch_tile_ranges(const uint64_t* keys, const uint32_t* d_start, const uin
                         int rank_bits, uint32_t tile_base, uint32_t n_tiles, uint2* ranges, cudaStream_t stream);
 
 // svr_render_fwd.cu / svr_render_bwd.cu
-// Plain one-view launches: one CTA per 16x16 tile; CTA i renders tile
-// order[i] (largest tiles first) or tile i when order is null.
+// Plain one-view launches over the reference's 16x16 tile lists: four 8x8
+// CTAs per list; CTA i renders quadrant i % 4 of list order[i / 4] (largest
+// tiles first) or of list i / 4 when order is null.  The forward combines
+// tile_last with atomicMax (the caller zeroes it).
 void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t* vals, const VoxelArrays& va,
                        const FwdTileOut& out, int ns, bool depth, bool dist, bool normal, bool maxw,
                        const uint32_t* order, cudaStream_t stream);

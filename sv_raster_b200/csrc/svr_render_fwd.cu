@@ -1,5 +1,5 @@
 // Forward compositing kernels and their template dispatch: the plain
-// one-view grid (one CTA per 16x16 tile, the reference's layout) and the
+// one-view grid (the reference's 16x16 tile lists, four 8x8 CTAs each) and the
 // multi-view form (one persistent launch over every (view, tile) of all
 // views, tile size and staging depth chosen per plan).
 #include <mutex>
