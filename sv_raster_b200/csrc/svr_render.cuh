@@ -39,9 +39,11 @@ using PlainTile = TileCfg<8, 64>;
 constexpr int kPlainSub = 4;  // 8x8 CTAs per 16x16 list
 
 // Resident CTAs per SM the compositing kernels are register-bounded for at
-// 256 threads (occupancy vs spills, chosen from -Xptxas -v and ncu
-// measurements); other CTA sizes keep the same threads per SM.
-constexpr int kFwdMinBlocks = 5;
+// 256 threads (64 registers each); other CTA sizes keep the same threads per
+// SM.  Chosen by measurement on the c4 step at 8x8 tiles: forward at 3 / 4 /
+// 5 / 6 gave 15.0 / 13.9 / 14.4 / 14.9 ms, backward at 3 / 4 / 5 gave
+// 31.2 / 29.0 / 41.6 ms.
+constexpr int kFwdMinBlocks = 4;
 constexpr int kBwdMinBlocks = 4;
 template <class CFG>
 constexpr int fwd_min_blocks() { return CFG::NT >= 1024 ? 1 : kFwdMinBlocks * 256 / CFG::NT; }
