@@ -168,7 +168,7 @@ class PlainWorkload:
         n = 0
         for cam, _, _ in self.cams:
             T_ = math.ceil(cam.width / 16) * math.ceil(cam.height / 16)
-            passes = math.ceil(int(T_).bit_length() / 8)  # radix passes over the tile bits only
+            passes = math.ceil(int(T_).bit_length() / 10)  # radix passes over the tile bits (8-10 bit digits)
             # preprocess 1 + scan 3 + duplicate 1 + sort 3/pass + ranges 1 + segment sort 4 + fwd 1 + bwd 1 + sh 2
             n += 1 + 3 + 1 + 3 * passes + 1 + 4 + 1 + 1 + 2
         return n
@@ -379,7 +379,7 @@ class BatchedWorkload:
 
     def launches_per_step(self):
         T_ = max(self.raster.n_tiles, 1)
-        passes = math.ceil(int(T_).bit_length() / 8)  # radix passes over the tile bits only
+        passes = math.ceil(int(T_).bit_length() / 10)  # radix passes over the tile bits (8-10 bit digits)
         g = self.raster.n_groups
         order = self.raster.schedule[0]
         # project 1 + scan 3 + segments 1 + duplicate 1 + (sort 3/pass + ranges 1) per group
