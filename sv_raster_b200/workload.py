@@ -169,8 +169,9 @@ class PlainWorkload:
         for cam, _, _ in self.cams:
             T_ = math.ceil(cam.width / 16) * math.ceil(cam.height / 16)
             passes = math.ceil(int(T_).bit_length() / 10)  # radix passes over the tile bits (8-10 bit digits)
-            # preprocess 1 + scan 3 + duplicate 1 + sort 3/pass + ranges 1 + segment sort 4 + fwd 1 + bwd 1 + sh 2
-            n += 1 + 3 + 1 + 3 * passes + 1 + 4 + 1 + 1 + 2
+            # preprocess 1 + scan 3 + duplicate 1 + sort 3/pass + ranges 1 + segment sort 4
+            # + tile order (key kernel + one 3-kernel sort pass) 4 + fwd 1 + bwd 1 + sh 2
+            n += 1 + 3 + 1 + 3 * passes + 1 + 4 + 4 + 1 + 1 + 2
         return n
 
     def kernel_stats(self):
