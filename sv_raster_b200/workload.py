@@ -425,14 +425,24 @@ class BatchedWorkload:
                 tgt[k % 2].copy_(host_t, non_blocking=True)
                 ready[k % 2].record(copy)
 
+        # mean over views of each view's MSE: with equal view sizes one weight
+        # for every pixel, so the fused sum-of-squares loss applies
+        uniform = len({h * w for h, w in self.raster.sizes}) == 1
+        w0 = float(self.scale[0]) * 0.5
+
         def one_step(k):
             upload(k + 1)  # prefetch the next step's inputs behind this step's compute
             main.wait_event(ready[k % 2])
             for c, a, b in zip(self.cams, host_w2c, host_c2w):
                 c.w2c.copy_(a, non_blocking=True)
                 c.c2w.copy_(b, non_blocking=True)
+            for t in (geos, sh0, shs):
+                t.grad = None  # as an optimizer's zero_grad(set_to_none=True) would
             color, T = BatchedRender.apply(self.raster, 3, geos, sh0, shs)
-            loss = (self.scale * 0.5 * (color - tgt[k % 2]) ** 2).sum()
+            if uniform:
+                loss = torch.nn.functional.mse_loss(color, tgt[k % 2], reduction="sum") * w0
+            else:
+                loss = (self.scale * 0.5 * (color - tgt[k % 2]) ** 2).sum()
             free[k % 2].record(main)
             loss.backward()
             return float(loss.detach().cpu())
