@@ -263,50 +263,83 @@ void launch_adam_fused(const AdamGroupTable& t, int num_sms, cudaStream_t stream
 // ---------------------------------------------------------------------------
 // Grid-point gathers
 // ---------------------------------------------------------------------------
-template <int DIM>
-__global__ void __launch_bounds__(256)
-gather_kernel(int n_care, const int64_t* __restrict__ vox_key, const int64_t* __restrict__ care_idx,
+// One slot per (cared voxel, corner): the 8 slots of a voxel read its 8 keys
+// and write its 8 outputs as one contiguous run, so key reads and output
+// stores are coalesced across the warp; only the grid-point reads (and the
+// backward's adds) are scattered.  Each thread carries U slots, 256 apart,
+// through every load stage together so U scattered reads are in flight.
+constexpr int kGatherThreads = 256;
+
+template <int DIM, int U>
+__global__ void __launch_bounds__(kGatherThreads)
+gather_kernel(int64_t n_slots, const int64_t* __restrict__ vox_key, const int64_t* __restrict__ care_idx,
               const float* __restrict__ grid_pts, float* __restrict__ out) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n_care) return;
-  const int64_t i = care_idx[t];
+  const int64_t base = (int64_t)blockIdx.x * (kGatherThreads * U) + threadIdx.x;
+  int64_t slot[U], k[U];
+  float v[U][DIM];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int64_t k = vox_key[8 * i + c];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) out[(8 * i + c) * DIM + d] = grid_pts[k * DIM + d];
+  for (int j = 0; j < U; ++j) {
+    const int64_t t = base + j * kGatherThreads;
+    slot[j] = t < n_slots ? 8 * care_idx[t >> 3] + (t & 7) : -1;
   }
+#pragma unroll
+  for (int j = 0; j < U; ++j) k[j] = slot[j] >= 0 ? vox_key[slot[j]] : 0;
+#pragma unroll
+  for (int j = 0; j < U; ++j)
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[j][d] = slot[j] >= 0 ? grid_pts[k[j] * DIM + d] : 0.f;
+#pragma unroll
+  for (int j = 0; j < U; ++j)
+    if (slot[j] >= 0)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) out[slot[j] * DIM + d] = v[j][d];
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(256)
-gather_bw_kernel(int n_care, const int64_t* __restrict__ vox_key, const int64_t* __restrict__ care_idx,
+template <int DIM, int U>
+__global__ void __launch_bounds__(kGatherThreads)
+gather_bw_kernel(int64_t n_slots, const int64_t* __restrict__ vox_key, const int64_t* __restrict__ care_idx,
                  const float* __restrict__ dL_dvox, float* __restrict__ dL_dgrid) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n_care) return;
-  const int64_t i = care_idx[t];
+  const int64_t base = (int64_t)blockIdx.x * (kGatherThreads * U) + threadIdx.x;
+  int64_t slot[U], k[U];
+  float g[U][DIM];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int64_t k = vox_key[8 * i + c];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) atomicAdd(dL_dgrid + k * DIM + d, dL_dvox[(8 * i + c) * DIM + d]);
+  for (int j = 0; j < U; ++j) {
+    const int64_t t = base + j * kGatherThreads;
+    slot[j] = t < n_slots ? 8 * care_idx[t >> 3] + (t & 7) : -1;
   }
+#pragma unroll
+  for (int j = 0; j < U; ++j) {
+    k[j] = slot[j] >= 0 ? vox_key[slot[j]] : 0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) g[j][d] = slot[j] >= 0 ? dL_dvox[slot[j] * DIM + d] : 0.f;
+  }
+#pragma unroll
+  for (int j = 0; j < U; ++j)
+    if (slot[j] >= 0)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) atomicAdd(dL_dgrid + k[j] * DIM + d, g[j][d]);
+}
+
+template <int DIM, int U, class KERNEL>
+static void launch_slots(KERNEL kernel, int n_care, const int64_t* vox_key, const int64_t* care_idx, const float* in,
+                         float* out, cudaStream_t stream) {
+  const int64_t n_slots = 8 * (int64_t)n_care;
+  const unsigned g = (unsigned)((n_slots + kGatherThreads * U - 1) / (kGatherThreads * U));
+  kernel<<<g, kGatherThreads, 0, stream>>>(n_slots, vox_key, care_idx, in, out);
 }
 
 void launch_gather(int dim, int n_care, const int64_t* vox_key, const int64_t* care_idx, const float* grid_pts,
                    float* out, cudaStream_t stream) {
   if (n_care <= 0) return;
-  const int g = (n_care + 255) / 256;
-  if (dim == 1) gather_kernel<1><<<g, 256, 0, stream>>>(n_care, vox_key, care_idx, grid_pts, out);
-  else gather_kernel<3><<<g, 256, 0, stream>>>(n_care, vox_key, care_idx, grid_pts, out);
+  if (dim == 1) launch_slots<1, 4>(gather_kernel<1, 4>, n_care, vox_key, care_idx, grid_pts, out, stream);
+  else launch_slots<3, 2>(gather_kernel<3, 2>, n_care, vox_key, care_idx, grid_pts, out, stream);
 }
 
 void launch_gather_bw(int dim, int n_care, const int64_t* vox_key, const int64_t* care_idx, const float* dL_dvox,
                       float* dL_dgrid, cudaStream_t stream) {
   if (n_care <= 0) return;
-  const int g = (n_care + 255) / 256;
-  if (dim == 1) gather_bw_kernel<1><<<g, 256, 0, stream>>>(n_care, vox_key, care_idx, dL_dvox, dL_dgrid);
-  else gather_bw_kernel<3><<<g, 256, 0, stream>>>(n_care, vox_key, care_idx, dL_dvox, dL_dgrid);
+  if (dim == 1) launch_slots<1, 4>(gather_bw_kernel<1, 4>, n_care, vox_key, care_idx, dL_dvox, dL_dgrid, stream);
+  else launch_slots<3, 2>(gather_bw_kernel<3, 2>, n_care, vox_key, care_idx, dL_dvox, dL_dgrid, stream);
 }
 
 }  // namespace svr

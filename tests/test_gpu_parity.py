@@ -249,12 +249,14 @@ def test_total_variation_matches_reference_dense(ref, no_tv_s):
     assert rel_err(a, b) < 1e-6
 
 
-def test_total_variation_sparse_rule():
+@pytest.mark.parametrize("C", [1, 2, 3])
+def test_total_variation_sparse_rule(C):
     """Sparse mode touches only voxels with a non-zero corner gradient, judged on
-    the gradient as it was before the call (numpy statement of the rule)."""
+    the gradient as it was before the call (numpy statement of the rule), for
+    the one- and three-channel kernels and the generic channel count."""
     from sv_raster_b200 import grid_loss_bw
     rng = np.random.default_rng(12)
-    M, N, C = 3000, 800, 3
+    M, N = 3000, 800
     key = rng.integers(0, M, (N, 8))
     pts = rng.standard_normal((M, C)).astype(np.float32)
     grad0 = np.where(rng.uniform(size=(M, C)) < 0.2, rng.standard_normal((M, C)), 0).astype(np.float32)
