@@ -239,6 +239,11 @@ int svr_batch_plan_set_schedule(svr_batch_plan* plan, int order_flags, int fwd_c
  * small CTA each, longer ones in runs of `chunk` (2048 or 4096) instances
  * merged afterwards.  Defaults 512 / 4096; the order is the same for all. */
 int svr_batch_plan_set_sort_buckets(svr_batch_plan* plan, int small_n, int chunk);
+/* How svr_batch_prepare groups the instances by tile before the per-tile
+ * segment sort: 1 (default) a counting sort (per-tile counts, their scan,
+ * one scatter pass with one atomic per tile per warp), 0 LSD radix passes
+ * over the tile bits of the keys.  The sorted lists are the same for both. */
+int svr_batch_plan_set_binning(svr_batch_plan* plan, int binning);
 /* Records staged into shared memory per round by the compositing kernels:
  * 128, 256 (default) or 512 with 16x16 tiles, 32, 64 (default) or 128 with
  * 8x8, 256 with 32x32. */

@@ -9,6 +9,9 @@ gradients agree up to the order of floating-point additions):
   (``BatchedRasterizer.set_schedule``; its cap on resident CTAs per SM can be
   searched too by listing ``(ordered, cap)`` pairs, but full occupancy won on
   every scene measured, so the default space leaves it out).
+* ``bin`` -- how instances are grouped by tile before the per-tile sort:
+  counting sort with atomics (1) or radix passes over the tile bits (0)
+  (``BatchedRasterizer.set_binning``).
 * ``sort`` -- segment-size buckets of the per-tile segment sort: the largest
   segment sorted by one small CTA and the chunk length of the chunked sort
   (``BatchedRasterizer.set_sort_buckets``).
@@ -33,6 +36,7 @@ import torch
 
 DEFAULT_SPACE = {
     "tile": [(16, 256), (8, 64), (8, 32), (8, 128), (16, 128), (16, 512), (32, 256)],
+    "bin": [1, 0],
     "sort": [(512, 4096), (256, 4096), (1024, 4096), (512, 2048)],
     "fwd": [(True, 0), (False, 0)],
     "bwd": [(True, 0), (False, 0)],
@@ -94,6 +98,8 @@ def apply(raster, choice):
     if "tile" in choice:
         ts, sb = choice["tile"]
         raster.set_tile_size(int(ts), int(sb))
+    if "bin" in choice:
+        raster.set_binning(int(choice["bin"]))
     if "sort" in choice:
         raster.set_sort_buckets(*[int(x) for x in choice["sort"]])
     if "reduce" in choice:
@@ -110,7 +116,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
     Returns ``dict(choice=..., timings=..., cached=bool)`` and leaves the
     choice applied to ``raster``.  ``timer(fn, reps, warmup)`` times a stage
     (replaceable for tests).  Stages are tuned in order: tile size (full
-    step), sort buckets (prepare), forward schedule (render), backward
+    step), binning and sort buckets (prepare), forward schedule (render), backward
     schedule (backward), each with the previous choices applied.
     """
     space = dict(DEFAULT_SPACE if space is None else space)
@@ -125,8 +131,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
             return dict(choice=choice, timings=hit.get("timings", {}), cached=True)
 
     M = 1 + shs.shape[1]
-    choice = {"tile": DEFAULT_SPACE["tile"][0], "sort": DEFAULT_SPACE["sort"][0], "fwd": DEFAULT_SPACE["fwd"][0],
-              "bwd": DEFAULT_SPACE["bwd"][0], "reduce": DEFAULT_SPACE["reduce"][0]}
+    choice = {name: cands[0] for name, cands in DEFAULT_SPACE.items()}
     timings = {}
     gen = torch.Generator(device=raster.dev)
     gen.manual_seed(0)
@@ -154,7 +159,8 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
         dC, dT = upstream()
         state["grads"] = raster.backward(geos, state["out"][1], dC, dT, sh_degree, M, state.get("grads"))
 
-    stages = [("tile", step), ("sort", prepare), ("fwd", render), ("bwd", backward), ("reduce", backward)]
+    stages = [("tile", step), ("bin", prepare), ("sort", prepare), ("fwd", render), ("bwd", backward),
+              ("reduce", backward)]
     for name, fn in stages:
         cands = space.get(name)
         if not cands:

@@ -55,6 +55,7 @@ class BatchedRasterizer:
         self.schedule = (3, 0, 0)
         self.sort_buckets = (512, 4096)
         self.atomic_lanes = 1
+        self.binning = 1
         self._make_plan(0 if capacity is None else int(capacity))
         self.capacity_auto = capacity is None
 
@@ -78,6 +79,14 @@ class BatchedRasterizer:
         check(L.svr_batch_plan_set_sort_buckets(plan, *self.sort_buckets), "batch_plan_set_sort_buckets")
         check(L.svr_batch_plan_set_staging(plan, self.staging), "batch_plan_set_staging")
         check(L.svr_batch_plan_set_reduction(plan, self.atomic_lanes), "batch_plan_set_reduction")
+        check(L.svr_batch_plan_set_binning(plan, self.binning), "batch_plan_set_binning")
+
+    def set_binning(self, binning=1):
+        """How prepare groups the instances by tile before the per-tile sort:
+        1 a counting sort (counts, scan, atomic scatter), 0 radix passes over
+        the tile bits.  The sorted lists are the same."""
+        check(lib().svr_batch_plan_set_binning(self.plan, int(binning)), "batch_plan_set_binning")
+        self.binning = int(binning)
 
     def set_reduction(self, atomic_lanes=1):
         """Backward: records with at most ``atomic_lanes`` contributing lanes

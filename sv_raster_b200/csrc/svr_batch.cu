@@ -140,13 +140,27 @@ __device__ __forceinline__ int nth_set_bit(uint32_t m, int k) {
 // scan; the warp walks that run 32 instances at a time, each lane decoding
 // its instance (owning voxel, then quadrant / tile row / tile column in the
 // plain path's generation order: quadrants ascending, tiles row-major,
-// forward.cu:540-562) and writing key and value at its own slot.
+// forward.cu:540-562).  MODE selects what happens to the decoded instance:
+//   kDupWrite   key and value at its own slot (generation order, for the
+//               radix sort over the tile bits);
+//   kDupCount   +1 on its tile's instance count (counts[global tile]);
+//   kDupScatter key and value at the next free position of its tile's range
+//               (ranges[t].y is the tile's cursor, starting at ranges[t].x).
+// Count and scatter aggregate the lanes of a warp that hit the same tile
+// (match.any) into one atomic.  Both skip exactly the instances whose
+// generation slot is beyond the capacity, so every tile's cursor ends at the
+// end of its range.  Positions inside a tile follow the atomics' order; the
+// per-tile segment sort that follows orders them by their unique rank
+// positions, so the final lists do not depend on it.
+constexpr int kDupWrite = 0, kDupCount = 1, kDupScatter = 2;
+
+template <int MODE>
 __global__ void __launch_bounds__(256)
 duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const uint32_t* __restrict__ rank_pos,
                        const uint2* __restrict__ bboxes, const uint32_t* __restrict__ quads,
                        const uint32_t* __restrict__ ndup, const uint32_t* __restrict__ scan,
                        uint64_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t cap,
-                       uint32_t* __restrict__ err) {
+                       uint32_t* __restrict__ err, uint32_t* __restrict__ counts, uint2* __restrict__ ranges) {
   const int view = blockIdx.y;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
@@ -192,16 +206,50 @@ duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const uin
     const int s_tx0 = __shfl_sync(0xffffffffu, tx0, sl), s_ty0 = __shfl_sync(0xffffffffu, ty0, sl);
     const uint32_t s_qb = __shfl_sync(0xffffffffu, qb, sl);
     const uint32_t slot = run0 + p;
-    if (p < total && slot < cap) {
+    const bool active = p < total && slot < cap;
+    uint32_t q = 0, vid = 0, local = 0;
+    if (active) {
       const uint32_t qi = k / s_tiles, rem = k - qi * s_tiles;
       const uint32_t ty = (uint32_t)s_ty0 + rem / s_w, tx = (uint32_t)s_tx0 + rem % s_w;
-      const uint32_t q = (uint32_t)nth_set_bit(s_qb, (int)qi);
-      const uint32_t vid = (uint32_t)(blockIdx.x * blockDim.x + (threadIdx.x & ~31) + sl);
-      const uint64_t tile = (uint64_t)(vp.sort_tile_off + ty * (uint32_t)vp.grid_x + tx);
-      keys[slot] = (tile << kPosShift) | rank_pos[8 * (size_t)vid + q];
-      vals[slot] = make_sort_val(vid, q);
+      q = (uint32_t)nth_set_bit(s_qb, (int)qi);
+      vid = (uint32_t)(blockIdx.x * blockDim.x + (threadIdx.x & ~31) + sl);
+      local = ty * (uint32_t)vp.grid_x + tx;
+    }
+    if (MODE == kDupWrite) {
+      if (active) {
+        keys[slot] = ((uint64_t)(vp.sort_tile_off + local) << kPosShift) | rank_pos[8 * (size_t)vid + q];
+        vals[slot] = make_sort_val(vid, q);
+      }
+    } else {
+      // global tile of the instance; inactive lanes share a value no tile has
+      const uint32_t gtile = active ? vp.tile_base + local : 0xffffffffu;
+      const uint32_t peers = __match_any_sync(0xffffffffu, gtile);
+      const int leader = __ffs(peers) - 1;
+      if (MODE == kDupCount) {
+        if (active && lane == leader) atomicAdd(counts + gtile, (uint32_t)__popc(peers));
+      } else {
+        uint32_t base = 0;
+        if (active && lane == leader) base = atomicAdd(&ranges[gtile].y, (uint32_t)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (active) {
+          const uint32_t pos = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+          keys[pos] = ((uint64_t)(vp.sort_tile_off + local) << kPosShift) | rank_pos[8 * (size_t)vid + q];
+          vals[pos] = make_sort_val(vid, q);
+        }
+      }
     }
   }
+}
+
+// Binned ranges: from each tile's instance count and its inclusive scan,
+// ranges[t] = (start, start); the scatter pass advances .y to the end.  Empty
+// tiles get (0, 0), as the radix path leaves them.
+__global__ void bin_ranges_kernel(uint32_t n_tiles, const uint32_t* __restrict__ counts,
+                                  const uint32_t* __restrict__ incl, uint2* __restrict__ ranges) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_tiles) return;
+  const uint32_t n = counts[t], start = n ? incl[t] - n : 0u;
+  ranges[t] = make_uint2(start, start);
 }
 
 // Rank-position table, step 1: the (compressed) Morton rank of every
@@ -331,6 +379,7 @@ struct svr_batch_plan {
   int tile_size;               // compositing tile size (8, 16 or 32), fixed at creation
   int stage;                   // records staged per round (svr_batch_plan_set_staging)
   int atomic_lanes;            // backward reduction threshold (svr_batch_plan_set_reduction)
+  int binning;                 // 1: counting sort by tile, 0: radix over the tile bits (svr_batch_plan_set_binning)
   // workspace layout (byte offsets)
   size_t o_header, o_ndup, o_scan, o_bbox, o_quad, o_scan_tmp, o_rgbs, o_drgbs;
   size_t o_ka, o_kb, o_va, o_vb, o_sort_tmp, o_ranges, o_tile_last, o_ncontrib;
@@ -393,7 +442,8 @@ BatchPtrs ptrs(const svr_batch_plan* p, void* ws) {
 
 // Header words: [0] instance count, [1] error word, [2] forward work counter,
 // [3] backward work counter, [4] tile count read by the order sort, [5] pair
-// count read by the rank-position sort, [16..] group segments.
+// count read by the rank-position sort, [6] binned instance count (counting
+// sort by tile), [16..] group segments.
 constexpr int kHeaderWords = 16 + 2 * kMaxViews;
 
 // Longest-first work order of all tiles into `order` (see launch_tile_order).
@@ -508,7 +558,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->o_scan = take(VP * 4);
   p->o_bbox = take(VP * 8);
   p->o_quad = take(VP * 4);
-  p->o_scan_tmp = take(scan_temp_bytes(VP));
+  p->o_scan_tmp = take(scan_temp_bytes(std::max(VP, (size_t)tiles)));  // instance scan, then the tile-count scan
   p->o_rgbs = take(VP * 12);
   p->o_drgbs = take(VP * 12);
   // the instance arrays also serve the one-time sort of the 8P rank keys
@@ -534,6 +584,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->seg_small_n = 512;
   p->seg_chunk = 4096;
   p->atomic_lanes = 1;
+  p->binning = 1;
   ensure_segsort_attributes();
   ensure_fwd_batch_attributes();
   ensure_bwd_batch_attributes();
@@ -571,6 +622,12 @@ int svr_batch_plan_tile_size(const svr_batch_plan* p) { return p ? p->tile_size 
 int svr_batch_plan_set_reduction(svr_batch_plan* p, int atomic_lanes) {
   if (!p || atomic_lanes < 1 || atomic_lanes > 32) return SVR_ERR_SHAPE;
   p->atomic_lanes = atomic_lanes;
+  return SVR_OK;
+}
+
+int svr_batch_plan_set_binning(svr_batch_plan* p, int binning) {
+  if (!p || (binning != 0 && binning != 1)) return SVR_ERR_SHAPE;
+  p->binning = binning;
   return SVR_OK;
 }
 
@@ -645,7 +702,7 @@ int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, 
   launch_scan_inclusive(q.ndup, q.scan, VP, q.scan_tmp, q.header, (unsigned long long)p->cap, q.header + 1, stream);
   uint32_t* segs = q.header + 16;
   group_segments_kernel<<<1, 64, 0, stream>>>(p->gt, P, q.scan, (uint32_t)p->cap, segs);
-  cudaMemsetAsync(q.ranges, 0, (size_t)p->total_tiles * sizeof(uint2), stream);
+  if (!p->binning) cudaMemsetAsync(q.ranges, 0, (size_t)p->total_tiles * sizeof(uint2), stream);
   if (!p->pos_ready || p->pos_paths != octree_paths) {
     // Rank positions of all (voxel, quadrant) pairs: one stable radix sort of
     // the 8P compressed ranks in the (still free) instance arrays.
@@ -660,23 +717,42 @@ int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, 
   }
   if (p->cap > 0) {
     // Two-level sort: LSD radix passes over the tile bits only put every
-    // tile's instances together in generation order (ending in ka/va), then
-    // one CTA per tile sorts its segment by the rank-position bits into
-    // kb/vb.  The result is the order of one stable sort by the full key.
+    // tile's instances together in generation order (ending in ka/va) -- or,
+    // with binning on, a counting sort by tile puts them together in no
+    // particular order -- then one CTA per tile sorts its segment by the
+    // rank-position bits into kb/vb.  Rank positions are unique inside a
+    // tile, so either way the result is the order of one stable sort by the
+    // full key.
     const bool odd = (sort_passes(p->key_bits - kPosShift) & 1) != 0;
     uint64_t* k0 = odd ? q.kb : q.ka;
     uint32_t* v0 = odd ? q.vb : q.va;
     uint64_t* k1 = odd ? q.ka : q.kb;
     uint32_t* v1 = odd ? q.va : q.vb;
-    duplicate_batch_kernel<<<grid, 256, 0, stream>>>(p->vt, P, q.rank_pos, q.bbox, q.quad, q.ndup, q.scan, k0, v0,
-                                                     (uint32_t)p->cap, q.header + 1);
-    for (int g = 0; g < p->gt.n; ++g) {
-      launch_radix_sort(k0, v0, k1, v1, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, p->key_bits, q.sort_tmp,
-                        stream, kPosShift);
-      const uint32_t g_tiles = (g + 1 < p->gt.n ? p->gt.tile_base[g + 1] : (uint32_t)p->total_tiles) -
-                               p->gt.tile_base[g];
-      launch_tile_ranges(q.ka, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, kPosShift, p->gt.tile_base[g],
-                         g_tiles, q.ranges, stream);
+    if (p->binning) {
+      // Counting sort by tile instead: per-tile counts, their scan, then
+      // every instance scattered into its tile's range (in ka/va directly).
+      const uint32_t T = (uint32_t)p->total_tiles;
+      cudaMemsetAsync(q.oval, 0, (size_t)T * sizeof(uint32_t), stream);
+      duplicate_batch_kernel<kDupCount><<<grid, 256, 0, stream>>>(p->vt, P, q.rank_pos, q.bbox, q.quad, q.ndup,
+                                                                  q.scan, q.ka, q.va, (uint32_t)p->cap, q.header + 1,
+                                                                  q.oval, q.ranges);
+      launch_scan_inclusive(q.oval, q.order_fwd, T, q.scan_tmp, q.header + 6, ~0ull, nullptr, stream);
+      bin_ranges_kernel<<<(T + 255) / 256, 256, 0, stream>>>(T, q.oval, q.order_fwd, q.ranges);
+      duplicate_batch_kernel<kDupScatter><<<grid, 256, 0, stream>>>(p->vt, P, q.rank_pos, q.bbox, q.quad, q.ndup,
+                                                                    q.scan, q.ka, q.va, (uint32_t)p->cap,
+                                                                    q.header + 1, q.oval, q.ranges);
+    } else {
+      duplicate_batch_kernel<kDupWrite><<<grid, 256, 0, stream>>>(p->vt, P, q.rank_pos, q.bbox, q.quad, q.ndup,
+                                                                  q.scan, k0, v0, (uint32_t)p->cap, q.header + 1,
+                                                                  nullptr, nullptr);
+      for (int g = 0; g < p->gt.n; ++g) {
+        launch_radix_sort(k0, v0, k1, v1, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, p->key_bits,
+                          q.sort_tmp, stream, kPosShift);
+        const uint32_t g_tiles = (g + 1 < p->gt.n ? p->gt.tile_base[g + 1] : (uint32_t)p->total_tiles) -
+                                 p->gt.tile_base[g];
+        launch_tile_ranges(q.ka, segs + 2 * g, segs + 2 * g + 1, (uint32_t)p->cap, kPosShift, p->gt.tile_base[g],
+                           g_tiles, q.ranges, stream);
+      }
     }
     // the radix histograms in sort_tmp are dead here; the segment sort reuses it
     launch_tile_segment_sort(q.ranges, (int)p->total_tiles, q.ka, q.va, q.kb, q.vb, p->pos_bits, p->cap,

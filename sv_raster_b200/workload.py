@@ -383,11 +383,14 @@ class BatchedWorkload:
         passes = math.ceil(int(T_).bit_length() / 10)  # radix passes over the tile bits (8-10 bit digits)
         g = self.raster.n_groups
         order = self.raster.schedule[0]
-        # project 1 + scan 3 + segments 1 + duplicate 1 + (sort 3/pass + ranges 1) per group
-        # + segment sort 4 (plan, small, chunk, merge) + per ordered compositing stage a
-        # tile-order key kernel and one 3-kernel sort pass + fwd 1 + bwd 1 + sh 1
+        # project 1 + scan 3 + segments 1 + grouping by tile + segment sort 4 (plan, small,
+        # chunk, merge) + per ordered compositing stage a tile-order key kernel and one
+        # 3-kernel sort pass + fwd 1 + bwd 1 + sh 1.  Grouping by tile: counting sort =
+        # count 1 + tile scan 3 + ranges 1 + scatter 1; radix = duplicate 1 + (sort 3/pass
+        # + ranges 1) per group.
         n_order = 4 * ((order & 1) + ((order >> 1) & 1))
-        return 1 + 3 + 1 + 1 + g * (3 * passes + 1) + 4 + n_order + 1 + 1 + 1
+        grouping = 6 if getattr(self.raster, "binning", 0) else 1 + g * (3 * passes + 1)
+        return 1 + 3 + 1 + grouping + 4 + n_order + 1 + 1 + 1
 
     def kernel_stats(self):
         torch.cuda.synchronize()

@@ -27,6 +27,9 @@ class FakeRaster:
     def set_reduction(self, k):
         self.atomic_lanes = k
 
+    def set_binning(self, b):
+        self.binning = b
+
     def set_schedule(self, fwd_ordered=True, bwd_ordered=True, fwd_ctas_per_sm=0, bwd_ctas_per_sm=0):
         self.schedule = (int(fwd_ordered) | (int(bwd_ordered) << 1), fwd_ctas_per_sm, bwd_ctas_per_sm)
 
@@ -57,6 +60,7 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
         t -= 1.5 if (r.schedule[0] & 1) == 0 else 0.0
         t -= 0.5 * (r.schedule[2] == 3)
         t -= 0.25 * (getattr(r, "atomic_lanes", 1) == 4)
+        t -= 0.125 * (getattr(r, "binning", 1) == 0)
         return t
 
     geos = torch.zeros(r.P, 8)
@@ -72,7 +76,8 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
     assert (r.tile_size, r.staging, r.sort_buckets) == (8, 64, (256, 4096))
     assert r.schedule == (2, 0, 3)
     assert res["choice"]["reduce"] == 4 and r.atomic_lanes == 4
-    assert set(res["timings"]) == {"tile", "sort", "fwd", "bwd", "reduce"}
+    assert res["choice"]["bin"] == 0 and r.binning == 0
+    assert set(res["timings"]) == {"tile", "bin", "sort", "fwd", "bwd", "reduce"}
     # second call: served from the cache, applied, no timing
     r2 = FakeRaster()
     res2 = autotune.tune_batched(r2, geos, sh0, shs, 3, timer=lambda *a: 1 / 0)

@@ -52,12 +52,16 @@ def _raster(C, max_level=None, views=(0, 1, 2), **kw):
     return r, cams
 
 
+@pytest.mark.parametrize("binning", [1, 0])
 @pytest.mark.parametrize("max_key_bits", [None, 40])
-def test_batched_forward_equals_plain(c1, max_key_bits, monkeypatch):
+def test_batched_forward_equals_plain(c1, max_key_bits, binning, monkeypatch):
+    """Counting sort by tile (binning 1) and radix passes over the tile bits
+    (0, with one or several sort groups) give the plain path's tile lists."""
     if max_key_bits:
         # 32 position bits + 8 bits for one view's tiles: one sort group per view
         monkeypatch.setenv("SVR_MAX_KEY_BITS", str(max_key_bits))
     r, _ = _raster(c1)
+    r.set_binning(binning)
     if max_key_bits:
         assert r.n_groups == 3
     total = r.fit_capacity(c1.sh0, c1.shs, 3)
@@ -96,9 +100,11 @@ def test_batched_forward_equals_plain(c1, max_key_bits, monkeypatch):
         tile0 += nt
 
 
-def test_large_tile_segments_match_plain_sort():
+@pytest.mark.parametrize("binning", [1, 0])
+def test_large_tile_segments_match_plain_sort(binning):
     """Low-resolution views put up to ~20k instances in one 16x16 tile, so the
-    per-tile segment sort takes its streamed (larger than shared memory) path;
+    per-tile segment sort takes its streamed (larger than shared memory) path
+    (and the counting sort's per-tile atomics are at their most contended);
     every tile list must still equal the plain path's full-key radix sort."""
     import dataclasses
     sc = synthetic.config_scene("c1")
@@ -106,6 +112,7 @@ def test_large_tile_segments_match_plain_sort():
             synthetic.make_camera(64, 64, 90.0, (2.2, 0.5, -1.8))]
     C = SceneTensors(dataclasses.replace(sc, cameras=cams))
     r = BatchedRasterizer([DevCam(c) for c in cams], C.octpath, C.centers, C.lengths, max_level=sc.max_level)
+    r.set_binning(binning)
     r.fit_capacity(C.sh0, C.shs, 3)
     r.prepare(C.sh0, C.shs, 3)
     color, T = r.render(C.geos)
@@ -265,16 +272,16 @@ def _render_and_grads(r, C, wC, wT):
     return color.clone(), T.clone(), dgeo.clone(), sub.clone(), dsh0.clone(), dshs.clone(), total
 
 
-@pytest.mark.parametrize("tile,stage,order,ctas,buckets,lanes", [
-    (8, 64, (True, True), (0, 0), (512, 4096), 4),
-    (8, 32, (True, False), (0, 0), (256, 4096), 1),
-    (8, 128, (False, True), (0, 0), (1024, 2048), 2),
-    (32, 256, (True, True), (0, 0), (512, 4096), 1),
-    (16, 128, (True, True), (0, 0), (256, 2048), 8),
-    (16, 512, (False, False), (0, 0), (1024, 4096), 2),
-    (16, 256, (False, True), (3, 2), (512, 2048), 32),
+@pytest.mark.parametrize("tile,stage,order,ctas,buckets,lanes,binning", [
+    (8, 64, (True, True), (0, 0), (512, 4096), 4, 1),
+    (8, 32, (True, False), (0, 0), (256, 4096), 1, 0),
+    (8, 128, (False, True), (0, 0), (1024, 2048), 2, 1),
+    (32, 256, (True, True), (0, 0), (512, 4096), 1, 0),
+    (16, 128, (True, True), (0, 0), (256, 2048), 8, 1),
+    (16, 512, (False, False), (0, 0), (1024, 4096), 2, 0),
+    (16, 256, (False, True), (3, 2), (512, 2048), 32, 0),
 ])
-def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas, buckets, lanes):
+def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas, buckets, lanes, binning):
     """Every tile size, staging depth, compositing schedule and sort-bucket
     setting the autotuner may pick renders bit-identical images and T (a pixel
     sees the same instances in the same order) and the same gradients up to
@@ -290,6 +297,7 @@ def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas,
     r.set_schedule(fwd_ordered=order[0], bwd_ordered=order[1], fwd_ctas_per_sm=ctas[0], bwd_ctas_per_sm=ctas[1])
     r.set_sort_buckets(*buckets)
     r.set_reduction(lanes)
+    r.set_binning(binning)
     got = _render_and_grads(r, c1, wC, wT)
     assert torch.equal(got[0], base[0]), "colour differs"
     assert torch.equal(got[1], base[1]), "T differs"
@@ -311,7 +319,7 @@ def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
     base = _render_and_grads(r0, c1, wC, wT)
     r, _ = _raster(c1)
     res = tune_batched(r, c1.geos, c1.sh0, c1.shs, 3, reps=2, warmup=1)
-    assert not res["cached"] and set(res["choice"]) == {"tile", "sort", "fwd", "bwd", "reduce"}
+    assert not res["cached"] and set(res["choice"]) == {"tile", "bin", "sort", "fwd", "bwd", "reduce"}
     got = _render_and_grads(r, c1, wC, wT)
     assert torch.equal(got[0], base[0])
     assert rel_err(got[2], base[2]) < 1e-5

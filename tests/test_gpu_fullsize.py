@@ -3,7 +3,8 @@ that do not depend on the size (the oracle is too slow at these sizes):
 
 * c4 (8M voxels, 8 views of 1920x1080, bf16 storage): the binning partitions
   the instances into per-tile ranges, every tile list is strictly increasing
-  in Morton rank and holds only instances whose bbox touches the tile;
+  in Morton rank and holds only instances whose bbox touches the tile; the
+  counting sort and the radix grouping produce the same instance array;
   images and T are bit-identical between 8x8 and 16x16 tiles; the backward is
   linear in the upstream gradient; no device error flag is raised.
 * c3 (2M voxels, 16 uneven views): every view of the batched path is
@@ -126,6 +127,17 @@ def test_c4_fullsize_binning_tiling_and_linearity(c4):
     for x1, x2 in zip(g1, g2):
         assert rel_err(x2, 2 * x1) < 1e-5
     assert float(g1[0].abs().sum()) > 0
+    # the counting sort by tile (default) and the radix passes over the tile
+    # bits give the same ranges and the same sorted instance array
+    assert r.binning == 1
+    vals1, rng1 = a["sorted_vals"][:total].clone(), a["ranges"].clone()
+    r.set_binning(0)
+    r.prepare(c4["sh0"], c4["shs"], 3)
+    torch.cuda.synchronize()
+    assert r.header() == (total, 0)
+    a0 = r.arrays()
+    assert torch.equal(a0["ranges"], rng1)
+    assert torch.equal(a0["sorted_vals"][:total], vals1)
     del r
     torch.cuda.empty_cache()
     # the same images with 16x16 tiles
