@@ -49,6 +49,13 @@ template <class CFG>
 constexpr int fwd_min_blocks() { return CFG::NT >= 1024 ? 1 : kFwdMinBlocks * 256 / CFG::NT; }
 template <class CFG>
 constexpr int bwd_min_blocks() { return CFG::NT >= 1024 ? 1 : kBwdMinBlocks * 256 / CFG::NT; }
+// Backward with the distortion terms: its extra per-pixel state spills at the
+// 64-register budget (44-64 bytes), so those variants run one CTA fewer per
+// 256 threads (85 registers at 64-thread CTAs).
+template <class CFG, bool DIST>
+constexpr int bwd_min_blocks_for() {
+  return (DIST && CFG::NT < 1024) ? (kBwdMinBlocks - 1) * 256 / CFG::NT : bwd_min_blocks<CFG>();
+}
 
 // Pixel of thread `tid` inside its tile: warp w owns micro-tile
 // (w % MX, w / MX) of 8x4 pixels, lanes row-major inside it.

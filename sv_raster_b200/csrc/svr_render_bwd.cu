@@ -29,7 +29,7 @@ struct BwdSmem {
 
 // CTA b back-propagates quadrant b % 4 of the 16x16 list order[b / 4].
 template <int NS, bool DEPTH, bool DIST, bool NORMAL>
-__global__ void __launch_bounds__(PlainTile::NT, bwd_min_blocks<PlainTile>())
+__global__ void __launch_bounds__(PlainTile::NT, (bwd_min_blocks_for<PlainTile, DIST>()))
 render_bwd_kernel(const __grid_constant__ BwdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BwdSmem<PlainTile>& sm = *reinterpret_cast<BwdSmem<PlainTile>*>(smem_raw);
