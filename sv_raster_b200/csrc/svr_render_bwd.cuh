@@ -46,50 +46,44 @@ __device__ __forceinline__ float warp_sum(float x) {
   return x;
 }
 
-// Reduce-scatter of 12 per-lane values over the warp in 16 shuffles (the
-// values are padded to 16 slots): after five halving steps lane l holds in
-// v[0] the warp total of slot (l >> 1) & 15; returns that slot for the even
-// lane that should publish it (-1 otherwise or for a padding slot).
+// Reduce-scatter of 12 per-lane values over the warp in 13 shuffles: halve
+// 12 -> 6 (xor 16) -> 3 (xor 8), pad the 3 to 4 and halve 4 -> 2 (xor 4)
+// -> 1 (xor 2), then add the pair (xor 1).  Lane l ends holding in v[0] the
+// warp total of slot 6*b4 + 3*b3 + 2*b2 + b1 (b_i = bit i of l) when
+// 2*b2 + b1 < 3; returns that slot for the even lane that should publish it
+// (-1 otherwise or for the padding slot).  Every slot 0-11 is published by
+// exactly one lane.
 __device__ __forceinline__ int warp_reduce_scatter12(float v[12], int lane) {
-  float a[8];
-  // step 1 (xor 16): keep slots 0-7 (lanes 0-15) or 8-15 (lanes 16-31)
+  // step 1 (xor 16): keep slots 0-5 (bit 4 clear) or 6-11 (bit 4 set)
+  float a[6];
   const bool hi16 = lane & 16;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const float lo_v = v[k];
-    const float hi_v = (k + 8 < 12) ? v[k + 8] : 0.f;
-    const float send = hi16 ? lo_v : hi_v;
-    const float keep = hi16 ? hi_v : lo_v;
+  for (int k = 0; k < 6; ++k) {
+    const float send = hi16 ? v[k] : v[k + 6];
+    const float keep = hi16 ? v[k + 6] : v[k];
     a[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
   }
-  // step 2 (xor 8): keep 4 of 8
-  float b[4];
+  // step 2 (xor 8): keep 3 of 6
+  float b[3];
   const bool hi8 = lane & 8;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const float send = hi8 ? a[k] : a[k + 4];
-    const float keep = hi8 ? a[k + 4] : a[k];
+  for (int k = 0; k < 3; ++k) {
+    const float send = hi8 ? a[k] : a[k + 3];
+    const float keep = hi8 ? a[k + 3] : a[k];
     b[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
   }
-  // step 3 (xor 4): keep 2 of 4
-  float c2[2];
+  // step 3 (xor 4): the 3 padded to 4, keep 2 (bit 2 set: slot 2 and the pad)
   const bool hi4 = lane & 4;
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const float send = hi4 ? b[k] : b[k + 2];
-    const float keep = hi4 ? b[k + 2] : b[k];
-    c2[k] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-  }
+  const float c0 = (hi4 ? b[2] : b[0]) + __shfl_xor_sync(0xffffffffu, hi4 ? b[0] : b[2], 4);
+  const float c1 = (hi4 ? 0.f : b[1]) + __shfl_xor_sync(0xffffffffu, hi4 ? b[1] : 0.f, 4);
   // step 4 (xor 2): keep 1 of 2
   const bool hi2 = lane & 2;
-  const float send = hi2 ? c2[0] : c2[1];
-  const float keep = hi2 ? c2[1] : c2[0];
-  float d = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  float d = (hi2 ? c1 : c0) + __shfl_xor_sync(0xffffffffu, hi2 ? c0 : c1, 2);
   // step 5 (xor 1): full sum on both lanes of the pair
   d += __shfl_xor_sync(0xffffffffu, d, 1);
   v[0] = d;
-  const int slot = (hi16 ? 8 : 0) + (hi8 ? 4 : 0) + (hi4 ? 2 : 0) + (hi2 ? 1 : 0);
-  return ((lane & 1) == 0 && slot < 12) ? slot : -1;
+  const int local = (hi4 ? 2 : 0) + (hi2 ? 1 : 0);
+  return ((lane & 1) == 0 && local < 3) ? (hi16 ? 6 : 0) + (hi8 ? 3 : 0) + local : -1;
 }
 
 template <class CFG, int NS, bool DEPTH, bool DIST, bool NORMAL>
