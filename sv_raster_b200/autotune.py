@@ -68,11 +68,17 @@ def _store_cache(path, data):
         pass
 
 
+# Bumped whenever the search space or the kernels behind it change, so that
+# choices cached by an older build are measured again rather than reused.
+CACHE_SCHEMA = 2
+
+
 def cache_key(raster, geos, sh0):
     dev = raster.dev
     name = torch.cuda.get_device_name(dev) if dev.type == "cuda" else "cpu"
     sizes = ",".join(f"{w}x{h}" for h, w in raster.sizes)
-    return f"{name}|P={raster.P}|views={sizes}|ns={raster.n_samp}|geo={geos.dtype}|sh={sh0.dtype}"
+    return (f"v{CACHE_SCHEMA}|{name}|P={raster.P}|views={sizes}|ns={raster.n_samp}|geo={geos.dtype}"
+            f"|sh={sh0.dtype}")
 
 
 def time_ms(fn, reps=5, warmup=2, stream=None):
