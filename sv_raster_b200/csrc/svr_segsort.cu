@@ -5,7 +5,10 @@
 // Together this yields exactly the order of one stable sort by the full
 // [tile | rank] key (forward.cu:678-686): the tile passes keep generation
 // order inside a tile, and every step below orders by rank with generation
-// order breaking ties.
+// order breaking ties.  The batched path may group by tile with a counting
+// sort instead, which leaves a tile's instances in no particular order; its
+// keys (rank positions) are unique inside a tile, so the sorted result is the
+// same.
 //
 // Tile sizes are heavy-tailed (in a dense 1080p scene the median tile holds a
 // few hundred instances while a few percent of the tiles hold tens of
