@@ -1,6 +1,8 @@
-"""The operator benchmark's grid builder (CPU): corner indices of octree voxels
-into a deduplicated grid address one point per distinct corner position."""
+"""The operator benchmark: its grid builder (CPU; corner indices of octree
+voxels into a deduplicated grid address one point per distinct corner
+position) and one small end-to-end run (GPU)."""
 import numpy as np
+import pytest
 import torch
 
 from sv_raster_b200 import synthetic
@@ -21,3 +23,21 @@ def test_grid_keys_share_coincident_corners():
     first[flat[::-1]] = np.arange(len(flat))[::-1]
     assert np.array_equal(pos, pos[first[flat]])
     assert len(np.unique(pos[first], axis=0)) == M
+
+
+@pytest.mark.gpu
+def test_opbench_runs_on_a_small_scene(tmp_path):
+    """The operator benchmark end to end on a 20k-voxel scene: every operator
+    timed, no error."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-m", "sv_raster_b200.opbench", "--voxels", "20000", "--reps", "1",
+                          "--warmup", "1"], cwd=root, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    res = json.loads(out.stdout.strip().splitlines()[-1])
+    assert set(res["ops"]) >= {"gather_geo", "gather_geo_bw", "gather_feat", "gather_feat_bw", "tv_bw",
+                               "tv_bw_sparse", "render_fwd_plain", "render_bwd_depth_normal_dist"}
+    assert all(v["ms"] > 0 for v in res["ops"].values())
