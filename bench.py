@@ -318,6 +318,7 @@ def run_train(args, sc, dev, world, rank):
             "scaling": "weak",
             "exchange": "sum all-reduce of the flat gradient buffer per step (NCCL)" if world > 1 else None,
             "plain_fp32": None if ms_p is None else {"ms_per_step": round(ms_p, 3), "steps": args.plain_steps,
+                                                     "untimed_first_steps": min(2, max(args.plain_steps - 1, 0)),
                                                      "peak_hbm_gb": round(peak_p / 1e9, 2)},
             "speedup_vs_plain": None if ms_p is None else round(ms_p / ms_b, 3),
             "peak_hbm_gb": round(peak_b / 1e9, 2),

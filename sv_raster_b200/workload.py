@@ -678,13 +678,21 @@ class PlainTrainWorkload:
         self.opt.step()
         return total
 
-    def run(self, steps):
+    def run(self, steps, warmup=2):
+        """Runs `steps` training steps from the initial parameters and returns
+        (ms per step, losses of all steps).  The first `warmup` steps (first
+        kernel loads, allocator growth, optimizer state) are left out of the
+        timing but not out of the losses, so the trajectories still compare
+        step for step with the batched form's."""
         st = torch.cuda.current_stream(self.dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        warmup = min(warmup, max(steps - 1, 0))
         losses = []
-        e0.record(st)
-        for _ in range(steps):
+        for k in range(steps):
+            if k == warmup:
+                torch.cuda.synchronize()
+                e0.record(st)
             losses.append(self._step())
         e1.record(st)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps, [float(x) for x in torch.stack(losses).cpu()]
+        return e0.elapsed_time(e1) / (steps - warmup), [float(x) for x in torch.stack(losses).cpu()]
