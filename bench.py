@@ -251,7 +251,7 @@ def main():
             "metric": "fwd+bwd ms/view", "value": round(value, 4), "unit": "ms/view", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if args.mode == "plain" else "bf16-storage/f32-compute", "data": "synthetic",
+            "dtype": "f32", "storage_dtype": "f32" if args.mode == "plain" else "bf16", "data": "synthetic",
             "config": {"workload": f"{args.config}: {sc.n_voxels} voxels, {n_views} views/rank "
                                    f"{sc.cameras[0].width}x{sc.cameras[0].height}, SH3, fwd+recompute bwd",
                        "mode": args.mode, "l2": "inputs larger than L2 (scene arrays > 126 MB)",
@@ -311,7 +311,7 @@ def run_train(args, sc, dev, world, rank):
     if rank == 0:
         print(json.dumps({
             "metric": "training ms/step", "value": round(ms_b, 3), "unit": "ms/step", "higher_is_better": False,
-            "n_gpus": world, "steps": args.steps, "data": "synthetic", "dtype": "bf16-storage/f32-compute",
+            "n_gpus": world, "steps": args.steps, "data": "synthetic", "dtype": "f32", "storage_dtype": "bf16",
             "config": {"workload": f"{args.config}: {sc.n_voxels} voxels, {len(sc.cameras)} views per step "
                                    f"({sc.cameras[0].width}x{sc.cameras[0].height} ... mixed), fwd + recompute bwd "
                                    f"+ fused Adam, one CUDA graph per step"},
