@@ -702,7 +702,9 @@ int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, 
   launch_scan_inclusive(q.ndup, q.scan, VP, q.scan_tmp, q.header, (unsigned long long)p->cap, q.header + 1, stream);
   uint32_t* segs = q.header + 16;
   group_segments_kernel<<<1, 64, 0, stream>>>(p->gt, P, q.scan, (uint32_t)p->cap, segs);
-  if (!p->binning) cudaMemsetAsync(q.ranges, 0, (size_t)p->total_tiles * sizeof(uint2), stream);
+  // the counting sort writes every tile's range itself; otherwise (radix
+  // grouping, or no instance capacity yet) empty tiles keep (0, 0)
+  if (!p->binning || p->cap == 0) cudaMemsetAsync(q.ranges, 0, (size_t)p->total_tiles * sizeof(uint2), stream);
   if (!p->pos_ready || p->pos_paths != octree_paths) {
     // Rank positions of all (voxel, quadrant) pairs: one stable radix sort of
     // the 8P compressed ranks in the (still free) instance arrays.

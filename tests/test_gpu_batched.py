@@ -233,6 +233,20 @@ def test_capacity_overflow_is_reported(c1):
     assert err & 0x4
 
 
+@pytest.mark.parametrize("binning", [1, 0])
+def test_zero_capacity_renders_background(c1, binning):
+    """A plan without instance capacity (before fit_capacity) reports the
+    overflow and composites every tile as empty: background colour, T = 1."""
+    r, _ = _raster(c1, capacity=0)
+    r.set_binning(binning)
+    r.prepare(c1.sh0, c1.shs, 3)
+    color, T = r.render(c1.geos)
+    torch.cuda.synchronize()
+    total, err = r.header()
+    assert total > 0 and err & 0x4
+    assert torch.all(T == 1.0) and torch.all(color == 0.0)
+
+
 def test_level_bound_is_checked(c1):
     r, _ = _raster(c1, max_level=5)  # the c1 voxels are at levels 6-8
     r.fit_capacity(c1.sh0, c1.shs, 3)
