@@ -273,7 +273,8 @@ int svr_batch_prepare(svr_batch_plan* plan, void* workspace, const int64_t* octr
                       const float* vox_lengths, const void* sh0, const void* shs, int sh_bf16, int sh_degree, int M,
                       void* stream);
 /* Compositing of every (view, tile) in one persistent launch; geos fp32 or bf16 [P,8].
- * Every pixel of out_color / out_T is written. */
+ * Every pixel of out_color / out_T is written.  Reads the tile lists of the
+ * last svr_batch_prepare on this workspace (call prepare first). */
 int svr_batch_render(svr_batch_plan* plan, void* workspace, const float* vox_centers, const float* vox_lengths,
                      const void* geos, int geos_bf16, float* out_color, float* out_T, void* stream);
 /* Recompute-backward of every (view, tile) in one persistent launch: dL_dgeos [P,8] and
