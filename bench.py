@@ -108,6 +108,20 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+def l2_note(sc, mode):
+    """Whether the step's inputs exceed the 126 MB L2 (no flush between steps
+    is needed then): the voxel arrays in their storage dtype plus the step's
+    per-view images."""
+    P = sc.n_voxels
+    elem = 4 if mode == "plain" else 2
+    vox = P * (8 + 12 + 4) + P * (8 + 3 + 45) * elem
+    pix = sum(c.width * c.height for c in sc.cameras) * 4 * 4  # colour + T, and their gradients
+    mb = (vox + pix) / 1e6
+    if mb > 126:
+        return f"inputs larger than L2 ({mb:.0f} MB of voxel arrays and images > 126 MB)"
+    return f"inputs fit in L2 ({mb:.0f} MB of voxel arrays and images), L2 not flushed between steps"
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -118,22 +132,7 @@ def load_peaks():
 
 def scene_for(args, rank, world):
     from sv_raster_b200 import synthetic
-    cache = f"/tmp/svr_scene_{args.config}_{args.voxels or 0}.pkl"
-    sc = None
-    if os.path.exists(cache):
-        import pickle
-        try:
-            sc = pickle.load(open(cache, "rb"))
-        except Exception:
-            sc = None
-    if sc is None:
-        sc = synthetic.config_scene(args.config, n_voxels=args.voxels)
-        try:
-            import pickle
-            pickle.dump(sc, open(cache + ".tmp", "wb"), protocol=4)
-            os.replace(cache + ".tmp", cache)
-        except OSError:
-            pass
+    sc = synthetic.cached_config_scene(args.config, n_voxels=args.voxels)
     from sv_raster_b200.workload import rank_cameras
     cams = sc.cameras[: args.views] if args.views else sc.cameras
     sc.cameras = rank_cameras(cams, rank, world)  # weak scaling: each rank its own views
@@ -254,7 +253,7 @@ def main():
             "dtype": "f32", "storage_dtype": "f32" if args.mode == "plain" else "bf16", "data": "synthetic",
             "config": {"workload": f"{args.config}: {sc.n_voxels} voxels, {n_views} views/rank "
                                    f"{sc.cameras[0].width}x{sc.cameras[0].height}, SH3, fwd+recompute bwd",
-                       "mode": args.mode, "l2": "inputs larger than L2 (scene arrays > 126 MB)",
+                       "mode": args.mode, "l2": l2_note(sc, args.mode),
                        "instances_per_view": wl.instances_per_view()},
             "autotuned": getattr(wl, "tuned", None),
             "render_fps": round(1000.0 / kstats["fwd_ms_per_view"], 2) if kstats.get("fwd_ms_per_view") else None,

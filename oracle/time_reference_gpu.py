@@ -41,12 +41,7 @@ def main():
     import build_ref
     from sv_raster_b200 import synthetic
     ref = build_ref.load()
-    cache = f"/tmp/svr_scene_{a.config}_{a.voxels or 0}.pkl"
-    if os.path.exists(cache):
-        import pickle
-        sc = pickle.load(open(cache, "rb"))
-    else:
-        sc = synthetic.config_scene(a.config, n_voxels=a.voxels)
+    sc = synthetic.cached_config_scene(a.config, n_voxels=a.voxels)
     cams = sc.cameras[: a.views] if a.views else sc.cameras
     dev = "cuda"
     t = lambda x, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(x)).to(dev, dt)
@@ -97,10 +92,10 @@ def main():
 def time_ops(n_voxels, reps=10, warmup=3):
     """The reference's counterparts of the opbench operators, same inputs."""
     import build_ref
-    from sv_raster_b200 import opbench
+    from sv_raster_b200 import opbench, synthetic
     ref = build_ref.load()
     dev = torch.device("cuda")
-    sc = opbench._scene(n_voxels)
+    sc = synthetic.cached_config_scene("c2", n_voxels=n_voxels)
     N = len(sc.octpath)
     key, M = opbench.grid_keys(sc.octpath, sc.octlevel, dev)
     care = torch.arange(N, device=dev)

@@ -22,7 +22,6 @@ bounded by the gather pattern rather than by streaming bandwidth.
 import argparse
 import json
 import os
-import pickle
 
 import numpy as np
 import torch
@@ -30,24 +29,6 @@ import torch
 from . import _C as mC
 from . import synthetic
 from .grid_loss_bw import total_variation
-
-
-def _scene(n_voxels):
-    path = f"/tmp/svr_scene_c2_0{'' if n_voxels is None else '_' + str(n_voxels)}.pkl"
-    if os.path.exists(path):
-        try:
-            with open(path, "rb") as f:
-                return pickle.load(f)
-        except Exception:
-            pass
-    sc = synthetic.config_scene("c2", n_voxels=n_voxels)
-    try:
-        with open(path + ".tmp", "wb") as f:
-            pickle.dump(sc, f, protocol=4)
-        os.replace(path + ".tmp", path)
-    except OSError:
-        pass
-    return sc
 
 
 def grid_keys(octpath, level, dev):
@@ -100,7 +81,7 @@ def main():
     if not torch.cuda.is_available():
         raise SystemExit("opbench needs a CUDA device")
     dev = torch.device("cuda")
-    sc = _scene(args.voxels)
+    sc = synthetic.cached_config_scene("c2", n_voxels=args.voxels)
     N = len(sc.octpath)
     key, M = grid_keys(sc.octpath, sc.octlevel, dev)
     care = torch.arange(N, device=dev)

@@ -16,6 +16,8 @@ Cameras are OpenCV pinholes (x right, y down, z forward) with row-major 4x4
 image centre.  All randomness comes from ``numpy.random.default_rng(seed)``.
 """
 import math
+import os
+import pickle
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -343,3 +345,37 @@ def config_scene(name, seed=0, n_voxels=None):
                                   fixed_size=(int(1920 * s) // 2 * 2, int(1080 * s) // 2 * 2))
         return build_scene("c5", n_voxels or 16_000_000, seed, "mixed", (6, 16), (5, 7), -2.0, 1.5, cams)
     raise ValueError(f"unknown config {name}")
+
+
+def scene_cache_dir():
+    """Directory of cached scenes: SVR_SCENE_CACHE, else a per-user cache
+    directory (created private to the user)."""
+    return os.environ.get("SVR_SCENE_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "sv_raster_b200",
+                                                              "scenes")
+
+
+def cached_config_scene(name, seed=0, n_voxels=None):
+    """config_scene with an on-disk cache (the 8M- and 16M-voxel scenes take
+    minutes to build on the CPU).  Scenes are deterministic in (name, seed,
+    n_voxels), so a cached copy equals a rebuilt one; the cache directory is
+    the user's own, never a shared temporary directory, because entries are
+    unpickled.  Writers use a per-process temporary name, so concurrent ranks
+    building the same scene do not interleave their writes."""
+    d = scene_cache_dir()
+    path = os.path.join(d, f"{name}_{seed}_{n_voxels or 0}.pkl")
+    if os.path.exists(path):
+        try:
+            with open(path, "rb") as f:
+                return pickle.load(f)
+        except Exception:
+            pass  # unreadable or partial entry: rebuild it
+    sc = config_scene(name, seed=seed, n_voxels=n_voxels)
+    try:
+        os.makedirs(d, mode=0o700, exist_ok=True)
+        tmp = f"{path}.{os.getpid()}.tmp"
+        with open(tmp, "wb") as f:
+            pickle.dump(sc, f, protocol=4)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+    return sc

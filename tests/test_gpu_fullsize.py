@@ -10,9 +10,6 @@ that do not depend on the size (the oracle is too slow at these sizes):
 * c3 (2M voxels, 16 uneven views): every view of the batched path is
   bit-identical to the plain per-view path (fp32 storage).
 """
-import os
-import pickle
-
 import numpy as np
 import pytest
 import torch
@@ -34,22 +31,8 @@ class DevCam:
 
 
 def _scene(name):
-    """The seeded scene of a configuration (cached in /tmp like bench.py)."""
-    path = f"/tmp/svr_scene_{name}_0.pkl"
-    if os.path.exists(path):
-        try:
-            with open(path, "rb") as f:
-                return pickle.load(f)
-        except Exception:
-            pass
-    sc = synthetic.config_scene(name)
-    try:
-        with open(path + ".tmp", "wb") as f:
-            pickle.dump(sc, f, protocol=4)
-        os.replace(path + ".tmp", path)
-    except OSError:
-        pass
-    return sc
+    """The seeded scene of a configuration (shared cache with bench.py)."""
+    return synthetic.cached_config_scene(name)
 
 
 def _octant_repeat(q):
