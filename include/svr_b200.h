@@ -67,16 +67,19 @@ int svr_rasterize_preprocess(const svr_camera* cam, int64_t P, const int64_t* oc
                              const float* vox_centers, const float* vox_lengths, int32_t* out_n_duplicates,
                              void* geom_buffer, size_t geom_bytes, int debug, void* stream);
 
-/* svr_rasterize_preprocess without any caller-provided scratch.  No
+/* svr_rasterize_preprocess whose scan scratch lives inside the library.  No
  * counterpart in the reference.  For callers that cannot allocate device
  * memory (an embedding host that owns every device buffer, code inside CUDA
  * graph capture, real-time loops): the scan's partial sums live in a static
  * device array of the library, so P is limited to svr_noalloc_max_voxels()
  * (67,108,864); larger P returns SVR_ERR_CAPACITY.  Same arguments and
- * outputs as svr_rasterize_preprocess; the geom buffer is still the caller's
- * output.  The first call on a device looks up the array's device address
- * (make it before any stream capture).  All calls share the array: calls that
- * overlap on the GPU race.  The function allocates nothing. */
+ * outputs as svr_rasterize_preprocess, and the geom buffer is sized the same
+ * way (svr_geom_buffer_bytes): its layout is shared with the other calls, so
+ * the scratch region it reserves stays unused here.  The first call on a
+ * device looks up the array's device address (make it before any stream
+ * capture; a failed lookup is retried by the next call).  All calls share
+ * the array: calls that overlap on the GPU race.  The function allocates
+ * nothing. */
 int svr_rasterize_preprocess_noalloc(const svr_camera* cam, int64_t P, const int64_t* octree_paths,
                                      const float* vox_centers, const float* vox_lengths, int32_t* out_n_duplicates,
                                      void* geom_buffer, size_t geom_bytes, int debug, void* stream);
@@ -252,7 +255,7 @@ int svr_batch_plan_tile_size(const svr_batch_plan* plan);
 /* Backward gradient reduction inside a warp: a staged record's 12 gradient
  * values from at most atomic_lanes (1-32, default 1) contributing lanes are
  * added to its shared accumulator with atomics, from more lanes through a
- * 16-shuffle reduce-scatter.  Only the order of additions changes. */
+ * 13-shuffle reduce-scatter.  Only the order of additions changes. */
 int svr_batch_plan_set_reduction(svr_batch_plan* plan, int atomic_lanes);
 int64_t svr_batch_plan_pixels(const svr_batch_plan* plan);
 int64_t svr_batch_plan_tiles(const svr_batch_plan* plan);

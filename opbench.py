@@ -1,6 +1,6 @@
 """Device timings of the plain-path operators around the core render step.
 
-Run on a GPU as ``python -m sv_raster_b200.opbench [--voxels N]``; prints one
+Run on a GPU as ``python opbench.py [--voxels N]``; prints one
 JSON object.  Every figure is the median of CUDA-event timings on the current
 stream after warm-up, on the seeded 2M-voxel scene with one 1297x840 view
 (the single-view benchmark scene):
@@ -22,29 +22,16 @@ bounded by the gather pattern rather than by streaming bandwidth.
 import argparse
 import json
 import os
+import sys
 
 import numpy as np
 import torch
 
-from . import _C as mC
-from . import synthetic
-from .grid_loss_bw import total_variation
-
-
-def grid_keys(octpath, level, dev):
-    """Corner-point indices [N,8] of octree voxels into a deduplicated grid.
-
-    Corner (i+di, j+dj, k+dk) of a level-l cell is expressed at the finest
-    level (shifted by 16-l) so coincident corners of cells of different sizes
-    share one grid point; corner order is di*4 + dj*2 + dk.
-    """
-    ijk = torch.from_numpy(synthetic.octpath_to_ijk(octpath, level)).to(dev)
-    shift = (16 - torch.from_numpy(np.asarray(level, dtype=np.int64).reshape(-1))).to(dev)
-    off = torch.tensor([[(c >> 2) & 1, (c >> 1) & 1, c & 1] for c in range(8)], dtype=torch.int64, device=dev)
-    corner = (ijk[:, None, :] + off[None]) << shift[:, None, None]
-    code = (corner[..., 0] << 34) | (corner[..., 1] << 17) | corner[..., 2]
-    uniq, inv = torch.unique(code.reshape(-1), return_inverse=True)
-    return inv.reshape(-1, 8).contiguous(), int(uniq.numel())
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from sv_raster_b200 import _C as mC  # noqa: E402
+from sv_raster_b200 import synthetic  # noqa: E402
+from sv_raster_b200.grid_loss_bw import total_variation  # noqa: E402
+from sv_raster_b200.synthetic import grid_keys  # noqa: E402
 
 
 def time_ms(fn, reps, warmup):
@@ -64,7 +51,7 @@ def time_ms(fn, reps, warmup):
 
 
 def _peak_gbs():
-    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    here = os.path.dirname(os.path.abspath(__file__))
     try:
         with open(os.path.join(here, "MEASURED_PEAKS.json")) as f:
             return float(json.load(f)["hbm_gbs"]), "measured"

@@ -12,6 +12,10 @@ The built module is used only by ``tests/`` (bit-exact integer parity and FP32
 tolerance parity on the GPU) and by the golden-fixture generator
 ``tests/golden/make_golden.py``.  Nothing in ``sv_raster_b200`` imports it.
 
+The reference checkout is taken from the command line, else from the
+SVR_REFERENCE_ROOT environment variable, else from the container's read-only
+mount (DEFAULT_ROOT).
+
 Usage:  python oracle/build_ref.py [REFERENCE_ROOT]
 """
 import os
@@ -21,6 +25,13 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 MODULE = "svraster_ref_C"
+DEFAULT_ROOT = "/root/reference"
+
+
+def reference_root():
+    """Where the reference checkout is read from (None when it is absent)."""
+    root = os.environ.get("SVR_REFERENCE_ROOT") or DEFAULT_ROOT
+    return root if os.path.isdir(os.path.join(root, "backends", "cuda")) else None
 
 SOURCES = [
     "src/raster_state.cu",
@@ -40,7 +51,10 @@ def built_path():
     return os.path.join(OUT_DIR, MODULE + ".so")
 
 
-def build(ref_root="/root/reference", verbose=False):
+def build(ref_root=None, verbose=False):
+    ref_root = ref_root or reference_root()
+    if ref_root is None:
+        raise FileNotFoundError("reference checkout not found (set SVR_REFERENCE_ROOT)")
     backend = os.path.join(ref_root, "backends", "cuda")
     if not os.path.isdir(backend):
         raise FileNotFoundError(f"reference backend not found at {backend}")
@@ -80,5 +94,4 @@ def load():
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    print(build(root, verbose=True))
+    print(build(sys.argv[1] if len(sys.argv) > 1 else None, verbose=True))

@@ -10,7 +10,7 @@ JSON line with ms/view (CUDA events around all views of a step, fp32).
 With --ops it instead times the reference's grid-point gathers, TV gradient
 and the plain forward / backward with depth, normal and distortion outputs on
 the 2M-voxel single-view scene, with the same inputs, keys and CUDA-event
-medians as ``python -m sv_raster_b200.opbench`` (one JSON object).
+medians as ``python opbench.py`` (one JSON object).
 
 Usage: python oracle/time_reference_gpu.py [--config c4] [--steps 3] [--warmup 1] [--ops]
 """
@@ -92,12 +92,13 @@ def main():
 def time_ops(n_voxels, reps=10, warmup=3):
     """The reference's counterparts of the opbench operators, same inputs."""
     import build_ref
-    from sv_raster_b200 import opbench, synthetic
+    import opbench
+    from sv_raster_b200 import synthetic
     ref = build_ref.load()
     dev = torch.device("cuda")
     sc = synthetic.cached_config_scene("c2", n_voxels=n_voxels)
     N = len(sc.octpath)
-    key, M = opbench.grid_keys(sc.octpath, sc.octlevel, dev)
+    key, M = synthetic.grid_keys(sc.octpath, sc.octlevel, dev)
     care = torch.arange(N, device=dev)
     g = torch.Generator(device=dev).manual_seed(0)
     pts1 = torch.randn(M, 1, device=dev, generator=g)

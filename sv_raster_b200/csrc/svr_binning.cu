@@ -26,10 +26,7 @@ namespace svr {
 // --------------------------------------------------------------------------
 // Inclusive scan of uint32 counts (three phases, no inter-CTA waiting)
 // --------------------------------------------------------------------------
-constexpr int kScanThreads = 256;
-constexpr int kScanItems = 16;
-constexpr int kScanTile = kScanThreads * kScanItems;
-
+// kScanThreads, kScanItems and kScanTile are declared in svr_kernels.h.
 size_t scan_temp_bytes(size_t n) {
   const size_t nb = (n + kScanTile - 1) / kScanTile;
   return (nb + 1) * sizeof(unsigned long long) + 256;

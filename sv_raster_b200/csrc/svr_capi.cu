@@ -2,7 +2,7 @@
 // of the plain (one view per call) path.  See include/svr_b200.h.
 #include <cmath>
 #include <cstring>
-#include <mutex>
+#include <atomic>
 
 #include "../../include/svr_b200.h"
 #include "svr_common.cuh"
@@ -566,25 +566,28 @@ int svr_read_error(uint32_t* device_word, uint32_t* host_value, void* stream_) {
 // in the caller's geom buffer.  It bounds P to kNoAllocMaxVoxels.
 //
 // The array is a host-side stand-in in host code, not a device address: its
-// device address is taken with cudaGetSymbolAddress once per device, on the
+// device address is taken with cudaGetSymbolAddress once per device, by the
 // first call made with that device current (so that first call should come
-// before any stream capture).  Every call shares the array: calls that
-// overlap on the GPU (two streams, or two threads) race on it.  Nothing in it
-// needs clearing between calls: each call writes every partial sum it later
-// reads.
+// before any stream capture; a lookup that fails is retried by the next
+// call).  Every call shares the array: calls that overlap on the GPU (two
+// streams, or two threads) race on it.  Nothing in it needs clearing between
+// calls: each call writes every partial sum it later reads.
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr int64_t kNoAllocScanTile = 4096;                 // items per scan CTA (svr_binning.cu)
-constexpr int64_t kNoAllocMaxBlocks = 16384;               // 128 KB of partial sums
-constexpr int64_t kNoAllocMaxVoxels = kNoAllocScanTile * kNoAllocMaxBlocks;  // 67,108,864
+// One 64-bit partial sum per scan CTA of kScanTile voxels (svr_kernels.h),
+// plus the alignment slack scan_temp_bytes() reserves.
+constexpr int64_t kNoAllocMaxBlocks = 16384;
+constexpr int64_t kNoAllocMaxVoxels = (int64_t)kScanTile * kNoAllocMaxBlocks;  // 67,108,864
+constexpr int64_t kNoAllocWords = kNoAllocMaxBlocks + 1 + 256 / sizeof(unsigned long long);
 
-__device__ __align__(256) unsigned long long g_noalloc_scan_partials[kNoAllocMaxBlocks + 32];
+__device__ __align__(256) unsigned long long g_noalloc_scan_partials[kNoAllocWords];
 
 constexpr int kNoAllocMaxDevices = 64;
-std::once_flag g_noalloc_once[kNoAllocMaxDevices];
-void* g_noalloc_ptr[kNoAllocMaxDevices];
-cudaError_t g_noalloc_status[kNoAllocMaxDevices];
+// Device address of the array per device, set once a lookup succeeds; a
+// failed lookup (made during a stream capture, say) leaves it null, and the
+// next call on that device tries again.
+std::atomic<void*> g_noalloc_ptr[kNoAllocMaxDevices];
 
 // Device address of the partial-sum array on the current device.
 void* noalloc_scratch(int& status) {
@@ -593,17 +596,17 @@ void* noalloc_scratch(int& status) {
     status = SVR_ERR_CUDA;
     return nullptr;
   }
-  std::call_once(g_noalloc_once[dev], [dev] {
-    void* ptr = nullptr;
-    g_noalloc_status[dev] = cudaGetSymbolAddress(&ptr, g_noalloc_scan_partials);
-    g_noalloc_ptr[dev] = ptr;
-  });
-  if (g_noalloc_status[dev] != cudaSuccess || !g_noalloc_ptr[dev]) {
-    status = SVR_ERR_CUDA;
-    return nullptr;
+  void* ptr = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+  if (!ptr) {
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_scan_partials) != cudaSuccess || !ptr) {
+      cudaGetLastError();  // clear it, so that a later launch check does not report it again
+      status = SVR_ERR_CUDA;
+      return nullptr;
+    }
+    g_noalloc_ptr[dev].store(ptr, std::memory_order_release);
   }
   status = SVR_OK;
-  return g_noalloc_ptr[dev];
+  return ptr;
 }
 
 }  // namespace
@@ -615,7 +618,7 @@ extern "C" int svr_rasterize_preprocess_noalloc(const svr_camera* cam, int64_t P
   (void)octree_paths;
   cudaStream_t stream = static_cast<cudaStream_t>(stream_);
   if (P < 0 || P >= (1ll << kVoxIdBits) || !valid_camera(cam)) return SVR_ERR_SHAPE;
-  if (P > kNoAllocMaxVoxels) return SVR_ERR_CAPACITY;
+  if (P > kNoAllocMaxVoxels || scan_temp_bytes((size_t)P) > sizeof(g_noalloc_scan_partials)) return SVR_ERR_CAPACITY;
   if (P == 0) return SVR_OK;
   GeomLayout g = geom_layout(geom_buffer, P);
   if (!geom_buffer || geom_bytes < g.bytes || !vox_centers || !vox_lengths || !out_n_duplicates) return SVR_ERR_SHAPE;

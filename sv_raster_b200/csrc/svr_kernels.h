@@ -20,6 +20,11 @@ void launch_preprocess(const ViewTable& views, int P, const float* centers, cons
                        uint32_t* ndup, uint2* bboxes, uint32_t* quads, cudaStream_t stream);
 
 // svr_binning.cu
+// Inclusive scan: CTAs of kScanThreads threads, kScanItems items each; the
+// scratch holds one 64-bit partial sum per CTA (scan_temp_bytes).
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
 size_t scan_temp_bytes(size_t n);
 void launch_scan_inclusive(const uint32_t* in, uint32_t* out, size_t n, void* temp, uint32_t* d_total,
                            unsigned long long cap, uint32_t* err, cudaStream_t stream);

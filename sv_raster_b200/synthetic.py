@@ -347,6 +347,24 @@ def config_scene(name, seed=0, n_voxels=None):
     raise ValueError(f"unknown config {name}")
 
 
+def grid_keys(octpath, level, dev):
+    """Corner-point indices [N,8] of octree voxels into a deduplicated grid.
+
+    Corner (i+di, j+dj, k+dk) of a level-l cell is expressed at the finest
+    level (shifted by 16-l) so coincident corners of cells of different sizes
+    share one grid point; corner order is di*4 + dj*2 + dk.  Returns
+    (vox_key int64[N,8] on `dev`, number of grid points).
+    """
+    import torch
+    ijk = torch.from_numpy(octpath_to_ijk(octpath, level)).to(dev)
+    shift = (16 - torch.from_numpy(np.asarray(level, dtype=np.int64).reshape(-1))).to(dev)
+    off = torch.tensor([[(c >> 2) & 1, (c >> 1) & 1, c & 1] for c in range(8)], dtype=torch.int64, device=dev)
+    corner = (ijk[:, None, :] + off[None]) << shift[:, None, None]
+    code = (corner[..., 0] << 34) | (corner[..., 1] << 17) | corner[..., 2]
+    uniq, inv = torch.unique(code.reshape(-1), return_inverse=True)
+    return inv.reshape(-1, 8).contiguous(), int(uniq.numel())
+
+
 def scene_cache_dir():
     """Directory of cached scenes: SVR_SCENE_CACHE, else a per-user cache
     directory (created private to the user)."""
@@ -354,15 +372,29 @@ def scene_cache_dir():
                                                               "scenes")
 
 
+def generator_digest():
+    """Short digest of this module's source: cached scenes are keyed by it, so
+    a change to the generator never reuses scenes an older one built."""
+    import hashlib
+    with open(os.path.abspath(__file__), "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()[:12]
+
+
+def cached_scene_path(name, seed=0, n_voxels=None):
+    """Cache file of a configuration's scene for the current generator."""
+    return os.path.join(scene_cache_dir(), f"{name}_{seed}_{n_voxels or 0}_{generator_digest()}.pkl")
+
+
 def cached_config_scene(name, seed=0, n_voxels=None):
     """config_scene with an on-disk cache (the 8M- and 16M-voxel scenes take
     minutes to build on the CPU).  Scenes are deterministic in (name, seed,
-    n_voxels), so a cached copy equals a rebuilt one; the cache directory is
+    n_voxels) for a given generator source (its digest is part of the file
+    name), so a cached copy equals a rebuilt one; the cache directory is
     the user's own, never a shared temporary directory, because entries are
     unpickled.  Writers use a per-process temporary name, so concurrent ranks
     building the same scene do not interleave their writes."""
-    d = scene_cache_dir()
-    path = os.path.join(d, f"{name}_{seed}_{n_voxels or 0}.pkl")
+    path = cached_scene_path(name, seed, n_voxels)
+    d = os.path.dirname(path)
     if os.path.exists(path):
         try:
             with open(path, "rb") as f:

@@ -76,3 +76,36 @@ def rel_err(a, b):
     b = b.double()
     den = b.norm().item()
     return (a - b).norm().item() / max(den, 1e-30)
+
+
+def sh_rgbs(C, cam_pos, deg=3):
+    """Per-voxel colours of every voxel from the native SH kernel."""
+    from sv_raster_b200 import _C as mC
+    return mC.sh_compute(deg, torch.empty(0, dtype=torch.int64), C.centers, cam_pos, C.sh0, C.shs)
+
+
+def run_view(mod, C, cam_i, ns, depth=False, dist=False, normal=False, maxw=False, bg=0.0, rgbs=None, geos=None):
+    """Projection + forward of one camera through `mod` (the native `_C` ops or
+    the reference module: same signatures, binding.cpp:24-55)."""
+    cam, w2c, c2w = C.cam(cam_i)
+    ndup, geom = mod.rasterize_preprocess(cam.width, cam.height, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w,
+                                          cam.near, C.octpath, C.centers, C.lengths, False)
+    if rgbs is None:
+        rgbs = sh_rgbs(C, c2w[:3, 3])
+    geos = C.geos if geos is None else geos
+    out = mod.rasterize_voxels(ns, cam.width, cam.height, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w, bg,
+                               depth, dist, normal, maxw, C.octpath, C.centers, C.lengths, geos, rgbs, geom, False)
+    return dict(ndup=ndup, geom=geom, R=out[0], binning=out[1], img=out[2], color=out[3], depth=out[4],
+                normal=out[5], T=out[6], max_w=out[7], rgbs=rgbs, geos=geos, cam=cam, w2c=w2c, c2w=c2w)
+
+
+def run_bwd(mod, C, r, ns, dC, dT, dD=None, dN=None, depth=False, normal=False, lam_R=0.0, gt=None, lam_asc=0.0,
+            lam_dist=0.0, bg=0.0):
+    """Backward of a run_view result through `mod`: (dL_dgeos, dL_drgbs, subdiv_p_bw)."""
+    cam = r["cam"]
+    e = torch.empty(0, device="cuda")
+    return mod.rasterize_voxels_backward(
+        r["R"], ns, cam.width, cam.height, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, r["w2c"], r["c2w"], bg,
+        C.octpath, C.centers, C.lengths, r["geos"], r["rgbs"], r["geom"], r["binning"], r["img"], r["T"], dC,
+        dD if dD is not None else e, dN if dN is not None else e, dT, lam_R, gt if gt is not None else e, lam_asc,
+        lam_dist, depth, normal, r["depth"], r["normal"], False)

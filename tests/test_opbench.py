@@ -6,7 +6,7 @@ import pytest
 import torch
 
 from sv_raster_b200 import synthetic
-from sv_raster_b200.opbench import grid_keys
+from sv_raster_b200.synthetic import grid_keys
 
 
 def test_grid_keys_share_coincident_corners():
@@ -34,7 +34,7 @@ def test_opbench_runs_on_a_small_scene(tmp_path):
     import subprocess
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    out = subprocess.run([sys.executable, "-m", "sv_raster_b200.opbench", "--voxels", "20000", "--reps", "1",
+    out = subprocess.run([sys.executable, os.path.join(root, "opbench.py"), "--voxels", "20000", "--reps", "1",
                           "--warmup", "1"], cwd=root, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     res = json.loads(out.stdout.strip().splitlines()[-1])

@@ -14,7 +14,8 @@ def test_cached_scene_equals_rebuilt(tmp_path, monkeypatch):
     a = synthetic.cached_config_scene("c1", n_voxels=2000)
     assert stat.S_IMODE(os.stat(d).st_mode) == 0o700
     files = os.listdir(d)
-    assert files == ["c1_0_2000.pkl"]
+    name = f"c1_0_2000_{synthetic.generator_digest()}.pkl"
+    assert files == [name]
     b = synthetic.cached_config_scene("c1", n_voxels=2000)  # from the cache
     c = synthetic.config_scene("c1", n_voxels=2000)          # rebuilt
     for x in (a, b):
@@ -22,6 +23,6 @@ def test_cached_scene_equals_rebuilt(tmp_path, monkeypatch):
             assert np.array_equal(getattr(x, f), getattr(c, f))
         assert [cam.width for cam in x.cameras] == [cam.width for cam in c.cameras]
     # a truncated entry is rebuilt, not trusted
-    (d / "c1_0_2000.pkl").write_bytes(b"\x80\x04truncated")
+    (d / name).write_bytes(b"\x80\x04truncated")
     e = synthetic.cached_config_scene("c1", n_voxels=2000)
     assert np.array_equal(e.centers, c.centers)
