@@ -14,6 +14,12 @@ densities / SH) or --mode plain (one view per call, fp32, the reference's
 call pattern).  --impl reference times the CPU restatement of the same path
 (oracle/, all host threads) on a bounded sample of the same workload.
 
+After the timed regions, a comparator leg (batched mode, N=1) times the plain
+fp32 path and the reference backend (oracle/_ref, its own per-view calls) on
+the same GPU and cameras, and reports the batched and plain images' and
+gradients' errors against the FP64 oracle on sampled tiles (`comparators`,
+`accuracy`); --no-compare skips it.
+
 Multi-GPU (torchrun): views are sharded, each rank renders its own views of
 the shared scene; no collective in the timed data path (weak scaling).
 """
@@ -43,6 +49,8 @@ def parse():
     ap.add_argument("--views", type=int, default=None, help="use only the first N views")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg (profiling runs)")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the comparator leg (plain fp32 path, reference backend, FP64-oracle accuracy)")
     ap.add_argument("--no-tune", action="store_true",
                     help="batched mode: default launch parameters instead of the autotuner's choice")
     ap.add_argument("--tile", default=None,
@@ -220,6 +228,24 @@ def main():
     if not args.no_e2e:
         e2e = wl.e2e(args.steps, args.warmup)
         e2e["ms_total"] = workload.max_over_ranks(e2e["ms_total"], device=dev)
+    r = getattr(wl, "raster", None)
+    tile_key = f"{r.tile_size},{r.staging}" if r is not None else "16,256"
+    inst_per_view = wl.instances_per_view()
+    launches = wl.launches_per_step()
+    tuned = getattr(wl, "tuned", None)
+    r = None
+
+    # Comparator leg (rank 0, N=1; after every timing of this path): the plain
+    # fp32 per-view path on the same scene and cameras, the reference backend's
+    # own per-view call sequence on the same GPU, and image / gradient errors
+    # against the FP64 oracle on sampled tiles of view 0.
+    comparators = None
+    if rank == 0 and world == 1 and not args.no_compare and args.mode == "batched":
+        kstats_keep = kstats
+        del wl
+        torch.cuda.empty_cache()
+        comparators = comparator_leg(args, sc, dev, value)
+        kstats = kstats_keep
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -235,11 +261,9 @@ def main():
         issue = None
         tf = os.path.join(ROOT, "profiles", "render_traffic.json")
         if os.path.exists(tf) and dom["name"] in ("render_fwd", "render_bwd"):
-            r = getattr(wl, "raster", None)
-            tkey = f"{r.tile_size},{r.staging}" if r is not None else "16,256"
-            t = json.load(open(tf))["tiles"].get(tkey)
+            t = json.load(open(tf))["tiles"].get(tile_key)
             if t is not None:
-                inst = wl.instances_per_view() * (n_views if args.mode == "batched" else 1)
+                inst = inst_per_view * (n_views if args.mode == "batched" else 1)
                 traffic = round(t[dom["name"]]["dram_bytes"] / t["instances_per_launch"] * inst)
                 # the compositing kernels are bounded by instruction issue, not HBM
                 ipc = t[dom["name"]].get("ipc")
@@ -254,12 +278,13 @@ def main():
             "config": {"workload": f"{args.config}: {sc.n_voxels} voxels, {n_views} views/rank "
                                    f"{sc.cameras[0].width}x{sc.cameras[0].height}, SH3, fwd+recompute bwd",
                        "mode": args.mode, "l2": l2_note(sc, args.mode),
-                       "instances_per_view": wl.instances_per_view()},
-            "autotuned": getattr(wl, "tuned", None),
+                       "instances_per_view": inst_per_view,
+                       "scene_file": os.path.basename(scene_file(args))},
+            "autotuned": tuned,
             "render_fps": round(1000.0 / kstats["fwd_ms_per_view"], 2) if kstats.get("fwd_ms_per_view") else None,
             "rays_per_s": round(sum(c.width * c.height for c in sc.cameras) * world / (ms_total / args.steps * 1e-3),
                                 1),
-            "gpu_launches": wl.launches_per_step() * args.steps,
+            "gpu_launches": launches * args.steps,
             "timed_form": "cuda-graph replay" if args.mode == "batched" else "eager per-view calls",
             "eager_instrumented_ms_per_step": round(eager_ms, 4),
             "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": round(achieved, 2),
@@ -273,6 +298,9 @@ def main():
         if e2e is not None:
             line["e2e"] = {"value": round(e2e["ms_total"] / (args.steps * views_all), 4), "unit": "ms/view",
                            "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}
+        if comparators is not None:
+            line["comparators"] = comparators.pop("timing")
+            line["accuracy"] = comparators.pop("accuracy")
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -328,46 +356,117 @@ def run_train(args, sc, dev, world, rank):
     return 0
 
 
-def cpu_baseline(sc, budget_s=15.0):
-    """The CPU oracle (fp32 mimic, all host threads) on a bounded sample: the
-    first view's full projection + binning, then forward + backward on a run of
-    tiles in the middle of the image; reported as ms/view extrapolated by tiles."""
+def scene_file(args):
+    """Cache file the scene of this run was loaded from (or written to)."""
+    from sv_raster_b200 import synthetic
+    return synthetic.cached_scene_path(args.config, n_voxels=args.voxels)
+
+
+def _timed_steps(step, steps, warmup, dev):
+    """Device ms of `steps` calls of `step` after `warmup` untimed ones (CUDA
+    events on the current stream) and the clocks sampled meanwhile."""
+    import torch
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev.index if dev.index is not None else 0)
+    sampler.start()
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), sampler.stop()
+
+
+def comparator_leg(args, sc, dev, batched_ms_per_view):
+    """The north-star comparators on the same GPU, scene and cameras, after the
+    batched path's timing: (1) this repository's plain fp32 path in the
+    reference's per-view call pattern; (2) the reference backend itself
+    (compiled from its sources into oracle/_ref) through its own per-view
+    call sequence; (3) errors of the batched bf16-storage and plain fp32 images
+    and gradients against the FP64 oracle on a seeded sample of tiles of view
+    0.  The oracle and the reference module are used here as comparators and
+    checker only, never inside the timed path."""
+    import torch
+    from sv_raster_b200 import workload
+    n_views = len(sc.cameras)
+    timing = {}
+    wp = workload.PlainWorkload(sc, dev)
+    ms, clk = _timed_steps(wp.step, args.steps, args.warmup, dev)
+    timing["plain_fp32"] = {"ms_per_view": round(ms / (args.steps * n_views), 4), "clocks": clk,
+                            "form": "this repository's plain path, fp32, one view per call with the reference's "
+                                    "host syncs (instance count, visible-index read)"}
+    del wp
+    torch.cuda.empty_cache()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        from time_reference_gpu import ReferenceSteps
+        rs = ReferenceSteps(sc, sc.cameras, dev)
+    except (ImportError, OSError) as e:
+        timing["reference_gpu"] = {"unavailable": f"reference backend module not loadable: {e}"}
+        rs = None
+    if rs is not None:
+        ms, clk = _timed_steps(rs.step, args.steps, args.warmup, dev)
+        timing["reference_gpu"] = {"ms_per_view": round(ms / (args.steps * n_views), 4), "clocks": clk,
+                                   "form": "reference CUDA backend (backends/cuda, compiled from its sources), its "
+                                           "per-view call sequence: preprocess, visible-index sync, SH, forward "
+                                           "(instance-count sync), L2-loss gradient, backward, SH backward; fp32"}
+        del rs
+        torch.cuda.empty_cache()
+    for k in ("plain_fp32", "reference_gpu"):
+        v = timing[k].get("ms_per_view")
+        if v:
+            timing[f"batched_over_{k}"] = round(v / batched_ms_per_view, 3)
+    import accuracy
+    cam = sc.cameras[0]
+    t0 = time.perf_counter()
+    acc = accuracy.measure(sc, cam, sc.targets[0])
+    acc["view"] = f"view 0 ({cam.width}x{cam.height}), {acc['tiles']} of " \
+                  f"{((cam.width + 15) // 16) * ((cam.height + 15) // 16)} 16x16 tiles (seeded runs of 16)"
+    acc["seconds"] = round(time.perf_counter() - t0, 1)
+    return {"timing": timing, "accuracy": acc}
+
+
+def cpu_baseline(sc, budget_s=15.0, view=0, seed=0):
+    """The CPU oracle (fp32 mimic, all host threads) on a bounded sample of one
+    view: its full SH, projection and binning, then forward + backward of
+    seeded runs of 8 tiles spread over the image until the budget is spent;
+    reported as ms/view = setup + mean time per sampled tile x tile count."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    cam = sc.cameras[0]
+    cam = sc.cameras[view % len(sc.cameras)]
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     t0 = time.perf_counter()
-    idx = np.arange(sc.n_voxels)
-    rgbs = O.sh_fwd(3, idx, sc.centers, cam.position, sc.sh0, sc.shs)
     ndup, bbox, quad = O.preprocess(cam, sc.centers, sc.lengths)
+    vis = np.nonzero(ndup)[0]
+    rgbs = O.sh_fwd(3, vis, sc.centers, cam.position, sc.sh0, sc.shs)
     keys, vals, ranges = O.binning(cam, sc.octpath, ndup, bbox, quad)
     t_setup = time.perf_counter() - t0
     gx, gy = (cam.width + 15) // 16, (cam.height + 15) // 16
     T = gx * gy
-    mid = T // 2
-    n_tiles = 8
-    spent = 0.0
-    done_tiles = 0
-    while spent < budget_s and done_tiles < T:
+    run = 8
+    order = np.random.default_rng(seed + view).permutation(max(1, T // run))
+    spent, done = 0.0, 0
+    for slot in order:
+        lo, hi = int(slot) * run, min(T, int(slot) * run + run)
         t1 = time.perf_counter()
-        lo, hi = max(0, mid - n_tiles // 2), min(T, mid - n_tiles // 2 + n_tiles)
         out = O.render_fwd(cam, ranges, vals, bbox, sc.centers, sc.lengths, sc.geos, rgbs, tiles=(lo, hi))
-        dC = np.zeros_like(out["color"])
-        dC[:] = 1e-3
+        dC = np.full_like(out["color"], 1e-3)
         O.render_bwd(cam, ranges, out["tile_last"], vals, bbox, sc.centers, sc.lengths, sc.geos, rgbs,
                      out["n_contrib"], out["T"], dC, np.zeros_like(out["T"], dtype=np.float32), tiles=(lo, hi))
-        dt = time.perf_counter() - t1
-        spent += dt
-        done_tiles = hi - lo
-        per_tile = dt / max(1, hi - lo)
-        if spent + per_tile * n_tiles * 2 > budget_s:
+        spent += time.perf_counter() - t1
+        done += hi - lo
+        if spent + t_setup >= budget_s:
             break
-        n_tiles *= 2
-    ms_view = (per_tile * T + t_setup) * 1e3
+    ms_view = (spent / max(done, 1) * T + t_setup) * 1e3
     return {"value": round(ms_view, 2), "unit": "ms/view", "cores": cores, "kind": "port",
-            "sample": f"view 0: full projection+binning ({len(vals)} instances) + fwd/bwd of {done_tiles} of {T} "
-                      f"central tiles, extrapolated by tile count"}
+            "sample": f"view {view % len(sc.cameras)}: full SH + projection + binning ({len(vals)} instances, "
+                      f"{t_setup:.1f} s) + fwd/bwd of {done} of {T} 16x16 tiles in seeded runs of {run} over the "
+                      f"image ({spent:.1f} s), per-tile mean x tile count"}
 
 
 def run_reference(args):
@@ -381,7 +480,7 @@ def run_reference(args):
     per_step = min(30.0, max(5.0, 60.0 / max(1, args.steps)))
     if args.warmup > 0:
         cpu_baseline(sc, budget_s=1.0)
-    vals = [cpu_baseline(sc, budget_s=per_step) for _ in range(max(1, args.steps))]
+    vals = [cpu_baseline(sc, budget_s=per_step, view=k) for k in range(max(1, args.steps))]
     v = float(np.median([x["value"] for x in vals]))
     line = {"metric": "fwd+bwd ms/view", "value": round(v, 2), "unit": "ms/view", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
@@ -389,7 +488,8 @@ def run_reference(args):
             "config": {"workload": f"{args.config}: {sc.n_voxels} voxels, {len(sc.cameras)} views "
                                    f"{sc.cameras[0].width}x{sc.cameras[0].height}", "mode": "cpu"},
             "cpu_baseline": {"value": round(v, 2), "unit": "ms/view", "cores": vals[0]["cores"], "kind": "port",
-                             "sample": vals[0]["sample"]},
+                             "sample": f"median of {len(vals)} per-step samples, step k on view k mod "
+                                       f"{len(sc.cameras)}; step 0: {vals[0]['sample']}"},
             "e2e": {"value": round(v, 2), "unit": "ms/view", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0

@@ -38,55 +38,69 @@ def main():
     a = ap.parse_args()
     if a.ops:
         return time_ops(a.voxels)
-    import build_ref
     from sv_raster_b200 import synthetic
-    ref = build_ref.load()
     sc = synthetic.cached_config_scene(a.config, n_voxels=a.voxels)
     cams = sc.cameras[: a.views] if a.views else sc.cameras
-    dev = "cuda"
-    t = lambda x, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(x)).to(dev, dt)
-    octpath, centers, lengths = t(sc.octpath.reshape(-1, 1), torch.int64), t(sc.centers), t(sc.lengths)
-    geos, sh0, shs = t(sc.geos), t(sc.sh0), t(sc.shs)
-    mats = [(c, t(c.w2c), t(c.c2w)) for c in cams]
-    rng = np.random.default_rng(0)
-    targets = [t(rng.uniform(0, 1, (3, c.height, c.width)).astype(np.float32)) for c in cams]
-    e = torch.empty(0, device=dev)
+    rs = ReferenceSteps(sc, cams)
+    ms, inst = rs.time(a.steps, a.warmup)
+    print(json.dumps({"impl": "reference-cuda-backend", "config": a.config, "voxels": sc.n_voxels,
+                      "views": len(cams), "size": [cams[0].width, cams[0].height], "ms_per_view": round(ms, 3),
+                      "instances_per_view": inst, "dtype": "f32", "device": torch.cuda.get_device_name()}))
 
-    def view(i):
-        cam, w2c, c2w = mats[i]
+
+class ReferenceSteps:
+    """The reference backend's per-view training call sequence over a set of
+    cameras (fp32 parameters, L2 loss against seeded targets)."""
+
+    def __init__(self, sc, cams, dev="cuda"):
+        import build_ref
+        self.ref = build_ref.load()
+        t = lambda x, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(x)).to(dev, dt)
+        self.octpath, self.centers, self.lengths = (t(sc.octpath.reshape(-1, 1), torch.int64), t(sc.centers),
+                                                    t(sc.lengths))
+        self.geos, self.sh0, self.shs = t(sc.geos), t(sc.sh0), t(sc.shs)
+        self.mats = [(c, t(c.w2c), t(c.c2w)) for c in cams]
+        rng = np.random.default_rng(0)
+        self.targets = [t(rng.uniform(0, 1, (3, c.height, c.width)).astype(np.float32)) for c in cams]
+        self.e = torch.empty(0, device=dev)
+
+    def view(self, i):
+        ref, e = self.ref, self.e
+        cam, w2c, c2w = self.mats[i]
         W, H = cam.width, cam.height
         ndup, geom = ref.rasterize_preprocess(W, H, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w, cam.near,
-                                              octpath, centers, lengths, False)
+                                              self.octpath, self.centers, self.lengths, False)
         vis = torch.where(ndup > 0)[0]
         pos = c2w[:3, 3].contiguous()
-        rgbs = ref.sh_compute(3, vis, centers, pos, sh0, shs)
+        rgbs = ref.sh_compute(3, vis, self.centers, pos, self.sh0, self.shs)
         out = ref.rasterize_voxels(1, W, H, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w, 0.0, False, False,
-                                   False, False, octpath, centers, lengths, geos, rgbs, geom, False)
+                                   False, False, self.octpath, self.centers, self.lengths, self.geos, rgbs, geom, False)
         color, T = out[3], out[6]
-        dC = (2.0 / color.numel()) * (color - targets[i])
+        dC = (2.0 / color.numel()) * (color - self.targets[i])
         g = ref.rasterize_voxels_backward(out[0], 1, W, H, cam.tanfovx, cam.tanfovy, cam.cx, cam.cy, w2c, c2w, 0.0,
-                                          octpath, centers, lengths, geos, rgbs, geom, out[1], out[2], T, dC, e, e,
-                                          torch.zeros_like(T), 0.0, e, 0.0, 0.0, False, False, out[4], out[5], False)
-        ref.sh_compute_bw(3, 16, vis, centers, pos, rgbs, g[1])
+                                          self.octpath, self.centers, self.lengths, self.geos, rgbs, geom, out[1],
+                                          out[2], T, dC, e, e, torch.zeros_like(T), 0.0, e, 0.0, 0.0, False, False,
+                                          out[4], out[5], False)
+        ref.sh_compute_bw(3, 16, vis, self.centers, pos, rgbs, g[1])
         return out[0]
 
-    for _ in range(a.warmup):
-        for i in range(len(mats)):
-            view(i)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    inst = 0
-    for _ in range(a.steps):
-        for i in range(len(mats)):
-            inst += view(i)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / (a.steps * len(mats))
-    print(json.dumps({"impl": "reference-cuda-backend", "config": a.config, "voxels": sc.n_voxels,
-                      "views": len(mats), "size": [cams[0].width, cams[0].height], "ms_per_view": round(ms, 3),
-                      "instances_per_view": inst // (a.steps * len(mats)), "dtype": "f32",
-                      "device": torch.cuda.get_device_name()}))
+    def step(self):
+        return sum(self.view(i) for i in range(len(self.mats)))
+
+    def time(self, steps, warmup):
+        """(device ms per view over `steps` steps after `warmup`, instances per view)."""
+        for _ in range(warmup):
+            self.step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        inst = 0
+        for _ in range(steps):
+            inst += self.step()
+        e1.record()
+        torch.cuda.synchronize()
+        n = steps * len(self.mats)
+        return e0.elapsed_time(e1) / n, inst // n
 
 
 def time_ops(n_voxels, reps=10, warmup=3):

@@ -251,3 +251,33 @@ def test_binning_is_a_stable_key_sort(c1):
     # multi-quadrant voxels appear once per (quadrant, tile)
     vid = vals & 0x1FFFFFFF
     assert np.array_equal(np.bincount(vid, minlength=c1.n_voxels), ndup)
+
+
+def test_sampled_tile_oracle_equals_whole_view():
+    """The FP64 accuracy oracle on a seeded sample of tile runs reproduces the
+    whole-view FP64 oracle on those tiles (image, T), and its backward equals
+    the whole-view backward of the masked upstream gradient."""
+    import accuracy
+    sc = synthetic.config_scene("c1", n_voxels=4000)
+    cam = sc.cameras[1]
+    runs = accuracy.tile_runs(cam, n_runs=6, run_len=4, seed=3)
+    assert len(runs) == 6 and all(hi - lo == 4 for lo, hi in runs)
+    assert all(b[0] >= a[1] for a, b in zip(runs, runs[1:]))  # disjoint, sorted
+    orc = accuracy.OracleView(sc, cam, runs)
+    m = orc.mask
+    assert m.sum() == 6 * 4 * 256
+    rgbs = O.sh_fwd(3, orc.vis, sc.centers, cam.position, sc.sh0, sc.shs, mode="f64")
+    full = O.render_view(cam, sc.octpath, sc.centers, sc.lengths, sc.geos, rgbs, mode="f64")
+    assert np.array_equal(orc.color[:, m], full["color"][:, m])
+    assert np.array_equal(orc.T[m], full["T"][m])
+    dC = np.random.default_rng(4).standard_normal((3, cam.height, cam.width)).astype(np.float32) * 1e-3
+    dgeo, dsh0, dshs = orc.backward(dC)
+    dCm = np.where(m[None], dC, 0).astype(np.float32)
+    g = O.render_bwd(cam, full["ranges"], full["tile_last"], full["vals"], full["bbox"], sc.centers, sc.lengths,
+                     sc.geos, rgbs, full["n_contrib"], full["T"], dCm, np.zeros((cam.height, cam.width), np.float32),
+                     mode="f64")
+    assert np.allclose(dgeo, g["dL_dgeos"], rtol=1e-12, atol=1e-18)
+    d0, _ = O.sh_bwd(3, 16, orc.vis, sc.centers, cam.position, g["dL_drgbs"], mode="f64")
+    assert np.allclose(dsh0, d0, rtol=1e-12, atol=1e-18)
+    rep = accuracy.report(orc, np.zeros((3, cam.height, cam.width), np.float32), {"same": full["color"]}, {}, dC)
+    assert rep["same"]["image_max_abs_err"] == 0.0 and rep["same"]["psnr_delta_db"] == 0.0
