@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--train", action="store_true",
                     help="training-step workload (fwd + bwd + fused Adam, graph-captured) vs the plain fp32 form")
     ap.add_argument("--plain-steps", type=int, default=10, help="steps of the plain form in --train mode")
+    ap.add_argument("--grid", action="store_true",
+                    help="--train: densities as grid points (vox_key [P,8] into a deduplicated corner grid), the "
+                         "reference's training parametrisation")
     return ap.parse_args()
 
 
@@ -143,9 +146,9 @@ def scene_for(args, rank, world):
     sc = synthetic.cached_config_scene(args.config, n_voxels=args.voxels)
     from sv_raster_b200.workload import rank_cameras
     cams = sc.cameras[: args.views] if args.views else sc.cameras
-    sc.cameras = rank_cameras(cams, rank, world)  # weak scaling: each rank its own views
+    sc.cameras = rank_cameras(cams, rank, world, config=args.config)  # weak scaling: each rank its own views
     trng = np.random.default_rng(1234 + rank)
-    sc.targets = [trng.uniform(0, 1, size=(3, c.height, c.width)).astype(np.float32) for c in cams]
+    sc.targets = [trng.uniform(0, 1, size=(3, c.height, c.width)).astype(np.float32) for c in sc.cameras]
     return sc
 
 
@@ -318,19 +321,24 @@ def run_train(args, sc, dev, world, rank):
     torch.zeros(1, device=dev)
     torch.cuda.reset_peak_memory_stats()
     exchange = workload.GradientExchange() if world > 1 else None
-    wl = workload.BatchedTrainWorkload(sc, dev, exchange=exchange)
+    grid = None
+    if args.grid:
+        from sv_raster_b200 import synthetic
+        grid = synthetic.grid_params(sc, dev)
+    wl = workload.BatchedTrainWorkload(sc, dev, exchange=exchange, grid=grid)
     wl.capture()
     peak_setup = torch.cuda.max_memory_allocated()  # includes the autotuner's trial plans
     torch.cuda.reset_peak_memory_stats()
     ms_b, loss_b = wl.run(args.steps)
     ms_b = workload.max_over_ranks(ms_b, device=dev)
     peak_b = torch.cuda.max_memory_allocated()
+    wl.release()
     del wl
     torch.cuda.empty_cache()
     ms_p = loss_p = peak_p = dev_rel = None
     if world == 1:  # the plain per-view form is the single-GPU comparator
         torch.cuda.reset_peak_memory_stats()
-        wp = workload.PlainTrainWorkload(sc, dev)
+        wp = workload.PlainTrainWorkload(sc, dev, grid=grid)
         ms_p, loss_p = wp.run(args.plain_steps)
         peak_p = torch.cuda.max_memory_allocated()
         n = min(len(loss_b), len(loss_p))
@@ -341,7 +349,9 @@ def run_train(args, sc, dev, world, rank):
             "n_gpus": world, "steps": args.steps, "data": "synthetic", "dtype": "f32", "storage_dtype": "bf16",
             "config": {"workload": f"{args.config}: {sc.n_voxels} voxels, {len(sc.cameras)} views per step "
                                    f"({sc.cameras[0].width}x{sc.cameras[0].height} ... mixed), fwd + recompute bwd "
-                                   f"+ fused Adam, one CUDA graph per step"},
+                                   f"+ fused Adam, one CUDA graph per step",
+                       "densities": (f"{grid[1].shape[0]} grid points gathered per step (vox_key [P,8])"
+                                     if grid is not None else "per-voxel corners [P,8]")},
             "scaling": "weak",
             "exchange": "sum all-reduce of the flat gradient buffer per step (NCCL)" if world > 1 else None,
             "plain_fp32": None if ms_p is None else {"ms_per_step": round(ms_p, 3), "steps": args.plain_steps,

@@ -189,6 +189,16 @@ int svr_gather_grid_params(int dim, int64_t n_care, const int64_t* vox_key, cons
                            const float* grid_pts, float* out, void* stream);
 int svr_gather_grid_params_bw(int dim, int64_t n_care, const int64_t* vox_key, const int64_t* care_idx,
                               const float* dL_dvox, float* dL_dgrid, void* stream);
+/* The grid-point gather of every voxel (GatherGeoParams with all voxels
+ * cared for, renderer.py:319-345, geo_params_gather.cu:22-46): geos_out[p,c] =
+ * grid_pts[vox_key[p,c]], grid and output each fp32 or bf16 -- the density
+ * input of the batched step when training grid points.  vox_key int64 [P,8]. */
+int svr_gather_grid_geo_all(int64_t P, const int64_t* vox_key, const void* grid_pts, int grid_bf16, void* geos_out,
+                            int out_bf16, void* stream);
+/* Its backward (geo_params_gather.cu:48-72 for all voxels): adds dL_dgeos
+ * [P,8] fp32 into dL_dgrid [M] fp32 at vox_key. */
+int svr_scatter_grid_geo_all(int64_t P, const int64_t* vox_key, const float* dL_dgeos, float* dL_dgrid,
+                             void* stream);
 
 /* Replaces TV_COMPUTE::total_variation_bw (tv_compute.cu:84-110): adds the
  * total-variation gradient of grid_pts [M,C] over the N voxels' 8 corners
@@ -257,6 +267,16 @@ int svr_batch_plan_tile_size(const svr_batch_plan* plan);
  * added to its shared accumulator with atomics, from more lanes through a
  * 13-shuffle reduce-scatter.  Only the order of additions changes. */
 int svr_batch_plan_set_reduction(svr_batch_plan* plan, int atomic_lanes);
+/* Arithmetic of the compositing loops of svr_batch_render / svr_batch_backward.
+ * exact = 1: the reference's operations (forward.cu:243-253, backward.cu:309-333:
+ * libdevice expf, IEEE division); images, T and contributor counts are
+ * bit-identical to svr_rasterize_render's.  exact = 0 (default): the hardware
+ * exponential and an approximate division (a few ulp each) for the
+ * per-(pixel, voxel) exponentials and the transmittance recovery -- fewer
+ * instructions in both loops; images and gradients then agree with the exact
+ * form to fp32 accumulation error (a pixel may stop one voxel earlier or later
+ * where its transmittance lands on the 1e-4 early-stop threshold). */
+int svr_batch_plan_set_arithmetic(svr_batch_plan* plan, int exact);
 int64_t svr_batch_plan_pixels(const svr_batch_plan* plan);
 int64_t svr_batch_plan_tiles(const svr_batch_plan* plan);
 int svr_batch_plan_groups(const svr_batch_plan* plan);
@@ -265,8 +285,9 @@ uint32_t* svr_batch_error_ptr(const svr_batch_plan* plan, void* workspace);
 /* Packed pixel bbox of every (view, voxel) pair [V,P] (uint2 as uint64:
  * .x = xmin << 16 | ymin, .y = xmax << 16 | ymax), valid after prepare. */
 const uint64_t* svr_batch_bbox_ptr(const svr_batch_plan* plan, const void* workspace);
-/* Device arrays inside a workspace: rgbs / dL_drgbs [V,P,3], ranges [T] (uint2
- * as uint64), tile_last [T], n_contrib [pixels], n_dup [V,P], sorted values. */
+/* Device arrays inside a workspace: rgbs [V,P,3], drgbs [V,P,4] (dL/drgb in
+ * xyz, the subdivision priority in w), ranges [T] (uint2 as uint64),
+ * tile_last [T], n_contrib [pixels], n_dup [V,P], sorted values. */
 int svr_batch_arrays(const svr_batch_plan* plan, const void* workspace, const float** rgbs, const float** drgbs,
                      const uint64_t** ranges, const uint32_t** tile_last, const uint32_t** n_contrib,
                      const uint32_t** n_dup, const uint32_t** sorted_vals);
@@ -280,15 +301,18 @@ int svr_batch_prepare(svr_batch_plan* plan, void* workspace, const int64_t* octr
  * last svr_batch_prepare on this workspace (call prepare first). */
 int svr_batch_render(svr_batch_plan* plan, void* workspace, const float* vox_centers, const float* vox_lengths,
                      const void* geos, int geos_bf16, float* out_color, float* out_T, void* stream);
-/* Recompute-backward of every (view, tile) in one persistent launch: dL_dgeos [P,8] and
- * subdiv [P] summed over views (caller-zeroed); per-view dL/drgb kept in the
- * workspace for svr_batch_sh_backward. */
+/* Recompute-backward of every (view, tile) in one persistent launch:
+ * dL_dgeos [P,8] summed over views (caller-zeroed, 16-byte aligned rows: it
+ * is accumulated with vector reductions); per-view dL/drgb and subdivision
+ * priority kept in the workspace for svr_batch_sh_backward. */
 int svr_batch_backward(svr_batch_plan* plan, void* workspace, const float* vox_centers, const float* vox_lengths,
                        const void* geos, int geos_bf16, const float* out_T, const float* dL_dcolor,
-                       const float* dL_dT, float* dL_dgeos, float* subdiv, void* stream);
-/* dL/dsh0 [P,3] and dL/dshs [P,M-1,3] summed over views (overwritten). */
+                       const float* dL_dT, float* dL_dgeos, void* stream);
+/* dL/dsh0 [P,3] and dL/dshs [P,M-1,3] summed over views (overwritten), and,
+ * when subdiv is not null, the subdivision priority subdiv_p_bw [P] summed
+ * over views (overwritten; backward.cu:514 per view). */
 int svr_batch_sh_backward(svr_batch_plan* plan, void* workspace, const float* vox_centers, int sh_degree, int M,
-                          float* dL_dsh0, float* dL_dshs, void* stream);
+                          float* dL_dsh0, float* dL_dshs, float* subdiv, void* stream);
 
 #ifdef __cplusplus
 }

@@ -72,6 +72,8 @@ _SIGS = {
                                            ctypes.POINTER(c_i64), ctypes.POINTER(c_d), c_d, c_d, c_f, c_p, c_p]),
     "svr_gather_grid_params": (c_int, [c_int, c_i64, c_p, c_p, c_p, c_p, c_p]),
     "svr_gather_grid_params_bw": (c_int, [c_int, c_i64, c_p, c_p, c_p, c_p, c_p]),
+    "svr_gather_grid_geo_all": (c_int, [c_i64, c_p, c_p, c_int, c_p, c_int, c_p]),
+    "svr_scatter_grid_geo_all": (c_int, [c_i64, c_p, c_p, c_p, c_p]),
     "svr_read_error": (c_int, [c_p, ctypes.POINTER(ctypes.c_uint32), c_p]),
     "svr_total_variation_bw": (c_int, [c_p, c_p, c_f, c_p, c_int, c_int, c_i64, c_int, c_p, c_p, c_p]),
     "svr_batch_plan_create": (c_int, [c_int, ctypes.POINTER(Camera), c_i64, c_i64, c_int, c_int, c_int,
@@ -83,6 +85,7 @@ _SIGS = {
     "svr_batch_plan_set_staging": (c_int, [c_p, c_int]),
     "svr_batch_plan_tile_size": (c_int, [c_p]),
     "svr_batch_plan_set_reduction": (c_int, [c_p, c_int]),
+    "svr_batch_plan_set_arithmetic": (c_int, [c_p, c_int]),
     "svr_batch_plan_set_binning": (c_int, [c_p, c_int]),
     "svr_batch_plan_pixels": (c_i64, [c_p]),
     "svr_batch_plan_tiles": (c_i64, [c_p]),
@@ -93,8 +96,8 @@ _SIGS = {
     "svr_batch_arrays": (c_int, [c_p, c_p] + [ctypes.POINTER(c_p)] * 7),
     "svr_batch_prepare": (c_int, [c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_int, c_int, c_int, c_p]),
     "svr_batch_render": (c_int, [c_p, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_p]),
-    "svr_batch_backward": (c_int, [c_p, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_p, c_p, c_p, c_p]),
-    "svr_batch_sh_backward": (c_int, [c_p, c_p, c_p, c_int, c_int, c_p, c_p, c_p]),
+    "svr_batch_backward": (c_int, [c_p, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_p, c_p, c_p]),
+    "svr_batch_sh_backward": (c_int, [c_p, c_p, c_p, c_int, c_int, c_p, c_p, c_p, c_p]),
 }
 
 _lib = None

@@ -25,10 +25,11 @@ class BatchedRasterizer:
     those matrices are baked into the plan; update them in place to move the
     cameras (e.g. between CUDA-graph replays).  ``max_level`` bounds the
     voxels' octree levels (shorter sort keys; checked on the device).
+    ``exact`` selects the compositing arithmetic (see set_arithmetic).
     """
 
     def __init__(self, cameras, octree_paths, vox_centers, vox_lengths, max_level=16, n_samp_per_vox=1,
-                 bg_color=0.0, capacity=None, headroom=1.25, tile_size=16):
+                 bg_color=0.0, capacity=None, headroom=1.25, tile_size=16, exact=False):
         self.dev = vox_centers.device
         self.cams = list(cameras)
         self.octree_paths = octree_paths.reshape(-1).contiguous()
@@ -56,6 +57,7 @@ class BatchedRasterizer:
         self.sort_buckets = (512, 4096)
         self.atomic_lanes = 1
         self.binning = 1
+        self.exact = bool(exact)
         self._make_plan(0 if capacity is None else int(capacity))
         self.capacity_auto = capacity is None
 
@@ -80,6 +82,7 @@ class BatchedRasterizer:
         check(L.svr_batch_plan_set_staging(plan, self.staging), "batch_plan_set_staging")
         check(L.svr_batch_plan_set_reduction(plan, self.atomic_lanes), "batch_plan_set_reduction")
         check(L.svr_batch_plan_set_binning(plan, self.binning), "batch_plan_set_binning")
+        check(L.svr_batch_plan_set_arithmetic(plan, int(self.exact)), "batch_plan_set_arithmetic")
 
     def set_binning(self, binning=1):
         """How prepare groups the instances by tile before the per-tile sort:
@@ -94,6 +97,14 @@ class BatchedRasterizer:
         reduce-scatter (only the order of additions changes)."""
         check(lib().svr_batch_plan_set_reduction(self.plan, int(atomic_lanes)), "batch_plan_set_reduction")
         self.atomic_lanes = int(atomic_lanes)
+
+    def set_arithmetic(self, exact=False):
+        """Compositing arithmetic: ``exact`` reproduces the plain path (and the
+        reference) bit for bit; the default fast form uses the hardware
+        exponential and an approximate division in the per-(pixel, voxel)
+        loops (see svr_batch_plan_set_arithmetic)."""
+        check(lib().svr_batch_plan_set_arithmetic(self.plan, int(bool(exact))), "batch_plan_set_arithmetic")
+        self.exact = bool(exact)
 
     def set_tile_size(self, tile_size, staging=None):
         """Compositing tile size (8, 16 or 32 pixels) and records staged per
@@ -181,22 +192,30 @@ class BatchedRasterizer:
     def backward(self, geos, out_T, dL_dcolor, dL_dT, sh_degree, M, grads=None):
         """Returns (dL_dgeos [P,8], subdiv [P], dL_dsh0 [P,3], dL_dshs [P,M-1,3]) fp32."""
         if grads is None:
-            # dL_dgeos and subdiv accumulate; the SH gradients are overwritten
-            grads = (torch.zeros(self.P, 8, device=self.dev), torch.zeros(self.P, device=self.dev),
+            # dL_dgeos accumulates; subdiv and the SH gradients are overwritten
+            grads = (torch.zeros(self.P, 8, device=self.dev), torch.empty(self.P, device=self.dev),
                      torch.empty(self.P, 3, device=self.dev), torch.empty(self.P, M - 1, 3, device=self.dev))
         else:
             grads[0].zero_()
-            grads[1].zero_()
-        dgeo, sub, dsh0, dshs = grads
-        L = lib()
-        check(L.svr_batch_backward(self.plan, self._p(self.ws), self._p(self.centers), self._p(self.lengths),
-                                   self._p(geos), int(geos.dtype == torch.bfloat16), self._p(out_T),
-                                   self._p(dL_dcolor), self._p(dL_dT), self._p(dgeo), self._p(sub), self._stream()),
-              "batch_backward")
-        check(L.svr_batch_sh_backward(self.plan, self._p(self.ws), self._p(self.centers), int(sh_degree), int(M),
-                                      self._p(dsh0), self._p(dshs) if dshs.numel() else None, self._stream()),
-              "batch_sh_backward")
+        self.backward_render(geos, out_T, dL_dcolor, dL_dT, grads[0])
+        self.backward_sh(sh_degree, M, grads[2], grads[3], grads[1])
         return grads
+
+    def backward_render(self, geos, out_T, dL_dcolor, dL_dT, dL_dgeos):
+        """The compositing backward alone: adds every view's density gradient
+        into dL_dgeos [P,8] (16-byte aligned) and keeps the per-view colour
+        gradients in the workspace for backward_sh."""
+        check(lib().svr_batch_backward(self.plan, self._p(self.ws), self._p(self.centers), self._p(self.lengths),
+                                       self._p(geos), int(geos.dtype == torch.bfloat16), self._p(out_T),
+                                       self._p(dL_dcolor), self._p(dL_dT), self._p(dL_dgeos), self._stream()),
+              "batch_backward")
+
+    def backward_sh(self, sh_degree, M, dL_dsh0, dL_dshs, subdiv=None):
+        """SH gradients (and the subdivision priority) summed over views, from
+        the colour gradients of the last backward_render (overwritten)."""
+        check(lib().svr_batch_sh_backward(self.plan, self._p(self.ws), self._p(self.centers), int(sh_degree), int(M),
+                                          self._p(dL_dsh0), self._p(dL_dshs) if dL_dshs.numel() else None,
+                                          self._p(subdiv), self._stream()), "batch_sh_backward")
 
     # -- views of the flat outputs ---------------------------------------------
     def split_color(self, flat):
@@ -219,7 +238,7 @@ class BatchedRasterizer:
         return dict(
             bbox=ws[ob:ob + 8 * VP].view(torch.int32).view(len(self.cams), self.P, 2),
             rgbs=ws[off[0]:off[0] + 12 * VP].view(torch.float32).view(len(self.cams), self.P, 3),
-            drgbs=ws[off[1]:off[1] + 12 * VP].view(torch.float32).view(len(self.cams), self.P, 3),
+            drgbs=ws[off[1]:off[1] + 16 * VP].view(torch.float32).view(len(self.cams), self.P, 4),
             ranges=ws[off[2]:off[2] + 8 * self.n_tiles].view(torch.int32).view(self.n_tiles, 2),
             tile_last=ws[off[3]:off[3] + 4 * self.n_tiles].view(torch.int32),
             n_contrib=ws[off[4]:off[4] + 4 * self.n_pixels].view(torch.int32),
@@ -250,3 +269,56 @@ class BatchedRender(torch.autograd.Function):
             dL_dT = torch.zeros_like(T)
         dgeo, _sub, dsh0, dshs = r.backward(geos, T, dL_dcolor.contiguous(), dL_dT.contiguous(), ctx.sh_degree, ctx.M)
         return None, None, dgeo.to(geos.dtype), dsh0.to(ctx.sh_dtype), dshs.to(ctx.sh_dtype)
+
+
+def gather_grid_geos(vox_key, grid_pts, out):
+    """out[p, c] = grid_pts[vox_key[p, c]] for every voxel (GatherGeoParams
+    with all voxels cared for; grid and out fp32 or bf16)."""
+    P = vox_key.shape[0]
+    check(lib().svr_gather_grid_geo_all(P, ctypes.c_void_p(vox_key.data_ptr()), ctypes.c_void_p(grid_pts.data_ptr()),
+                                        int(grid_pts.dtype == torch.bfloat16), ctypes.c_void_p(out.data_ptr()),
+                                        int(out.dtype == torch.bfloat16),
+                                        ctypes.c_void_p(torch.cuda.current_stream(out.device).cuda_stream)),
+          "gather_grid_geo_all")
+    return out
+
+
+def scatter_grid_grad(vox_key, dL_dgeos, dL_dgrid):
+    """dL_dgrid[vox_key[p, c]] += dL_dgeos[p, c] (fp32) for every voxel."""
+    P = vox_key.shape[0]
+    check(lib().svr_scatter_grid_geo_all(P, ctypes.c_void_p(vox_key.data_ptr()), ctypes.c_void_p(dL_dgeos.data_ptr()),
+                                         ctypes.c_void_p(dL_dgrid.data_ptr()),
+                                         ctypes.c_void_p(torch.cuda.current_stream(dL_dgrid.device).cuda_stream)),
+          "scatter_grid_geo_all")
+    return dL_dgrid
+
+
+class GridBatchedRender(torch.autograd.Function):
+    """Autograd wrapper over grid-point densities, the reference's training
+    parametrisation (GatherGeoParams then rasterize, renderer.py:319-345):
+    (grid_pts [M], sh0, shs) -> (color flat, T flat) over all views.  The
+    corner densities are gathered once per step for all views into a [P,8]
+    buffer of the grid's dtype, and the density gradients are added back into
+    the grid gradient once per step."""
+
+    @staticmethod
+    def forward(ctx, raster, sh_degree, vox_key, grid_pts, sh0, shs):
+        geos = torch.empty(vox_key.shape[0], 8, dtype=grid_pts.dtype, device=grid_pts.device)
+        gather_grid_geos(vox_key, grid_pts, geos)
+        raster.prepare(sh0, shs, sh_degree)
+        color, T = raster.render(geos)
+        ctx.raster, ctx.sh_degree, ctx.M = raster, sh_degree, 1 + shs.shape[1]
+        ctx.sh_dtype, ctx.grid_dtype, ctx.M_grid = sh0.dtype, grid_pts.dtype, grid_pts.shape[0]
+        ctx.save_for_backward(vox_key, geos, T)
+        return color, T
+
+    @staticmethod
+    def backward(ctx, dL_dcolor, dL_dT):
+        vox_key, geos, T = ctx.saved_tensors
+        r = ctx.raster
+        if dL_dT is None:
+            dL_dT = torch.zeros_like(T)
+        dgeo, _sub, dsh0, dshs = r.backward(geos, T, dL_dcolor.contiguous(), dL_dT.contiguous(), ctx.sh_degree, ctx.M)
+        dgrid = torch.zeros(ctx.M_grid, dtype=torch.float32, device=dgeo.device)
+        scatter_grid_grad(vox_key, dgeo, dgrid)
+        return None, None, None, dgrid.to(ctx.grid_dtype), dsh0.to(ctx.sh_dtype), dshs.to(ctx.sh_dtype)

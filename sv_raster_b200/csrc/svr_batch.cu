@@ -277,8 +277,9 @@ __global__ void rank_pos_scatter_kernel(size_t n, const uint32_t* __restrict__ s
 }
 
 // dL/dSH of every voxel summed over views: sum_v basis(dir_v) * dL/drgb_v
-// (sh_compute.cu:110-176 per view).  Views where the voxel got no gradient
-// are skipped.  Each CTA stages its voxels' 3 + 3*(M-1) outputs in shared
+// (sh_compute.cu:110-176 per view), and the subdivision priority summed over
+// views (backward.cu:514).  Views where the voxel got no colour gradient are
+// skipped.  Each CTA stages its voxels' 3 + 3*(M-1) outputs in shared
 // memory and stores them as contiguous rows (the per-voxel rows of dsh0 and
 // dshs are 12 B and 180 B long, too short for coalesced per-thread stores).
 constexpr int kShBwThreads = 128;
@@ -286,7 +287,8 @@ constexpr int kShBwThreads = 128;
 template <int DEG>
 __global__ void __launch_bounds__(kShBwThreads)
 sh_bw_batch_kernel(const __grid_constant__ ViewTable views, int P, int M, const float* __restrict__ centers,
-                   const float* __restrict__ drgbs, float* __restrict__ dsh0, float* __restrict__ dshs) {
+                   const float4* __restrict__ drgbs, float* __restrict__ dsh0, float* __restrict__ dshs,
+                   float* __restrict__ subdiv) {
   constexpr int NB = (DEG + 1) * (DEG + 1) - 1;
   __shared__ float s_pos[kMaxViews][3];
   extern __shared__ __align__(16) float s_out[];  // [kShBwThreads][3 + 3 * (M - 1)] then written out
@@ -300,14 +302,16 @@ sh_bw_batch_kernel(const __grid_constant__ ViewTable views, int P, int M, const 
   const int i0 = blockIdx.x * kShBwThreads;
   const int i = i0 + threadIdx.x;
   float a0[3] = {0.f, 0.f, 0.f};
+  float sub = 0.f;
   float acc[NB > 0 ? NB : 1][3];
 #pragma unroll
   for (int k = 0; k < (NB > 0 ? NB : 1); ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.f;
   if (i < P) {
     const float cx = centers[3 * (size_t)i], cy = centers[3 * (size_t)i + 1], cz = centers[3 * (size_t)i + 2];
     for (int v = 0; v < views.n; ++v) {
-      const float* g = drgbs + 3 * ((size_t)v * P + i);
-      const float g0 = g[0], g1 = g[1], g2 = g[2];
+      const float4 g = drgbs[(size_t)v * P + i];
+      const float g0 = g.x, g1 = g.y, g2 = g.z;
+      sub += g.w;
       if (g0 == 0.f && g1 == 0.f && g2 == 0.f) continue;
       float x = cx - s_pos[v][0], y = cy - s_pos[v][1], z = cz - s_pos[v][2];
       const float rn = rnorm3df(x, y, z);
@@ -323,6 +327,7 @@ sh_bw_batch_kernel(const __grid_constant__ ViewTable views, int P, int M, const 
       }
     }
   }
+  if (subdiv && i < P) subdiv[i] = sub;
   // stage: dsh0 rows first ([kShBwThreads][3]), then dshs rows ([kShBwThreads][rest])
   float* s0 = s_out;
   float* s1 = s_out + 3 * kShBwThreads;
@@ -379,6 +384,7 @@ struct svr_batch_plan {
   int tile_size;               // compositing tile size (8, 16 or 32), fixed at creation
   int stage;                   // records staged per round (svr_batch_plan_set_staging)
   int atomic_lanes;            // backward reduction threshold (svr_batch_plan_set_reduction)
+  int exact;                   // compositing arithmetic (svr_batch_plan_set_arithmetic): 1 exact, 0 fast
   int binning;                 // 1: counting sort by tile, 0: radix over the tile bits (svr_batch_plan_set_binning)
   // workspace layout (byte offsets)
   size_t o_header, o_ndup, o_scan, o_bbox, o_quad, o_scan_tmp, o_rgbs, o_drgbs;
@@ -560,7 +566,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->o_quad = take(VP * 4);
   p->o_scan_tmp = take(scan_temp_bytes(std::max(VP, (size_t)tiles)));  // instance scan, then the tile-count scan
   p->o_rgbs = take(VP * 12);
-  p->o_drgbs = take(VP * 12);
+  p->o_drgbs = take(VP * 16);  // [V,P,4]: dL/drgb (xyz) and the subdivision priority (w)
   // the instance arrays also serve the one-time sort of the 8P rank keys
   const size_t kv = std::max(p->cap, (size_t)(8 * P));
   p->o_ka = take(kv * 8);
@@ -584,6 +590,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->seg_small_n = 512;
   p->seg_chunk = 4096;
   p->atomic_lanes = 1;
+  p->exact = 0;
   p->binning = 1;
   ensure_segsort_attributes();
   ensure_fwd_batch_attributes();
@@ -618,6 +625,12 @@ int svr_batch_plan_set_staging(svr_batch_plan* p, int stage) {
 }
 
 int svr_batch_plan_tile_size(const svr_batch_plan* p) { return p ? p->tile_size : 0; }
+
+int svr_batch_plan_set_arithmetic(svr_batch_plan* p, int exact) {
+  if (!p || (exact != 0 && exact != 1)) return SVR_ERR_SHAPE;
+  p->exact = exact;
+  return SVR_OK;
+}
 
 int svr_batch_plan_set_reduction(svr_batch_plan* p, int atomic_lanes) {
   if (!p || atomic_lanes < 1 || atomic_lanes > 32) return SVR_ERR_SHAPE;
@@ -775,35 +788,37 @@ int svr_batch_render(svr_batch_plan* p, void* ws, const float* vox_centers, cons
   const bool ordered = (p->order_flags & 1) != 0;
   if (ordered) build_tile_order(p, q, nullptr, q.order_fwd, stream);
   launch_render_fwd_batch(p->vt, (int)p->total_tiles, q.ranges, p->cap > 0 ? q.vb : nullptr, va, (int)p->P,
-                          (size_t)p->P * 3, out, p->n_samp, p->tile_size, p->stage,
+                          (size_t)p->P * 3, out, p->n_samp, p->tile_size, p->stage, !p->exact,
                           ordered ? q.order_fwd : nullptr, q.header + 2, p->fwd_ctas_per_sm, stream);
   return check_last();
 }
 
 int svr_batch_backward(svr_batch_plan* p, void* ws, const float* vox_centers, const float* vox_lengths,
                        const void* geos, int geos_bf16, const float* out_T, const float* dL_dcolor,
-                       const float* dL_dT, float* dL_dgeos, float* subdiv, void* stream_) {
+                       const float* dL_dT, float* dL_dgeos, void* stream_) {
   cudaStream_t stream = static_cast<cudaStream_t>(stream_);
-  if (!p || !ws || !vox_centers || !vox_lengths || !geos || !out_T || !dL_dcolor || !dL_dT || !dL_dgeos || !subdiv)
+  if (!p || !ws || !vox_centers || !vox_lengths || !geos || !out_T || !dL_dcolor || !dL_dT || !dL_dgeos)
     return SVR_ERR_SHAPE;
-  if ((reinterpret_cast<uintptr_t>(geos) & 15u) != 0) return SVR_ERR_ALIGN;
+  if ((reinterpret_cast<uintptr_t>(geos) & 15u) != 0 || (reinterpret_cast<uintptr_t>(dL_dgeos) & 15u) != 0)
+    return SVR_ERR_ALIGN;
   BatchPtrs q = ptrs(p, ws);
-  cudaMemsetAsync(q.drgbs, 0, (size_t)p->V * p->P * 12, stream);
+  cudaMemsetAsync(q.drgbs, 0, (size_t)p->V * p->P * 16, stream);
   VoxelArrays va{q.bbox, vox_centers, vox_lengths, geos_bf16 ? nullptr : (const float*)geos,
                  geos_bf16 ? (const __nv_bfloat16*)geos : nullptr, q.rgbs};
   BwdTileIn in{out_T, q.ncontrib, dL_dcolor, nullptr, nullptr, dL_dT, nullptr, nullptr, 0.f, 0.f, 0.f,
                p->atomic_lanes};
-  BwdTileOut out{dL_dgeos, q.drgbs, subdiv, q.header + 1};
+  BwdTileOut out{dL_dgeos, q.drgbs, nullptr, q.header + 1, 1};
   const bool ordered = (p->order_flags & 2) != 0;
   if (ordered) build_tile_order(p, q, q.tile_last, q.order_bwd, stream);
   launch_render_bwd_batch(p->vt, (int)p->total_tiles, q.ranges, q.tile_last, p->cap > 0 ? q.vb : nullptr, va,
-                          (int)p->P, (size_t)p->P * 3, in, out, p->n_samp, p->tile_size, p->stage,
-                          ordered ? q.order_bwd : nullptr, q.header + 3, p->bwd_ctas_per_sm, stream);
+                          (int)p->P, (size_t)p->P * 3, (size_t)p->P * 4, in, out, p->n_samp, p->tile_size,
+                          p->stage, !p->exact, ordered ? q.order_bwd : nullptr, q.header + 3, p->bwd_ctas_per_sm,
+                          stream);
   return check_last();
 }
 
 int svr_batch_sh_backward(svr_batch_plan* p, void* ws, const float* vox_centers, int sh_degree, int M,
-                          float* dL_dsh0, float* dL_dshs, void* stream_) {
+                          float* dL_dsh0, float* dL_dshs, float* subdiv, void* stream_) {
   cudaStream_t stream = static_cast<cudaStream_t>(stream_);
   if (!p || !ws || !vox_centers || !dL_dsh0 || sh_degree < 0 || sh_degree > 3 ||
       M - 1 < (sh_degree + 1) * (sh_degree + 1) - 1 || (M > 1 && !dL_dshs))
@@ -813,11 +828,12 @@ int svr_batch_sh_backward(svr_batch_plan* p, void* ws, const float* vox_centers,
   const int g = (P + kShBwThreads - 1) / kShBwThreads;
   const size_t smem = (size_t)kShBwThreads * (3 + 3 * (M - 1)) * sizeof(float);
   if (smem > 48 * 1024) return SVR_ERR_SHAPE;  // M <= 32 coefficients per channel
+  const float4* d4 = reinterpret_cast<const float4*>(q.drgbs);
   switch (sh_degree) {
-    case 0: sh_bw_batch_kernel<0><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
-    case 1: sh_bw_batch_kernel<1><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
-    case 2: sh_bw_batch_kernel<2><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
-    default: sh_bw_batch_kernel<3><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, q.drgbs, dL_dsh0, dL_dshs); break;
+    case 0: sh_bw_batch_kernel<0><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, d4, dL_dsh0, dL_dshs, subdiv); break;
+    case 1: sh_bw_batch_kernel<1><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, d4, dL_dsh0, dL_dshs, subdiv); break;
+    case 2: sh_bw_batch_kernel<2><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, d4, dL_dsh0, dL_dshs, subdiv); break;
+    default: sh_bw_batch_kernel<3><<<g, kShBwThreads, smem, stream>>>(p->vt, P, M, vox_centers, d4, dL_dsh0, dL_dshs, subdiv); break;
   }
   return check_last();
 }

@@ -350,7 +350,7 @@ int svr_rasterize_backward(const svr_camera* cam, int n_samp, int64_t P, int64_t
   BwdTileIn in{out_T, im.n_contrib, dL_dcolor, need_depth ? dL_ddepth : nullptr,
                need_normal ? dL_dnormal : nullptr, dL_dT, lambda_R_concen > 0 ? gt_color : nullptr,
                need_dist ? out_depth : nullptr, lambda_R_concen, lambda_ascending, lambda_dist, 1};
-  BwdTileOut out{dL_dgeos, dL_drgbs, subdiv_p_bw, g.header + 1};
+  BwdTileOut out{dL_dgeos, dL_drgbs, subdiv_p_bw, g.header + 1, aligned16(dL_dgeos) ? 1 : 0};
   // the forward's tile order (read only: the image buffer is the forward's saved state)
   launch_render_bwd(vp, im.ranges, im.tile_last, num_rendered > 0 ? bl.vals_b : nullptr, va, in, out, n_samp,
                     need_depth != 0, need_dist, need_normal != 0, im.order, stream);
@@ -528,6 +528,22 @@ int svr_gather_grid_params_bw(int dim, int64_t n_care, const int64_t* vox_key, c
   cudaStream_t stream = static_cast<cudaStream_t>(stream_);
   if ((dim != 1 && dim != 3) || n_care < 0 || n_care >= (1ll << 31)) return SVR_ERR_SHAPE;
   launch_gather_bw(dim, (int)n_care, vox_key, care_idx, dL_dvox, dL_dgrid, stream);
+  return check_launch(0, stream);
+}
+
+int svr_gather_grid_geo_all(int64_t P, const int64_t* vox_key, const void* grid_pts, int grid_bf16, void* geos_out,
+                            int out_bf16, void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (P < 0 || (P > 0 && (!vox_key || !grid_pts || !geos_out))) return SVR_ERR_SHAPE;
+  launch_gather_all_geo(P, vox_key, grid_pts, grid_bf16 != 0, geos_out, out_bf16 != 0, stream);
+  return check_launch(0, stream);
+}
+
+int svr_scatter_grid_geo_all(int64_t P, const int64_t* vox_key, const float* dL_dgeos, float* dL_dgrid,
+                             void* stream_) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  if (P < 0 || (P > 0 && (!vox_key || !dL_dgeos || !dL_dgrid))) return SVR_ERR_SHAPE;
+  launch_scatter_all_geo(P, vox_key, dL_dgeos, dL_dgrid, stream);
   return check_launch(0, stream);
 }
 

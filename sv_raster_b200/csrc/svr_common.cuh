@@ -102,6 +102,37 @@ __device__ __forceinline__ void density_act_and_grad(float x, float& act, float&
   }
 }
 
+// Arithmetic of the compositing loops.  EXACT is the reference's own
+// operations (IEEE division, libdevice expf): contributor counts and images
+// come out bit-identical.  FAST uses the hardware exponential (ex2.approx of
+// x*log2(e), a few ulp) and an approximate division (reciprocal and multiply,
+// 2 ulp) for the per-(pixel, voxel) exponentials and the transmittance
+// recovery; results then differ from EXACT in the last bits, and a pixel may
+// stop one voxel earlier or later where T lands on the early-stop threshold.
+template <bool FAST>
+__device__ __forceinline__ float exp_f(float x) {
+  return FAST ? __expf(x) : expf(x);
+}
+template <bool FAST>
+__device__ __forceinline__ float div_f(float a, float b) {
+  return FAST ? __fdividef(a, b) : a / b;
+}
+template <bool FAST>
+__device__ __forceinline__ float density_act_f(float x) {
+  return (x > 1.1f) ? x : exp_f<FAST>(0.909090909091f * x - 0.904689820196f);
+}
+template <bool FAST>
+__device__ __forceinline__ void density_act_and_grad_f(float x, float& act, float& grad) {
+  if (x > 1.1f) {
+    act = x;
+    grad = 1.0f;
+  } else {
+    const float e = exp_f<FAST>(0.909090909091f * x - 0.904689820196f);
+    act = e;
+    grad = 0.909090909091f * e;
+  }
+}
+
 __device__ __forceinline__ float contract_depth(float x) {  // auxiliary.h:235-238
   return (x < 1.f) ? x : 2.f - 1.f / x;
 }

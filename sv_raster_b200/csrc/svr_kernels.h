@@ -78,16 +78,16 @@ void ensure_fwd_batch_attributes();
 void ensure_bwd_batch_attributes();
 void launch_render_fwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* vals, const VoxelArrays& va, int P, size_t rgb_view_stride,
-                             const FwdTileOut& out, int ns, int tile, int stage, const uint32_t* order,
+                             const FwdTileOut& out, int ns, int tile, int stage, bool fast, const uint32_t* order,
                              uint32_t* counter, int ctas_per_sm, cudaStream_t stream);
 void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t* tile_last, const uint32_t* vals,
                        const VoxelArrays& va, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
                        bool dist, bool normal, const uint32_t* order, cudaStream_t stream);
 void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
-                             size_t rgb_view_stride, const BwdTileIn& in, const BwdTileOut& out, int ns, int tile,
-                             int stage, const uint32_t* order, uint32_t* counter, int ctas_per_sm,
-                             cudaStream_t stream);
+                             size_t rgb_view_stride, size_t drgb_view_stride, const BwdTileIn& in,
+                             const BwdTileOut& out, int ns, int tile, int stage, bool fast, const uint32_t* order,
+                             uint32_t* counter, int ctas_per_sm, cudaStream_t stream);
 // Grid of a persistent launch: resident CTAs of `kernel` on this device
 // (capped at ctas_per_sm per SM when > 0), at most n_items.
 int persistent_grid(const void* kernel, int threads, size_t dyn_smem, int n_items, int ctas_per_sm);
@@ -126,6 +126,12 @@ void launch_gather(int dim, int n_care, const int64_t* vox_key, const int64_t* c
                    float* out, cudaStream_t stream);
 void launch_gather_bw(int dim, int n_care, const int64_t* vox_key, const int64_t* care_idx, const float* dL_dvox,
                       float* dL_dgrid, cudaStream_t stream);
+// All voxels (no care list): corner densities from the grid (fp32 or bf16 in,
+// fp32 or bf16 rows out), and the density gradients added into the grid's.
+void launch_gather_all_geo(int64_t P, const int64_t* vox_key, const void* grid_pts, bool grid_bf16, void* out,
+                           bool out_bf16, cudaStream_t stream);
+void launch_scatter_all_geo(int64_t P, const int64_t* vox_key, const float* dL_dgeos, float* dL_dgrid,
+                            cudaStream_t stream);
 
 // svr_tv.cu
 void launch_total_variation_bw(const float* grid, const int64_t* vox_key, float weight, const float* vox_size_inv,

@@ -52,14 +52,15 @@ struct BwdBatchArgs {
   const uint32_t* vals;
   VoxelArrays va;
   int P;
-  size_t rgb_view_stride;
+  size_t rgb_view_stride;   // elements between views in va.rgbs ([V,P,3])
+  size_t drgb_view_stride;  // elements between views in out.dL_drgbs ([V,P,4])
   BwdTileIn in;    // base pointers, offset per view
-  BwdTileOut out;  // dL_drgbs offset per view by rgb_view_stride
+  BwdTileOut out;  // dL_drgbs offset per view by drgb_view_stride
   const uint32_t* order;  // [n_items] work order, or nullptr
   uint32_t* counter;      // work counter, zero at launch
 };
 
-template <class CFG, int NS>
+template <class CFG, int NS, bool FAST>
 __global__ void __launch_bounds__(CFG::NT, bwd_min_blocks<CFG>())
 render_bwd_batch_kernel(const __grid_constant__ BwdBatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -86,9 +87,9 @@ render_bwd_batch_kernel(const __grid_constant__ BwdBatchArgs a) {
     in.dL_dcolor = a.in.dL_dcolor + 3 * pb;
     in.dL_dT = a.in.dL_dT + pb;
     BwdTileOut o = a.out;
-    o.dL_drgbs = a.out.dL_drgbs + (size_t)view * a.rgb_view_stride;
-    render_tile_bwd<CFG, NS, false, false, false>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.tile_last[item],
-                                                  a.vals, va, in, o, sm.s, sm.grad);
+    o.dL_drgbs = a.out.dL_drgbs + (size_t)view * a.drgb_view_stride;
+    render_tile_bwd<CFG, NS, false, false, false, FAST, true>(vp, sm.c2w, tile_x, tile_y, a.ranges[item],
+                                                              a.tile_last[item], a.vals, va, in, o, sm.s, sm.grad);
     __syncthreads();  // shared state (item, camera, staging) is free for the next tile
   }
 }
@@ -118,7 +119,9 @@ void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t
 
 template <class CFG, int NS>
 static void set_bwd_batch_attr() {
-  cudaFuncSetAttribute(render_bwd_batch_kernel<CFG, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(render_bwd_batch_kernel<CFG, NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(BwdSmem<CFG>));
+  cudaFuncSetAttribute(render_bwd_batch_kernel<CFG, NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(BwdSmem<CFG>));
 }
 
@@ -144,34 +147,41 @@ void ensure_bwd_batch_attributes() {
   });
 }
 
-template <class CFG>
-static void launch_bwd_batch_cfg(const BwdBatchArgs& args, int ns, int ctas_per_sm, cudaStream_t stream) {
+template <class CFG, bool FAST>
+static void launch_bwd_batch_arith(const BwdBatchArgs& args, int ns, int ctas_per_sm, cudaStream_t stream) {
   const size_t smem = sizeof(BwdSmem<CFG>);
   auto go = [&](auto kfn) {
     const int grid = persistent_grid((const void*)kfn, CFG::NT, smem, args.n_items, ctas_per_sm);
     kfn<<<grid, CFG::NT, smem, stream>>>(args);
   };
-  if (ns == 1) go(render_bwd_batch_kernel<CFG, 1>);
-  else if (ns == 2) go(render_bwd_batch_kernel<CFG, 2>);
-  else go(render_bwd_batch_kernel<CFG, 3>);
+  if (ns == 1) go(render_bwd_batch_kernel<CFG, 1, FAST>);
+  else if (ns == 2) go(render_bwd_batch_kernel<CFG, 2, FAST>);
+  else go(render_bwd_batch_kernel<CFG, 3, FAST>);
+}
+
+template <class CFG>
+static void launch_bwd_batch_cfg(const BwdBatchArgs& args, int ns, bool fast, int ctas_per_sm, cudaStream_t stream) {
+  if (fast) launch_bwd_batch_arith<CFG, true>(args, ns, ctas_per_sm, stream);
+  else launch_bwd_batch_arith<CFG, false>(args, ns, ctas_per_sm, stream);
 }
 
 void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
-                             size_t rgb_view_stride, const BwdTileIn& in, const BwdTileOut& out, int ns, int tile,
-                             int stage, const uint32_t* order, uint32_t* counter, int ctas_per_sm,
-                             cudaStream_t stream) {
+                             size_t rgb_view_stride, size_t drgb_view_stride, const BwdTileIn& in,
+                             const BwdTileOut& out, int ns, int tile, int stage, bool fast, const uint32_t* order,
+                             uint32_t* counter, int ctas_per_sm, cudaStream_t stream) {
   if (n_items <= 0) return;
   ensure_bwd_batch_attributes();
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
-  const BwdBatchArgs args{views, n_items, ranges, tile_last, vals, va, P, rgb_view_stride, in, out, order, counter};
-  if (tile == 8 && stage == 32) launch_bwd_batch_cfg<TileCfg<8, 32>>(args, ns, ctas_per_sm, stream);
-  else if (tile == 8 && stage == 128) launch_bwd_batch_cfg<TileCfg<8, 128>>(args, ns, ctas_per_sm, stream);
-  else if (tile == 8) launch_bwd_batch_cfg<TileCfg<8, 64>>(args, ns, ctas_per_sm, stream);
-  else if (tile == 32) launch_bwd_batch_cfg<TileCfg<32, 256>>(args, ns, ctas_per_sm, stream);
-  else if (stage == 128) launch_bwd_batch_cfg<TileCfg<16, 128>>(args, ns, ctas_per_sm, stream);
-  else if (stage == 512) launch_bwd_batch_cfg<TileCfg<16, 512>>(args, ns, ctas_per_sm, stream);
-  else launch_bwd_batch_cfg<TileCfg<16, 256>>(args, ns, ctas_per_sm, stream);
+  const BwdBatchArgs args{views, n_items, ranges, tile_last, vals, va, P, rgb_view_stride, drgb_view_stride, in, out,
+                          order, counter};
+  if (tile == 8 && stage == 32) launch_bwd_batch_cfg<TileCfg<8, 32>>(args, ns, fast, ctas_per_sm, stream);
+  else if (tile == 8 && stage == 128) launch_bwd_batch_cfg<TileCfg<8, 128>>(args, ns, fast, ctas_per_sm, stream);
+  else if (tile == 8) launch_bwd_batch_cfg<TileCfg<8, 64>>(args, ns, fast, ctas_per_sm, stream);
+  else if (tile == 32) launch_bwd_batch_cfg<TileCfg<32, 256>>(args, ns, fast, ctas_per_sm, stream);
+  else if (stage == 128) launch_bwd_batch_cfg<TileCfg<16, 128>>(args, ns, fast, ctas_per_sm, stream);
+  else if (stage == 512) launch_bwd_batch_cfg<TileCfg<16, 512>>(args, ns, fast, ctas_per_sm, stream);
+  else launch_bwd_batch_cfg<TileCfg<16, 256>>(args, ns, fast, ctas_per_sm, stream);
 }
 
 }  // namespace svr

@@ -9,7 +9,8 @@
 // gradient pack (:515-522).  The reference issues 12 global atomics per
 // contributing (pixel, voxel); here each warp reduces its lanes' gradients
 // with shuffles into a shared-memory accumulator per staged record, and each
-// record is flushed once per tile with 12 global reductions.
+// record is flushed once per tile (16-byte vector reductions where the
+// gradient rows are aligned).
 #pragma once
 
 #include "svr_render.cuh"
@@ -33,9 +34,10 @@ struct BwdTileIn {
 
 struct BwdTileOut {
   float* dL_dgeos;   // [P,8]
-  float* dL_drgbs;   // [P,3] (this view)
-  float* subdiv;     // [P]
+  float* dL_drgbs;   // [P,3] (this view), or [P,4] with RGB4 (xyz = dL/drgb, w = subdivision priority)
+  float* subdiv;     // [P] (unused with RGB4)
   uint32_t* err;     // device error word
+  int geo_vec4;      // dL_dgeos is 16-byte aligned: flush its rows with vector reductions
 };
 
 constexpr int kGradStride = 13;  // 12 gradient floats + 1 pad (bank spread)
@@ -86,7 +88,10 @@ __device__ __forceinline__ int warp_reduce_scatter12(float v[12], int lane) {
   return ((lane & 1) == 0 && local < 3) ? (hi16 ? 6 : 0) + (hi8 ? 3 : 0) + local : -1;
 }
 
-template <class CFG, int NS, bool DEPTH, bool DIST, bool NORMAL>
+// FAST selects the arithmetic of the per-(pixel, voxel) loop (exp_f, div_f in
+// svr_common.cuh); RGB4 the [P,4] colour-gradient layout whose rows, like the
+// density rows, are flushed with one 16-byte vector reduction each.
+template <class CFG, int NS, bool DEPTH, bool DIST, bool NORMAL, bool FAST = false, bool RGB4 = false>
 __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const float* __restrict__ c2w_s, int tile_x,
                                                 int tile_y, uint2 range_raw, uint32_t tile_last,
                                                 const uint32_t* __restrict__ vals, const VoxelArrays& va,
@@ -209,10 +214,10 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
 #pragma unroll
                 for (int c = 0; c < 8; ++c) d += geo[c] * w[c];
                 float act, act_grad;
-                density_act_and_grad(d, act, act_grad);
+                density_act_and_grad_f<FAST>(d, act, act_grad);
                 const float lvi = kStepScale * step_sz * act;
                 vol_int += lvi;
-                if (DEPTH && NS > 1) local_alpha[k] = fminf(kMaxAlpha, 1.f - expf(-lvi));
+                if (DEPTH && NS > 1) local_alpha[k] = fminf(kMaxAlpha, 1.f - exp_f<FAST>(-lvi));
                 const float dd_dd = kStepScale * step_sz * act_grad;
 #pragma unroll
                 for (int c = 0; c < 8; ++c) {
@@ -222,11 +227,11 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
                 }
                 qx = qx + qsx; qy = qy + qsy; qz = qz + qsz;
               }
-              const float exp_neg = expf(-vol_int);
+              const float exp_neg = exp_f<FAST>(-vol_int);
               const float alpha = fminf(kMaxAlpha, 1.f - exp_neg);
               if (!(alpha < kMinAlpha)) {
                 contrib = true;
-                T = T / (1.f - alpha);
+                T = div_f<FAST>(T, 1.f - alpha);
                 const float pt_w = alpha * T;
                 const float4 rgbv = s.rgb[j];
                 float dL_dpt_w = gx * rgbv.x + gy * rgbv.y + gz * rgbv.z;
@@ -365,11 +370,21 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
       for (int c = 0; c < 12; ++c) gsum += fabsf(acc[c]);
       if (gsum != 0.f) {
         const uint32_t vid = (uint32_t)__float_as_int(s.corner[t].w);
+        float* g = out.dL_dgeos + 8 * (size_t)vid;
+        if (RGB4 || out.geo_vec4) {
+          atomicAdd(reinterpret_cast<float4*>(g), make_float4(acc[0], acc[1], acc[2], acc[3]));
+          atomicAdd(reinterpret_cast<float4*>(g) + 1, make_float4(acc[4], acc[5], acc[6], acc[7]));
+        } else {
 #pragma unroll
-        for (int c = 0; c < 8; ++c) atomicAdd(out.dL_dgeos + 8 * (size_t)vid + c, acc[c]);
+          for (int c = 0; c < 8; ++c) atomicAdd(g + c, acc[c]);
+        }
+        if (RGB4) {
+          atomicAdd(reinterpret_cast<float4*>(out.dL_drgbs) + vid, make_float4(acc[8], acc[9], acc[10], acc[11]));
+        } else {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) atomicAdd(out.dL_drgbs + 3 * (size_t)vid + c, acc[8 + c]);
-        atomicAdd(out.subdiv + vid, acc[11]);
+          for (int c = 0; c < 3; ++c) atomicAdd(out.dL_drgbs + 3 * (size_t)vid + c, acc[8 + c]);
+          atomicAdd(out.subdiv + vid, acc[11]);
+        }
       }
 #pragma unroll
       for (int c = 0; c < 12; ++c) acc[c] = 0.f;

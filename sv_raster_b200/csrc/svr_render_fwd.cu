@@ -75,7 +75,7 @@ struct FwdBatchSmem {
   uint32_t item;
 };
 
-template <class CFG, int NS>
+template <class CFG, int NS, bool FAST>
 __global__ void __launch_bounds__(CFG::NT, fwd_min_blocks<CFG>())
 render_fwd_batch_kernel(const __grid_constant__ FwdBatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -100,8 +100,9 @@ render_fwd_batch_kernel(const __grid_constant__ FwdBatchArgs a) {
     o.n_contrib = a.out.n_contrib + vp.pix_base;
     o.color = a.out.color + 3 * (size_t)vp.pix_base;
     o.T = a.out.T + vp.pix_base;
-    render_tile_fwd<CFG, NS, false, false, false, false>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.vals, va, o,
-                                                         o.tile_last + local, sm.s, sm.red);
+    render_tile_fwd<CFG, NS, false, false, false, false, false, FAST>(vp, sm.c2w, tile_x, tile_y, a.ranges[item],
+                                                                      a.vals, va, o, o.tile_last + local, sm.s,
+                                                                      sm.red);
     __syncthreads();  // shared state (item, camera, staging) is free for the next tile
   }
 }
@@ -150,7 +151,9 @@ bool batch_tile_supported(int tile, int stage) {
 
 template <class CFG, int NS>
 static void set_fwd_batch_attr() {
-  cudaFuncSetAttribute(render_fwd_batch_kernel<CFG, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(render_fwd_batch_kernel<CFG, NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(FwdBatchSmem<CFG>));
+  cudaFuncSetAttribute(render_fwd_batch_kernel<CFG, NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(FwdBatchSmem<CFG>));
 }
 
@@ -176,33 +179,39 @@ void ensure_fwd_batch_attributes() {
   });
 }
 
-template <class CFG>
-static void launch_fwd_batch_cfg(const FwdBatchArgs& args, int ns, int ctas_per_sm, cudaStream_t stream) {
+template <class CFG, bool FAST>
+static void launch_fwd_batch_arith(const FwdBatchArgs& args, int ns, int ctas_per_sm, cudaStream_t stream) {
   const size_t smem = sizeof(FwdBatchSmem<CFG>);
   auto go = [&](auto kfn) {
     const int grid = persistent_grid((const void*)kfn, CFG::NT, smem, args.n_items, ctas_per_sm);
     kfn<<<grid, CFG::NT, smem, stream>>>(args);
   };
-  if (ns == 1) go(render_fwd_batch_kernel<CFG, 1>);
-  else if (ns == 2) go(render_fwd_batch_kernel<CFG, 2>);
-  else go(render_fwd_batch_kernel<CFG, 3>);
+  if (ns == 1) go(render_fwd_batch_kernel<CFG, 1, FAST>);
+  else if (ns == 2) go(render_fwd_batch_kernel<CFG, 2, FAST>);
+  else go(render_fwd_batch_kernel<CFG, 3, FAST>);
+}
+
+template <class CFG>
+static void launch_fwd_batch_cfg(const FwdBatchArgs& args, int ns, bool fast, int ctas_per_sm, cudaStream_t stream) {
+  if (fast) launch_fwd_batch_arith<CFG, true>(args, ns, ctas_per_sm, stream);
+  else launch_fwd_batch_arith<CFG, false>(args, ns, ctas_per_sm, stream);
 }
 
 void launch_render_fwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* vals, const VoxelArrays& va, int P, size_t rgb_view_stride,
-                             const FwdTileOut& out, int ns, int tile, int stage, const uint32_t* order,
+                             const FwdTileOut& out, int ns, int tile, int stage, bool fast, const uint32_t* order,
                              uint32_t* counter, int ctas_per_sm, cudaStream_t stream) {
   if (n_items <= 0) return;
   ensure_fwd_batch_attributes();
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
   const FwdBatchArgs args{views, n_items, ranges, vals, va, P, rgb_view_stride, out, order, counter};
-  if (tile == 8 && stage == 32) launch_fwd_batch_cfg<TileCfg<8, 32>>(args, ns, ctas_per_sm, stream);
-  else if (tile == 8 && stage == 128) launch_fwd_batch_cfg<TileCfg<8, 128>>(args, ns, ctas_per_sm, stream);
-  else if (tile == 8) launch_fwd_batch_cfg<TileCfg<8, 64>>(args, ns, ctas_per_sm, stream);
-  else if (tile == 32) launch_fwd_batch_cfg<TileCfg<32, 256>>(args, ns, ctas_per_sm, stream);
-  else if (stage == 128) launch_fwd_batch_cfg<TileCfg<16, 128>>(args, ns, ctas_per_sm, stream);
-  else if (stage == 512) launch_fwd_batch_cfg<TileCfg<16, 512>>(args, ns, ctas_per_sm, stream);
-  else launch_fwd_batch_cfg<TileCfg<16, 256>>(args, ns, ctas_per_sm, stream);
+  if (tile == 8 && stage == 32) launch_fwd_batch_cfg<TileCfg<8, 32>>(args, ns, fast, ctas_per_sm, stream);
+  else if (tile == 8 && stage == 128) launch_fwd_batch_cfg<TileCfg<8, 128>>(args, ns, fast, ctas_per_sm, stream);
+  else if (tile == 8) launch_fwd_batch_cfg<TileCfg<8, 64>>(args, ns, fast, ctas_per_sm, stream);
+  else if (tile == 32) launch_fwd_batch_cfg<TileCfg<32, 256>>(args, ns, fast, ctas_per_sm, stream);
+  else if (stage == 128) launch_fwd_batch_cfg<TileCfg<16, 128>>(args, ns, fast, ctas_per_sm, stream);
+  else if (stage == 512) launch_fwd_batch_cfg<TileCfg<16, 512>>(args, ns, fast, ctas_per_sm, stream);
+  else launch_fwd_batch_cfg<TileCfg<16, 256>>(args, ns, fast, ctas_per_sm, stream);
 }
 
 }  // namespace svr

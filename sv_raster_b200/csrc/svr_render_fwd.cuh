@@ -30,7 +30,8 @@ struct FwdTileOut {
 // `last_slot` receives range.x + the tile's largest contributor count, with
 // atomicMax when SHARED_LAST (several CTAs share one list and slot, which
 // then starts at 0).
-template <class CFG, int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW, bool SHARED_LAST = false>
+// FAST selects the arithmetic of the per-(pixel, voxel) loop (exp_f, svr_common.cuh).
+template <class CFG, int NS, bool DEPTH, bool DIST, bool NORMAL, bool MAXW, bool SHARED_LAST = false, bool FAST = false>
 __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const float* __restrict__ c2w_s, int tile_x,
                                                 int tile_y, uint2 range, const uint32_t* __restrict__ vals,
                                                 const VoxelArrays& va, const FwdTileOut& out, uint32_t* last_slot,
@@ -104,12 +105,12 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
           float d = 0.f;
 #pragma unroll
           for (int c = 0; c < 8; ++c) d += geo[c] * w[c];
-          const float lvi = kStepScale * step_sz * density_act(d);
+          const float lvi = kStepScale * step_sz * density_act_f<FAST>(d);
           vol_int += lvi;
-          if (DEPTH && NS > 1) local_alpha[k] = fminf(kMaxAlpha, 1.f - expf(-lvi));
+          if (DEPTH && NS > 1) local_alpha[k] = fminf(kMaxAlpha, 1.f - exp_f<FAST>(-lvi));
           qx = qx + qsx; qy = qy + qsy; qz = qz + qsz;
         }
-        const float alpha = fminf(kMaxAlpha, 1.f - expf(-vol_int));
+        const float alpha = fminf(kMaxAlpha, 1.f - exp_f<FAST>(-vol_int));
         if (alpha < kMinAlpha) continue;
 
         const float pt_w = T * alpha;

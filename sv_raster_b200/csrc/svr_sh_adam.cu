@@ -342,4 +342,86 @@ void launch_gather_bw(int dim, int n_care, const int64_t* vox_key, const int64_t
   else launch_slots<3, 2>(gather_bw_kernel<3, 2>, n_care, vox_key, care_idx, dL_dvox, dL_dgrid, stream);
 }
 
+// Batched training over grid points: every voxel's 8 corner densities
+// gathered from the grid (fp32 or bf16 grid, fp32 or bf16 output rows), and
+// the density gradients [P,8] added back into the grid gradient.  One slot
+// per (voxel, corner), U slots per thread, as above; no care list (all
+// voxels are rendered by the batched step).
+__device__ __forceinline__ float to_f32(float x) { return x; }
+__device__ __forceinline__ float to_f32(__nv_bfloat16 x) { return __bfloat162float(x); }
+template <class T>
+__device__ __forceinline__ T from_f32(float x);
+template <>
+__device__ __forceinline__ float from_f32<float>(float x) { return x; }
+template <>
+__device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
+
+template <int U, class GT, class OT>
+__global__ void __launch_bounds__(kGatherThreads)
+gather_all_geo_kernel(int64_t n_slots, const int64_t* __restrict__ vox_key, const GT* __restrict__ grid_pts,
+                      OT* __restrict__ out) {
+  const int64_t base = (int64_t)blockIdx.x * (kGatherThreads * U) + threadIdx.x;
+  int64_t k[U];
+#pragma unroll
+  for (int j = 0; j < U; ++j) {
+    const int64_t t = base + j * kGatherThreads;
+    k[j] = t < n_slots ? vox_key[t] : -1;
+  }
+  float v[U];
+#pragma unroll
+  for (int j = 0; j < U; ++j) v[j] = k[j] >= 0 ? to_f32(grid_pts[k[j]]) : 0.f;
+#pragma unroll
+  for (int j = 0; j < U; ++j) {
+    const int64_t t = base + j * kGatherThreads;
+    if (t < n_slots) out[t] = from_f32<OT>(v[j]);
+  }
+}
+
+template <int U>
+__global__ void __launch_bounds__(kGatherThreads)
+scatter_all_geo_kernel(int64_t n_slots, const int64_t* __restrict__ vox_key, const float* __restrict__ dL_dgeos,
+                       float* __restrict__ dL_dgrid) {
+  const int64_t base = (int64_t)blockIdx.x * (kGatherThreads * U) + threadIdx.x;
+  int64_t k[U];
+  float g[U];
+#pragma unroll
+  for (int j = 0; j < U; ++j) {
+    const int64_t t = base + j * kGatherThreads;
+    k[j] = t < n_slots ? vox_key[t] : -1;
+    g[j] = t < n_slots ? dL_dgeos[t] : 0.f;
+  }
+#pragma unroll
+  for (int j = 0; j < U; ++j)
+    if (k[j] >= 0 && g[j] != 0.f) atomicAdd(dL_dgrid + k[j], g[j]);
+}
+
+void launch_gather_all_geo(int64_t P, const int64_t* vox_key, const void* grid_pts, bool grid_bf16, void* out,
+                           bool out_bf16, cudaStream_t stream) {
+  if (P <= 0) return;
+  constexpr int U = 4;
+  const int64_t n_slots = 8 * P;
+  const unsigned g = (unsigned)((n_slots + kGatherThreads * U - 1) / (kGatherThreads * U));
+  using bf = __nv_bfloat16;
+  if (grid_bf16 && out_bf16)
+    gather_all_geo_kernel<U, bf, bf><<<g, kGatherThreads, 0, stream>>>(n_slots, vox_key, (const bf*)grid_pts, (bf*)out);
+  else if (grid_bf16)
+    gather_all_geo_kernel<U, bf, float><<<g, kGatherThreads, 0, stream>>>(n_slots, vox_key, (const bf*)grid_pts,
+                                                                          (float*)out);
+  else if (out_bf16)
+    gather_all_geo_kernel<U, float, bf><<<g, kGatherThreads, 0, stream>>>(n_slots, vox_key, (const float*)grid_pts,
+                                                                          (bf*)out);
+  else
+    gather_all_geo_kernel<U, float, float><<<g, kGatherThreads, 0, stream>>>(n_slots, vox_key,
+                                                                             (const float*)grid_pts, (float*)out);
+}
+
+void launch_scatter_all_geo(int64_t P, const int64_t* vox_key, const float* dL_dgeos, float* dL_dgrid,
+                            cudaStream_t stream) {
+  if (P <= 0) return;
+  constexpr int U = 4;
+  const int64_t n_slots = 8 * P;
+  const unsigned g = (unsigned)((n_slots + kGatherThreads * U - 1) / (kGatherThreads * U));
+  scatter_all_geo_kernel<U><<<g, kGatherThreads, 0, stream>>>(n_slots, vox_key, dL_dgeos, dL_dgrid);
+}
+
 }  // namespace svr

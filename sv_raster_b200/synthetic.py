@@ -307,6 +307,43 @@ def build_scene(name, n_voxels, seed, kind, surf_levels, bg_levels, geo_mu, geo_
     return Scene(name, path, lv, centers, lengths, geos, sh0, shs, cameras, targets)
 
 
+def _unit(rng):
+    d = rng.standard_normal(3)
+    return d / np.linalg.norm(d)
+
+
+def config_cameras(name, seed=0, view_set=0):
+    """Cameras of a benchmark configuration (see config_scene).  view_set 0
+    is the configuration's own set; view_set k > 0 draws another set of the
+    same count, sizes and distance distribution (the views of rank k in a
+    view-parallel run, so every rank does the single-GPU amount of work)."""
+    rng = np.random.default_rng(seed + 7919 * view_set)
+    if name == "c1":
+        if view_set == 0:
+            d1 = np.array([0.9, -0.7, -1.0]) / np.linalg.norm([0.9, -0.7, -1.0])
+            return [make_camera(256, 256, 50.0, (0.0, 0.0, -1.5)), make_camera(256, 256, 50.0, d1 * 1.5),
+                    # inside the sphere shell: voxels straddle the camera's axis planes (multi-quadrant)
+                    make_camera(200, 136, 70.0, (0.03, -0.02, 0.01), target=(0.4, 0.1, 0.3))]
+        return [make_camera(256, 256, 50.0, _unit(rng) * 1.5), make_camera(256, 256, 50.0, _unit(rng) * 1.5),
+                make_camera(200, 136, 70.0, _unit(rng) * 0.03, target=_unit(rng) * 0.5)]
+    if name == "c2":
+        d = np.array([0.6, -0.5, -1.2]) if view_set == 0 else _unit(rng)
+        return [make_camera(1297, 840, 50.0, d / np.linalg.norm(d) * 1.6)]
+    if name == "c3":
+        return orbit_cameras(16, seed + 10 + 7919 * view_set)
+    if name == "c4":
+        return orbit_cameras(8, seed + 20 + 7919 * view_set, radius=(1.5, 2.0), fixed_size=(1920, 1080))
+    if name == "c5":
+        rng = np.random.default_rng(seed + 30 + 7919 * view_set)
+        cams = []
+        for _ in range(32):
+            sc = rng.uniform(0.5, 1.0)
+            cams += orbit_cameras(1, int(rng.integers(1 << 30)), radius=(1.5, 2.5), hemisphere=True,
+                                  fixed_size=(int(1920 * sc) // 2 * 2, int(1080 * sc) // 2 * 2))
+        return cams
+    raise ValueError(f"unknown config {name}")
+
+
 def config_scene(name, seed=0, n_voxels=None):
     """Synthetic stand-ins for the five benchmark configurations.
 
@@ -320,31 +357,14 @@ def config_scene(name, seed=0, n_voxels=None):
     c5: 16M voxels (levels 6-16), 32 views 960x540..1920x1080 on a hemisphere.
     `n_voxels` overrides the voxel count (for scaled-down tests).
     """
+    cams = config_cameras(name, seed)
     if name == "c1":
-        cams = [make_camera(256, 256, 50.0, (0.0, 0.0, -1.5)),
-                make_camera(256, 256, 50.0, np.array([0.9, -0.7, -1.0]) / np.linalg.norm([0.9, -0.7, -1.0]) * 1.5),
-                # inside the sphere shell: voxels straddle the camera's axis planes (multi-quadrant)
-                make_camera(200, 136, 70.0, (0.03, -0.02, 0.01), target=(0.4, 0.1, 0.3))]
         return build_scene("c1", n_voxels or 20000, seed, "sphere", (6, 8), (6, 8), -1.0, 1.0, cams)
-    if name == "c2":
-        d = np.array([0.6, -0.5, -1.2])
-        cams = [make_camera(1297, 840, 50.0, d / np.linalg.norm(d) * 1.6)]
-        return build_scene("c2", n_voxels or 2_000_000, seed, "mixed", (8, 12), (5, 7), -2.0, 1.5, cams)
-    if name == "c3":
-        cams = orbit_cameras(16, seed + 10)
-        return build_scene("c3", n_voxels or 2_000_000, seed, "mixed", (8, 12), (5, 7), -2.0, 1.5, cams)
+    if name in ("c2", "c3"):
+        return build_scene(name, n_voxels or 2_000_000, seed, "mixed", (8, 12), (5, 7), -2.0, 1.5, cams)
     if name == "c4":
-        cams = orbit_cameras(8, seed + 20, radius=(1.5, 2.0), fixed_size=(1920, 1080))
         return build_scene("c4", n_voxels or 8_000_000, seed, "mixed", (8, 14), (5, 7), -2.0, 1.5, cams)
-    if name == "c5":
-        rng = np.random.default_rng(seed + 30)
-        cams = []
-        for _ in range(32):
-            s = rng.uniform(0.5, 1.0)
-            cams += orbit_cameras(1, int(rng.integers(1 << 30)), radius=(1.5, 2.5), hemisphere=True,
-                                  fixed_size=(int(1920 * s) // 2 * 2, int(1080 * s) // 2 * 2))
-        return build_scene("c5", n_voxels or 16_000_000, seed, "mixed", (6, 16), (5, 7), -2.0, 1.5, cams)
-    raise ValueError(f"unknown config {name}")
+    return build_scene("c5", n_voxels or 16_000_000, seed, "mixed", (6, 16), (5, 7), -2.0, 1.5, cams)
 
 
 def grid_keys(octpath, level, dev):
@@ -363,6 +383,18 @@ def grid_keys(octpath, level, dev):
     code = (corner[..., 0] << 34) | (corner[..., 1] << 17) | corner[..., 2]
     uniq, inv = torch.unique(code.reshape(-1), return_inverse=True)
     return inv.reshape(-1, 8).contiguous(), int(uniq.numel())
+
+
+def grid_params(sc, dev, seed=0):
+    """Grid-point parametrisation of a scene's densities, as the reference
+    trains them (sparse_voxel_gears/constructor.py:71-73): vox_key int64
+    [P,8] on `dev` (grid_keys) and seeded grid values [M] drawn from the
+    scene's density distribution (the mean and spread of its per-voxel
+    corner values).  Returns (vox_key, grid_pts numpy fp32)."""
+    key, M = grid_keys(sc.octpath, sc.octlevel, dev)
+    rng = np.random.default_rng(seed + 5)
+    mu, sd = float(np.mean(sc.geos)), float(np.std(sc.geos))
+    return key, rng.normal(mu, sd, size=M).astype(np.float32)
 
 
 def scene_cache_dir():

@@ -15,16 +15,20 @@ from ._native import Camera, check, lib
 RECORD_BYTES = 68  # bbox 8 + centre 12 + length 4 + 8 densities 32 + rgb 12
 
 
-def rank_cameras(cameras, rank, world, seed=1007):
-    """Views rendered by `rank` of `world` (weak scaling: every rank renders
-    as many views as the single-GPU workload, all at the same resolution).
-    Rank 0 keeps the workload's own cameras; other ranks get distinct seeded
-    orbit cameras of the same size, deterministic for a given (rank, world)."""
+def rank_cameras(cameras, rank, world, config=None, seed=0):
+    """Views rendered by `rank` of `world` (weak scaling: every rank does the
+    single-GPU workload's amount of work).  Rank 0 keeps the workload's own
+    cameras; rank k > 0 gets view set k of the same configuration
+    (synthetic.config_cameras): the same count, sizes and distance
+    distribution, other seeded positions.  Without a configuration name,
+    rank k gets seeded orbit cameras of the first camera's size."""
     if world <= 1 or rank == 0:
         return list(cameras)
     from . import synthetic
     n = len(cameras)
-    extra = synthetic.orbit_cameras(n * world, seed, radius=(1.5, 2.0),
+    if config is not None:
+        return synthetic.config_cameras(config, seed, view_set=rank)[:n]
+    extra = synthetic.orbit_cameras(n * world, 1007 + seed, radius=(1.5, 2.0),
                                     fixed_size=(cameras[0].width, cameras[0].height))
     return extra[rank * n:(rank + 1) * n]
 
@@ -331,19 +335,18 @@ class BatchedWorkload:
         L = lib()
         g = self.grads
         g[0].zero_()
-        g[1].zero_()
         p = lambda t: ctypes.c_void_p(t.data_ptr())
         s = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
         check(L.svr_batch_backward(r.plan, p(r.ws), p(self.centers), p(self.lengths), p(self.geos),
                                    int(self.geos.dtype == torch.bfloat16), p(self.T), p(self.dC), p(self.dT),
-                                   p(g[0]), p(g[1]), s), "batch_backward")
+                                   p(g[0]), s), "batch_backward")
 
     def _bwd_sh(self):
         r = self.raster
         g = self.grads
         p = lambda t: ctypes.c_void_p(t.data_ptr())
         s = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
-        check(lib().svr_batch_sh_backward(r.plan, p(r.ws), p(self.centers), 3, 16, p(g[2]), p(g[3]), s),
+        check(lib().svr_batch_sh_backward(r.plan, p(r.ws), p(self.centers), 3, 16, p(g[2]), p(g[3]), p(g[1]), s),
               "batch_sh_backward")
 
     def capture(self):
@@ -516,6 +519,22 @@ class GradientExchange:
             self.dist.all_reduce(loss, group=self.group)
             loss.mul_(1.0 / self.world)
 
+    def start(self, bucket):
+        """Start the sum all-reduce of one bucket without waiting for it (with
+        NCCL it runs on the collective stream once the work already queued on
+        the current stream is done, overlapping what is queued after it)."""
+        if self.world == 1:
+            return None
+        return self.dist.all_reduce(bucket, group=self.group, async_op=True)
+
+    def finish(self, pending):
+        """Wait for started buckets ([(work, bucket)], the current stream waits
+        on the collective stream) and turn their sums into means."""
+        for work, bucket in pending:
+            if work is not None:
+                work.wait()
+                bucket.mul_(1.0 / self.world)
+
 
 class BatchedTrainWorkload:
     """One training step over all views: batched projection + SH, binning,
@@ -523,18 +542,35 @@ class BatchedTrainWorkload:
     fused Adam update of densities and SH (bf16 storage, fp32 moments);
     capturable as one CUDA graph (the step count lives on the device).
 
+    With ``grid`` (vox_key [P,8], grid values [M]) the trained densities are
+    grid points: gathered into the [P,8] corner buffer at the start of the
+    step, their gradient scattered back after the compositing backward (the
+    reference's GatherGeoParams around its rasterizer, once per step for all
+    views).
+
     With ``exchange`` (a GradientExchange over several ranks) each rank
-    renders its own views and the step becomes: graph (forward + backward) ->
-    all-reduce of the flat gradient buffer -> graph (Adam)."""
+    renders its own views and the step becomes: graph (forward + compositing
+    backward) -> start the all-reduce of the density gradients -> graph (SH
+    backward, overlapping that all-reduce) -> all-reduce of the SH gradients
+    and the loss -> graph (Adam)."""
 
     def __init__(self, scene, dev, storage=torch.bfloat16, lr_geo=0.025, lr_sh=0.01, betas=(0.1, 0.99),
-                 eps=1e-15, tune=True, exchange=None):
-        from .batched import BatchedRasterizer
+                 eps=1e-15, tune=True, exchange=None, grid=None):
+        from .batched import BatchedRasterizer, gather_grid_geos
         self.sc, self.dev, self.P = scene, dev, scene.n_voxels
         self.octpath = _t(scene.octpath.reshape(-1, 1), dev, torch.int64)
         self.centers = _t(scene.centers, dev)
         self.lengths = _t(scene.lengths, dev)
-        self.geos = _t(scene.geos, dev).to(storage).contiguous()
+        # densities: per-voxel corners, or (grid = (vox_key [P,8], grid values [M])) grid points
+        # gathered into the [P,8] corner buffer every step, as the reference trains them
+        self.grid = None
+        if grid is not None:
+            self.vox_key = grid[0].to(dev).contiguous()
+            self.grid = _t(grid[1], dev).to(storage).contiguous()
+            self.geos = torch.empty(self.P, 8, dtype=storage, device=dev)
+            gather_grid_geos(self.vox_key, self.grid, self.geos)
+        else:
+            self.geos = _t(scene.geos, dev).to(storage).contiguous()
         self.sh0 = _t(scene.sh0, dev).to(storage).contiguous()
         self.shs = _t(scene.shs, dev).to(storage).contiguous()
         self.cams = [_DevCam(c, dev) for c in scene.cameras]
@@ -555,27 +591,50 @@ class BatchedTrainWorkload:
         self.dT = torch.zeros(r.n_pixels, device=dev)
         self.dC = torch.zeros_like(self.color)
         self.loss = torch.zeros((), device=dev)
-        # one flat buffer for the exchanged gradients: densities, sh0, shs (then subdiv, not exchanged)
+        # one flat buffer for the exchanged gradients: densities (per-voxel corners or grid
+        # points), sh0, shs; the subdivision priority is not exchanged
         P = self.P
-        self.flat_grad = torch.zeros(P * (8 + 3 + 45), device=dev)
-        self.grads = (self.flat_grad[:8 * P].view(P, 8), torch.zeros(P, device=dev),
-                      self.flat_grad[8 * P:11 * P].view(P, 3), self.flat_grad[11 * P:].view(P, 15, 3))
-        self.adam = DeviceAdam([self.geos, self.sh0, self.shs], [lr_geo, lr_sh, lr_sh], betas, eps)
+        self.n_dens = 8 * P if self.grid is None else self.grid.numel()
+        nd = self.n_dens
+        self.flat_grad = torch.zeros(nd + P * (3 + 45), device=dev)
+        dgeo = self.flat_grad[:nd].view(P, 8) if self.grid is None else torch.zeros(P, 8, device=dev)
+        self.grads = (dgeo, torch.zeros(P, device=dev), self.flat_grad[nd:nd + 3 * P].view(P, 3),
+                      self.flat_grad[nd + 3 * P:].view(P, 15, 3))
+        dens = self.geos if self.grid is None else self.grid
+        self.adam_grads = [self.flat_grad[:nd].view(dens.shape), self.grads[2], self.grads[3]]
+        self.adam = DeviceAdam([dens, self.sh0, self.shs], [lr_geo, lr_sh, lr_sh], betas, eps)
         self.exchange = exchange if (exchange is not None and exchange.world > 1) else None
         self.graph = None
+        self.graph_sh = None
         self.graph_adam = None
 
-    def _forward_backward(self):
+    def _forward_backward_render(self):
+        from .batched import gather_grid_geos, scatter_grid_grad
         r = self.raster
+        if self.grid is not None:
+            gather_grid_geos(self.vox_key, self.grid, self.geos)
         r.prepare(self.sh0, self.shs, 3)
         r.render(self.geos, self.color, self.T)
         diff = self.color - self.target
         torch.mul(self.scale, diff, out=self.dC)
         self.loss.copy_((self.dC * diff).sum() * 0.5)  # mean over views of MSE (scale = 2 / (N_v V))
-        r.backward(self.geos, self.T, self.dC, self.dT, 3, 16, grads=self.grads)
+        self.grads[0].zero_()
+        r.backward_render(self.geos, self.T, self.dC, self.dT, self.grads[0])
+        if self.grid is not None:
+            dgrid = self.flat_grad[:self.n_dens]
+            dgrid.zero_()
+            scatter_grid_grad(self.vox_key, self.grads[0], dgrid)
+
+    def _backward_sh(self):
+        g = self.grads
+        self.raster.backward_sh(3, 16, g[2], g[3], g[1])
+
+    def _forward_backward(self):
+        self._forward_backward_render()
+        self._backward_sh()
 
     def _adam(self):
-        self.adam.step([self.grads[0], self.grads[2], self.grads[3]])
+        self.adam.step(self.adam_grads)
 
     def _step(self):
         self._forward_backward()
@@ -593,30 +652,35 @@ class BatchedTrainWorkload:
                 self._step()
             self.graph = g
         else:
-            # the collective stays outside the graphs: forward + backward, then Adam
-            g = torch.cuda.CUDAGraph()
+            # the collectives stay outside the graphs: forward + compositing
+            # backward, SH backward, Adam
+            g, gs, ga = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
-                self._forward_backward()
-            ga = torch.cuda.CUDAGraph()
+                self._forward_backward_render()
+            with torch.cuda.graph(gs):
+                self._backward_sh()
             with torch.cuda.graph(ga):
                 self._adam()
-            self.graph, self.graph_adam = g, ga
+            self.graph, self.graph_sh, self.graph_adam = g, gs, ga
 
     def replay(self):
         """One training step from the captured graph(s)."""
         self.graph.replay()
         if self.exchange is not None:
-            self.exchange(self.flat_grad, self.loss)
+            dens, sh = self.flat_grad[:self.n_dens], self.flat_grad[self.n_dens:]
+            w_dens = self.exchange.start(dens)       # densities are final: exchange them ...
+            self.graph_sh.replay()                   # ... while the SH backward runs
+            pending = [(w_dens, dens), (self.exchange.start(sh), sh), (self.exchange.start(self.loss), self.loss)]
+            self.exchange.finish(pending)
             self.graph_adam.replay()
 
     def _eager_probe(self):
         # one forward/backward without the optimizer update, so parameters are untouched
-        r = self.raster
-        r.prepare(self.sh0, self.shs, 3)
-        r.render(self.geos, self.color, self.T)
-        diff = self.color - self.target
-        torch.mul(self.scale, diff, out=self.dC)
-        r.backward(self.geos, self.T, self.dC, self.dT, 3, 16, grads=self.grads)
+        self._forward_backward()
+
+    def release(self):
+        """Drop the captured graphs (before the process group is destroyed)."""
+        self.graph = self.graph_sh = self.graph_adam = None
 
     def run(self, steps):
         if self.graph is None:
@@ -640,26 +704,37 @@ class PlainTrainWorkload:
     """The same training step in the reference's form: fp32 parameters, one
     view per call with its host syncs (visible-index and instance-count
     reads), gradients accumulated over the views, then SparseAdam's
-    per-parameter launches with host-side bias correction."""
+    per-parameter launches with host-side bias correction.  With ``grid``
+    (vox_key, grid values) the densities are grid points gathered per view
+    through GatherGeoParams, as the reference's model does."""
 
-    def __init__(self, scene, dev, lr_geo=0.025, lr_sh=0.01, betas=(0.1, 0.99), eps=1e-15):
+    def __init__(self, scene, dev, lr_geo=0.025, lr_sh=0.01, betas=(0.1, 0.99), eps=1e-15, grid=None):
         from .sparse_adam import SparseAdam
         self.sc, self.dev, self.P = scene, dev, scene.n_voxels
         self.octpath = _t(scene.octpath.reshape(-1, 1), dev, torch.int64)
         self.centers = _t(scene.centers, dev)
         self.lengths = _t(scene.lengths, dev)
-        self.geos = _t(scene.geos, dev).requires_grad_(True)
+        self.grid = None
+        if grid is not None:  # grid-point densities through GatherGeoParams (sparse_voxel_gears/renderer.py)
+            self.vox_key = grid[0].to(dev).contiguous()
+            self.care_idx = torch.arange(self.P, device=dev)
+            self.grid = _t(grid[1], dev).reshape(-1, 1).requires_grad_(True)
+            self.geos = None
+        else:
+            self.geos = _t(scene.geos, dev).requires_grad_(True)
         self.sh0 = _t(scene.sh0, dev).requires_grad_(True)
         self.shs = _t(scene.shs, dev).requires_grad_(True)
         self.cams = [(c, _t(c.w2c, dev), _t(c.c2w, dev)) for c in scene.cameras]
         self.targets = [_t(t, dev) for t in scene.targets]
-        self.opt = SparseAdam([{"params": [self.geos], "lr": lr_geo}, {"params": [self.sh0], "lr": lr_sh},
+        dens = self.geos if self.grid is None else self.grid
+        self.opt = SparseAdam([{"params": [dens], "lr": lr_geo}, {"params": [self.sh0], "lr": lr_sh},
                                {"params": [self.shs], "lr": lr_sh}], betas=betas, eps=eps)
 
     def _step(self):
         from . import renderer
-        for p in (self.geos, self.sh0, self.shs):
-            p.grad = None
+        for p in (self.geos, self.grid, self.sh0, self.shs):
+            if p is not None:
+                p.grad = None
         total = None
         nv = len(self.cams)
         ones = torch.ones(self.P, 1, device=self.dev)
@@ -669,7 +744,9 @@ class PlainTrainWorkload:
 
             def vox_fn(idx, cam_pos, mode):
                 rg = renderer.SH_eval.apply(3, idx, self.centers, cam_pos, None, self.sh0, self.shs)
-                return {"geos": self.geos, "rgbs": rg, "subdiv_p": ones}
+                geos = self.geos if self.grid is None else \
+                    renderer.GatherGeoParams.apply(self.vox_key, self.care_idx, self.grid)
+                return {"geos": geos, "rgbs": rg, "subdiv_p": ones}
 
             color, _, _, _, _ = renderer.rasterize_voxels(s, self.octpath, self.centers, self.lengths, vox_fn)
             loss = ((color - self.targets[i % len(self.targets)]) ** 2).mean() / nv

@@ -1,5 +1,6 @@
 """GPU tests of the multi-view batched path: per view it must reproduce the
-plain path (bit-identical images and contributor counts in fp32 storage),
+plain path (bit-identical images and contributor counts in fp32 storage
+with the exact arithmetic; within fp32 accumulation error with the fast one),
 gradients summed over views must match the plain per-view sums, bf16 storage
 must stay within the PSNR budget of the FP64 oracle, the CUDA-graph replay
 must equal eager execution, and capacity overflow must be reported, not
@@ -60,7 +61,7 @@ def test_batched_forward_equals_plain(c1, max_key_bits, binning, monkeypatch):
     if max_key_bits:
         # 32 position bits + 8 bits for one view's tiles: one sort group per view
         monkeypatch.setenv("SVR_MAX_KEY_BITS", str(max_key_bits))
-    r, _ = _raster(c1)
+    r, _ = _raster(c1, exact=True)
     r.set_binning(binning)
     if max_key_bits:
         assert r.n_groups == 3
@@ -111,7 +112,8 @@ def test_large_tile_segments_match_plain_sort(binning):
     cams = [synthetic.make_camera(16, 16, 70.0, (0.3, -0.4, 3.2)), synthetic.make_camera(48, 40, 60.0, (0.0, 2.0, 2.5)),
             synthetic.make_camera(64, 64, 90.0, (2.2, 0.5, -1.8))]
     C = SceneTensors(dataclasses.replace(sc, cameras=cams))
-    r = BatchedRasterizer([DevCam(c) for c in cams], C.octpath, C.centers, C.lengths, max_level=sc.max_level)
+    r = BatchedRasterizer([DevCam(c) for c in cams], C.octpath, C.centers, C.lengths, max_level=sc.max_level,
+                          exact=True)
     r.set_binning(binning)
     r.fit_capacity(C.sh0, C.shs, 3)
     r.prepare(C.sh0, C.shs, 3)
@@ -170,6 +172,45 @@ def test_batched_backward_equals_plain_sum(c1):
     assert rel_err(geos.grad, geos2.grad) < 1e-5
     assert rel_err(sh0.grad, sh02.grad) < 1e-5
     assert rel_err(shs.grad, shs2.grad) < 1e-5
+
+
+@pytest.mark.parametrize("views", [(0, 1, 2), "c3"])
+def test_fast_arithmetic_matches_exact(c1, views):
+    """The default fast compositing arithmetic (hardware exponential,
+    approximate division) against the exact form that is bit-identical to the
+    plain path: images within 1e-5 norm-wise (a pixel whose transmittance
+    lands on the early-stop threshold may take one voxel more or less, at most
+    about 1e-4 of colour), contributor counts equal almost everywhere, and
+    gradients within 1e-5."""
+    if views == "c3":
+        C = SceneTensors(synthetic.cached_config_scene("c3"))
+        cams = [DevCam(C.scene.cameras[i]) for i in (0, 5)]
+    else:
+        C = c1
+        cams = [DevCam(C.scene.cameras[i]) for i in views]
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(13)
+    for exact in (True, False):
+        r = BatchedRasterizer(cams, C.octpath, C.centers, C.lengths, max_level=C.scene.max_level, tile_size=8,
+                              exact=exact)
+        if "wC" not in out:
+            out["wC"] = torch.randn(3 * r.n_pixels, device="cuda", generator=g) * 1e-3
+            out["wT"] = torch.randn(r.n_pixels, device="cuda", generator=g) * 1e-3
+        res = _render_and_grads(r, C, out["wC"], out["wT"])
+        out[exact] = res + (r.arrays()["n_contrib"].clone(),)
+        del r
+    e, f = out[True], out[False]
+    img_rel = rel_err(f[0], e[0])
+    img_max = (f[0] - e[0]).abs().max().item()
+    nc_mism = (f[7] != e[7]).float().mean().item()
+    grads = {name: rel_err(a, b) for a, b, name in zip(f[2:6], e[2:6], ("dL_dgeos", "subdiv", "dL_dsh0", "dL_dshs"))}
+    print(f"fast vs exact ({views}): image rel {img_rel:.2e}, max {img_max:.2e}, n_contrib mismatch {nc_mism:.2e}, "
+          + ", ".join(f"{k} {v:.2e}" for k, v in grads.items()))
+    assert img_rel < 1e-5 and img_max < 2e-4
+    assert rel_err(f[1], e[1]) < 1e-5
+    assert nc_mism < 1e-3
+    for k, v in grads.items():
+        assert v < 1e-5, k
 
 
 def _psnr(a, b):
@@ -273,6 +314,26 @@ def test_training_step_graph_matches_plain_form():
         assert abs(x - y) / y < 1e-4
     assert rel_err(b.geos.float(), p.geos.detach()) < 1e-4
     assert rel_err(b.shs.float(), p.shs.detach()) < 1e-4
+
+
+def test_training_grid_step_graph_matches_plain_form():
+    """Training grid points (the reference's parametrisation): the captured
+    batched step (gather, render, backward, scatter, fused Adam over the grid
+    and SH) tracks the plain per-view step with GatherGeoParams + SparseAdam."""
+    from sv_raster_b200.workload import BatchedTrainWorkload, PlainTrainWorkload
+    sc = synthetic.config_scene("c1")
+    sc.targets = [np.random.default_rng(4).uniform(0, 1, (3, c.height, c.width)).astype(np.float32)
+                  for c in sc.cameras]
+    dev = torch.device("cuda")
+    grid = synthetic.grid_params(sc, dev)
+    b = BatchedTrainWorkload(sc, dev, storage=torch.float32, tune=False, grid=grid)
+    _, lb = b.run(3)
+    p = PlainTrainWorkload(sc, dev, grid=grid)
+    _, lp = p.run(3)
+    assert lb[2] < lb[0]
+    for x, y in zip(lb, lp):
+        assert abs(x - y) / y < 1e-4
+    assert rel_err(b.grid.float(), p.grid.detach().reshape(-1)) < 1e-4
 
 
 def _render_and_grads(r, C, wC, wT):

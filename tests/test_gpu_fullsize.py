@@ -7,8 +7,8 @@ that do not depend on the size (the oracle is too slow at these sizes):
   counting sort and the radix grouping produce the same instance array;
   images and T are bit-identical between 8x8 and 16x16 tiles; the backward is
   linear in the upstream gradient; no device error flag is raised.
-* c3 (2M voxels, 16 uneven views): every view of the batched path is
-  bit-identical to the plain per-view path (fp32 storage).
+* c3 (2M voxels, 16 uneven views): every view of the batched path (exact
+  arithmetic) is bit-identical to the plain per-view path (fp32 storage).
 """
 import numpy as np
 import pytest
@@ -136,7 +136,7 @@ def test_c3_fullsize_batched_views_equal_plain():
     sc = _scene("c3")
     C = SceneTensors(sc)
     cams = [DevCam(c) for c in sc.cameras]
-    r = BatchedRasterizer(cams, C.octpath, C.centers, C.lengths, max_level=sc.max_level, tile_size=8)
+    r = BatchedRasterizer(cams, C.octpath, C.centers, C.lengths, max_level=sc.max_level, tile_size=8, exact=True)
     r.fit_capacity(C.sh0, C.shs, 3)
     r.prepare(C.sh0, C.shs, 3)
     color, T = r.render(C.geos)
