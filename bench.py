@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--tile", default=None,
                     help="batched mode: fixed compositing tile 'TS' or 'TS,SB' (8,64 | 16,128|256|512 | 32,256); "
                          "no autotuning")
+    ap.add_argument("--exact", action="store_true",
+                    help="batched mode: the exact compositing arithmetic (bit-identical to the plain path) instead "
+                         "of the default fast form")
     ap.add_argument("--train", action="store_true",
                     help="training-step workload (fwd + bwd + fused Adam, graph-captured) vs the plain fp32 form")
     ap.add_argument("--plain-steps", type=int, default=10, help="steps of the plain form in --train mode")
@@ -181,7 +184,7 @@ def main():
         if args.tile:
             parts = [int(x) for x in args.tile.split(",")]
             tile = (parts[0], parts[1] if len(parts) > 1 else (64 if parts[0] == 8 else 256))
-        wl = workload.BatchedWorkload(sc, dev, tune=not (args.no_tune or tile), tile=tile)
+        wl = workload.BatchedWorkload(sc, dev, tune=not (args.no_tune or tile), tile=tile, exact=args.exact)
     n_views = len(sc.cameras)
 
     for _ in range(args.warmup):
@@ -281,6 +284,7 @@ def main():
             "config": {"workload": f"{args.config}: {sc.n_voxels} voxels, {n_views} views/rank "
                                    f"{sc.cameras[0].width}x{sc.cameras[0].height}, SH3, fwd+recompute bwd",
                        "mode": args.mode, "l2": l2_note(sc, args.mode),
+                       "arithmetic": ("exact" if args.exact or args.mode == "plain" else "fast"),
                        "instances_per_view": inst_per_view,
                        "scene_file": os.path.basename(scene_file(args))},
             "autotuned": tuned,

@@ -78,7 +78,7 @@ def cache_key(raster, geos, sh0):
     name = torch.cuda.get_device_name(dev) if dev.type == "cuda" else "cpu"
     sizes = ",".join(f"{w}x{h}" for h, w in raster.sizes)
     return (f"v{CACHE_SCHEMA}|{name}|P={raster.P}|views={sizes}|ns={raster.n_samp}|geo={geos.dtype}"
-            f"|sh={sh0.dtype}")
+            f"|sh={sh0.dtype}|arith={'exact' if getattr(raster, 'exact', False) else 'fast'}")
 
 
 def time_ms(fn, reps=5, warmup=2, stream=None):

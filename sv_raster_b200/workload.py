@@ -250,7 +250,7 @@ class BatchedWorkload:
     fp32 compositing / gradients, no host sync inside a step (the step is
     also captured as a CUDA graph)."""
 
-    def __init__(self, scene, dev, storage=torch.bfloat16, graph=True, tune=True, tile=None):
+    def __init__(self, scene, dev, storage=torch.bfloat16, graph=True, tune=True, tile=None, exact=False):
         from .batched import BatchedRasterizer
         self.sc = scene
         self.dev = dev
@@ -263,7 +263,7 @@ class BatchedWorkload:
         self.shs = _t(scene.shs, dev).to(storage).contiguous()
         self.cams = [_DevCam(c, dev) for c in scene.cameras]
         self.raster = BatchedRasterizer(self.cams, self.octpath, self.centers, self.lengths,
-                                        max_level=scene.max_level)
+                                        max_level=scene.max_level, exact=exact)
         self.tuned = None
         if tile is not None:
             self.raster.set_tile_size(*tile)
