@@ -70,7 +70,7 @@ def _store_cache(path, data):
 
 # Bumped whenever the search space or the kernels behind it change, so that
 # choices cached by an older build are measured again rather than reused.
-CACHE_SCHEMA = 2
+CACHE_SCHEMA = 3
 
 
 def cache_key(raster, geos, sh0):
