@@ -307,7 +307,7 @@ def build_scene(name, n_voxels, seed, kind, surf_levels, bg_levels, geo_mu, geo_
     return Scene(name, path, lv, centers, lengths, geos, sh0, shs, cameras, targets)
 
 
-def _unit(rng):
+def _unit_dir(rng):
     d = rng.standard_normal(3)
     return d / np.linalg.norm(d)
 
@@ -324,10 +324,10 @@ def config_cameras(name, seed=0, view_set=0):
             return [make_camera(256, 256, 50.0, (0.0, 0.0, -1.5)), make_camera(256, 256, 50.0, d1 * 1.5),
                     # inside the sphere shell: voxels straddle the camera's axis planes (multi-quadrant)
                     make_camera(200, 136, 70.0, (0.03, -0.02, 0.01), target=(0.4, 0.1, 0.3))]
-        return [make_camera(256, 256, 50.0, _unit(rng) * 1.5), make_camera(256, 256, 50.0, _unit(rng) * 1.5),
-                make_camera(200, 136, 70.0, _unit(rng) * 0.03, target=_unit(rng) * 0.5)]
+        return [make_camera(256, 256, 50.0, _unit_dir(rng) * 1.5), make_camera(256, 256, 50.0, _unit_dir(rng) * 1.5),
+                make_camera(200, 136, 70.0, _unit_dir(rng) * 0.03, target=_unit_dir(rng) * 0.5)]
     if name == "c2":
-        d = np.array([0.6, -0.5, -1.2]) if view_set == 0 else _unit(rng)
+        d = np.array([0.6, -0.5, -1.2]) if view_set == 0 else _unit_dir(rng)
         return [make_camera(1297, 840, 50.0, d / np.linalg.norm(d) * 1.6)]
     if name == "c3":
         return orbit_cameras(16, seed + 10 + 7919 * view_set)
