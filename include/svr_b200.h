@@ -277,6 +277,13 @@ int svr_batch_plan_set_reduction(svr_batch_plan* plan, int atomic_lanes);
  * form to fp32 accumulation error (a pixel may stop one voxel earlier or later
  * where its transmittance lands on the 1e-4 early-stop threshold). */
 int svr_batch_plan_set_arithmetic(svr_batch_plan* plan, int exact);
+/* Pixels per thread of the compositing kernels: 1 (default) or 2 (a warp
+ * covers an 8x8 block, each lane two pixels four rows apart; a record's
+ * shared-memory fields are read once for both and, in the backward, one warp
+ * reduction serves both).  Used with 8x8 tiles staging 32 or 64 records and
+ * 16x16 tiles staging 128 or 256; other tile configurations run one pixel
+ * per thread.  Images, T and contributor counts do not depend on it. */
+int svr_batch_plan_set_pixels_per_thread(svr_batch_plan* plan, int pixels);
 int64_t svr_batch_plan_pixels(const svr_batch_plan* plan);
 int64_t svr_batch_plan_tiles(const svr_batch_plan* plan);
 int svr_batch_plan_groups(const svr_batch_plan* plan);

@@ -18,6 +18,10 @@ gradients agree up to the order of floating-point additions):
 * ``reduce`` -- backward gradient reduction threshold: records touched by at
   most this many lanes of a warp add their gradients with shared-memory
   atomics instead of a warp reduce-scatter (``set_reduction``).
+* ``ppt`` -- pixels per compositing thread, 1 or 2 (two pixels of an 8x8
+  warp block share each record's loads and, in the backward, its warp
+  reduction; ``BatchedRasterizer.set_pixels_per_thread``), tuned with the
+  full step after the tile.
 * ``tile`` -- compositing tile size of the batched path (8, 16 or 32 pixels)
   with the voxel-staging depth (records staged into shared memory per round)
   (``BatchedRasterizer.set_tile_size``; the tile size changes the binning, so
@@ -41,6 +45,7 @@ DEFAULT_SPACE = {
     "fwd": [(True, 0), (False, 0)],
     "bwd": [(True, 0), (False, 0)],
     "reduce": [1, 2, 4, 8],
+    "ppt": [1, 2],
 }
 
 
@@ -70,7 +75,7 @@ def _store_cache(path, data):
 
 # Bumped whenever the search space or the kernels behind it change, so that
 # choices cached by an older build are measured again rather than reused.
-CACHE_SCHEMA = 3
+CACHE_SCHEMA = 4
 
 
 def cache_key(raster, geos, sh0):
@@ -110,6 +115,8 @@ def apply(raster, choice):
         raster.set_sort_buckets(*[int(x) for x in choice["sort"]])
     if "reduce" in choice:
         raster.set_reduction(int(choice["reduce"]))
+    if "ppt" in choice:
+        raster.set_pixels_per_thread(int(choice["ppt"]))
     f = choice.get("fwd", (True, 0))
     b = choice.get("bwd", (True, 0))
     raster.set_schedule(fwd_ordered=bool(f[0]), bwd_ordered=bool(b[0]), fwd_ctas_per_sm=int(f[1]),
@@ -165,8 +172,8 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
         dC, dT = upstream()
         state["grads"] = raster.backward(geos, state["out"][1], dC, dT, sh_degree, M, state.get("grads"))
 
-    stages = [("tile", step), ("bin", prepare), ("sort", prepare), ("fwd", render), ("bwd", backward),
-              ("reduce", backward)]
+    stages = [("tile", step), ("ppt", step), ("bin", prepare), ("sort", prepare), ("fwd", render),
+              ("bwd", backward), ("reduce", backward)]
     for name, fn in stages:
         cands = space.get(name)
         if not cands:

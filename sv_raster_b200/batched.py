@@ -58,6 +58,7 @@ class BatchedRasterizer:
         self.atomic_lanes = 1
         self.binning = 1
         self.exact = bool(exact)
+        self.pixels_per_thread = 1
         self._make_plan(0 if capacity is None else int(capacity))
         self.capacity_auto = capacity is None
 
@@ -83,6 +84,8 @@ class BatchedRasterizer:
         check(L.svr_batch_plan_set_reduction(plan, self.atomic_lanes), "batch_plan_set_reduction")
         check(L.svr_batch_plan_set_binning(plan, self.binning), "batch_plan_set_binning")
         check(L.svr_batch_plan_set_arithmetic(plan, int(self.exact)), "batch_plan_set_arithmetic")
+        check(L.svr_batch_plan_set_pixels_per_thread(plan, self.pixels_per_thread),
+              "batch_plan_set_pixels_per_thread")
 
     def set_binning(self, binning=1):
         """How prepare groups the instances by tile before the per-tile sort:
@@ -105,6 +108,13 @@ class BatchedRasterizer:
         loops (see svr_batch_plan_set_arithmetic)."""
         check(lib().svr_batch_plan_set_arithmetic(self.plan, int(bool(exact))), "batch_plan_set_arithmetic")
         self.exact = bool(exact)
+
+    def set_pixels_per_thread(self, pixels=1):
+        """Pixels per compositing thread, 1 or 2 (see
+        svr_batch_plan_set_pixels_per_thread); results do not depend on it
+        beyond the order of gradient additions."""
+        check(lib().svr_batch_plan_set_pixels_per_thread(self.plan, int(pixels)), "batch_plan_set_pixels_per_thread")
+        self.pixels_per_thread = int(pixels)
 
     def set_tile_size(self, tile_size, staging=None):
         """Compositing tile size (8, 16 or 32 pixels) and records staged per

@@ -385,6 +385,7 @@ struct svr_batch_plan {
   int stage;                   // records staged per round (svr_batch_plan_set_staging)
   int atomic_lanes;            // backward reduction threshold (svr_batch_plan_set_reduction)
   int exact;                   // compositing arithmetic (svr_batch_plan_set_arithmetic): 1 exact, 0 fast
+  int pair;                    // two pixels per compositing thread (svr_batch_plan_set_pixels_per_thread)
   int binning;                 // 1: counting sort by tile, 0: radix over the tile bits (svr_batch_plan_set_binning)
   // workspace layout (byte offsets)
   size_t o_header, o_ndup, o_scan, o_bbox, o_quad, o_scan_tmp, o_rgbs, o_drgbs;
@@ -591,6 +592,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->seg_chunk = 4096;
   p->atomic_lanes = 1;
   p->exact = 0;
+  p->pair = 0;
   p->binning = 1;
   ensure_segsort_attributes();
   ensure_fwd_batch_attributes();
@@ -625,6 +627,12 @@ int svr_batch_plan_set_staging(svr_batch_plan* p, int stage) {
 }
 
 int svr_batch_plan_tile_size(const svr_batch_plan* p) { return p ? p->tile_size : 0; }
+
+int svr_batch_plan_set_pixels_per_thread(svr_batch_plan* p, int pixels) {
+  if (!p || (pixels != 1 && pixels != 2)) return SVR_ERR_SHAPE;
+  p->pair = pixels == 2;
+  return SVR_OK;
+}
 
 int svr_batch_plan_set_arithmetic(svr_batch_plan* p, int exact) {
   if (!p || (exact != 0 && exact != 1)) return SVR_ERR_SHAPE;
@@ -788,7 +796,7 @@ int svr_batch_render(svr_batch_plan* p, void* ws, const float* vox_centers, cons
   const bool ordered = (p->order_flags & 1) != 0;
   if (ordered) build_tile_order(p, q, nullptr, q.order_fwd, stream);
   launch_render_fwd_batch(p->vt, (int)p->total_tiles, q.ranges, p->cap > 0 ? q.vb : nullptr, va, (int)p->P,
-                          (size_t)p->P * 3, out, p->n_samp, p->tile_size, p->stage, !p->exact,
+                          (size_t)p->P * 3, out, p->n_samp, p->tile_size, p->stage, !p->exact, p->pair,
                           ordered ? q.order_fwd : nullptr, q.header + 2, p->fwd_ctas_per_sm, stream);
   return check_last();
 }
@@ -812,8 +820,8 @@ int svr_batch_backward(svr_batch_plan* p, void* ws, const float* vox_centers, co
   if (ordered) build_tile_order(p, q, q.tile_last, q.order_bwd, stream);
   launch_render_bwd_batch(p->vt, (int)p->total_tiles, q.ranges, q.tile_last, p->cap > 0 ? q.vb : nullptr, va,
                           (int)p->P, (size_t)p->P * 3, (size_t)p->P * 4, in, out, p->n_samp, p->tile_size,
-                          p->stage, !p->exact, ordered ? q.order_bwd : nullptr, q.header + 3, p->bwd_ctas_per_sm,
-                          stream);
+                          p->stage, !p->exact, p->pair, ordered ? q.order_bwd : nullptr, q.header + 3,
+                          p->bwd_ctas_per_sm, stream);
   return check_last();
 }
 

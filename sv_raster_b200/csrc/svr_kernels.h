@@ -73,21 +73,22 @@ void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t
 // grids taking tiles from `counter` (zeroed here) in the order of `order`
 // (identity when null); ctas_per_sm caps the resident CTAs per SM (0 = as
 // many as fit).  (tile, stage) must satisfy batch_tile_supported.
+bool batch_pair_supported(int tile, int stage);
 bool batch_tile_supported(int tile, int stage);
 void ensure_fwd_batch_attributes();
 void ensure_bwd_batch_attributes();
 void launch_render_fwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* vals, const VoxelArrays& va, int P, size_t rgb_view_stride,
-                             const FwdTileOut& out, int ns, int tile, int stage, bool fast, const uint32_t* order,
-                             uint32_t* counter, int ctas_per_sm, cudaStream_t stream);
+                             const FwdTileOut& out, int ns, int tile, int stage, bool fast, int pair,
+                             const uint32_t* order, uint32_t* counter, int ctas_per_sm, cudaStream_t stream);
 void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t* tile_last, const uint32_t* vals,
                        const VoxelArrays& va, const BwdTileIn& in, const BwdTileOut& out, int ns, bool depth,
                        bool dist, bool normal, const uint32_t* order, cudaStream_t stream);
 void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
                              size_t rgb_view_stride, size_t drgb_view_stride, const BwdTileIn& in,
-                             const BwdTileOut& out, int ns, int tile, int stage, bool fast, const uint32_t* order,
-                             uint32_t* counter, int ctas_per_sm, cudaStream_t stream);
+                             const BwdTileOut& out, int ns, int tile, int stage, bool fast, int pair,
+                             const uint32_t* order, uint32_t* counter, int ctas_per_sm, cudaStream_t stream);
 // Grid of a persistent launch: resident CTAs of `kernel` on this device
 // (capped at ctas_per_sm per SM when > 0), at most n_items.
 int persistent_grid(const void* kernel, int threads, size_t dyn_smem, int n_items, int ctas_per_sm);

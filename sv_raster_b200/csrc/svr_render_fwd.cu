@@ -6,6 +6,7 @@
 
 #include "svr_kernels.h"
 #include "svr_render_fwd.cuh"
+#include "svr_render_pair.cuh"
 
 namespace svr {
 
@@ -107,6 +108,38 @@ render_fwd_batch_kernel(const __grid_constant__ FwdBatchArgs a) {
   }
 }
 
+// The same persistent form with two pixels per thread (svr_render_pair.cuh).
+template <class CFG, int NS, bool FAST>
+__global__ void __launch_bounds__(CFG::NT, pair_min_blocks<CFG>())
+render_fwd_batch_pair_kernel(const __grid_constant__ FwdBatchArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FwdBatchSmem<CFG>& sm = *reinterpret_cast<FwdBatchSmem<CFG>*>(smem_raw);
+  for (;;) {
+    if (threadIdx.x == 0) sm.item = atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const uint32_t k = sm.item;
+    if (k >= (uint32_t)a.n_items) break;
+    const int item = a.order ? (int)a.order[k] : (int)k;
+    const int view = view_of_tile(a.views, item);
+    const ViewParams& vp = a.views.v[view];
+    if (threadIdx.x < 12) sm.c2w[threadIdx.x] = vp.c2w[threadIdx.x];
+    __syncthreads();
+    const int local = item - (int)vp.tile_base;
+    const int tile_x = local % vp.grid_x, tile_y = local / vp.grid_x;
+    VoxelArrays va = a.va;
+    va.bboxes = a.va.bboxes + (size_t)view * a.P;
+    va.rgbs = a.va.rgbs + (size_t)view * a.rgb_view_stride;
+    FwdTileOut o = a.out;
+    o.tile_last = a.out.tile_last + vp.tile_base;
+    o.n_contrib = a.out.n_contrib + vp.pix_base;
+    o.color = a.out.color + 3 * (size_t)vp.pix_base;
+    o.T = a.out.T + vp.pix_base;
+    render_tile_fwd_pair<CFG, NS, FAST>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.vals, va, o,
+                                        o.tile_last + local, sm.s, sm.red);
+    __syncthreads();
+  }
+}
+
 #define SVR_FWD_DISPATCH(KERNEL, GRID, STREAM, ...)                                                   \
   do {                                                                                                \
     const int _ns = ns;                                                                               \
@@ -143,10 +176,26 @@ void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t
   SVR_FWD_DISPATCH(render_fwd_kernel, grid, stream, args);
 }
 
+// Tile configurations with a two-pixels-per-thread variant.
+bool batch_pair_supported(int tile, int stage) {
+  return (tile == 8 && (stage == 32 || stage == 64)) || (tile == 16 && (stage == 128 || stage == 256));
+}
+
 // Batched tile configurations: (tile size, staging depth).
 bool batch_tile_supported(int tile, int stage) {
   return (tile == 16 && (stage == 128 || stage == 256 || stage == 512)) ||
          (tile == 8 && (stage == 32 || stage == 64 || stage == 128)) || (tile == 32 && stage == 256);
+}
+
+template <class CFG>
+static void set_fwd_pair_attrs() {
+  const int smem = (int)sizeof(FwdBatchSmem<CFG>);
+  cudaFuncSetAttribute(render_fwd_batch_pair_kernel<CFG, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(render_fwd_batch_pair_kernel<CFG, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(render_fwd_batch_pair_kernel<CFG, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(render_fwd_batch_pair_kernel<CFG, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(render_fwd_batch_pair_kernel<CFG, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(render_fwd_batch_pair_kernel<CFG, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 template <class CFG, int NS>
@@ -176,6 +225,10 @@ void ensure_fwd_batch_attributes() {
     set_fwd_batch_attrs<TileCfg<8, 64>>();
     set_fwd_batch_attrs<TileCfg<8, 128>>();
     set_fwd_batch_attrs<TileCfg<32, 256>>();
+    set_fwd_pair_attrs<PairCfg<8, 32>>();
+    set_fwd_pair_attrs<PairCfg<8, 64>>();
+    set_fwd_pair_attrs<PairCfg<16, 128>>();
+    set_fwd_pair_attrs<PairCfg<16, 256>>();
   });
 }
 
@@ -191,6 +244,24 @@ static void launch_fwd_batch_arith(const FwdBatchArgs& args, int ns, int ctas_pe
   else go(render_fwd_batch_kernel<CFG, 3, FAST>);
 }
 
+template <class CFG, bool FAST>
+static void launch_fwd_pair_arith(const FwdBatchArgs& args, int ns, int ctas_per_sm, cudaStream_t stream) {
+  const size_t smem = sizeof(FwdBatchSmem<CFG>);
+  auto go = [&](auto kfn) {
+    const int grid = persistent_grid((const void*)kfn, CFG::NT, smem, args.n_items, ctas_per_sm);
+    kfn<<<grid, CFG::NT, smem, stream>>>(args);
+  };
+  if (ns == 1) go(render_fwd_batch_pair_kernel<CFG, 1, FAST>);
+  else if (ns == 2) go(render_fwd_batch_pair_kernel<CFG, 2, FAST>);
+  else go(render_fwd_batch_pair_kernel<CFG, 3, FAST>);
+}
+
+template <class CFG>
+static void launch_fwd_pair_cfg(const FwdBatchArgs& args, int ns, bool fast, int ctas_per_sm, cudaStream_t stream) {
+  if (fast) launch_fwd_pair_arith<CFG, true>(args, ns, ctas_per_sm, stream);
+  else launch_fwd_pair_arith<CFG, false>(args, ns, ctas_per_sm, stream);
+}
+
 template <class CFG>
 static void launch_fwd_batch_cfg(const FwdBatchArgs& args, int ns, bool fast, int ctas_per_sm, cudaStream_t stream) {
   if (fast) launch_fwd_batch_arith<CFG, true>(args, ns, ctas_per_sm, stream);
@@ -199,12 +270,19 @@ static void launch_fwd_batch_cfg(const FwdBatchArgs& args, int ns, bool fast, in
 
 void launch_render_fwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* vals, const VoxelArrays& va, int P, size_t rgb_view_stride,
-                             const FwdTileOut& out, int ns, int tile, int stage, bool fast, const uint32_t* order,
-                             uint32_t* counter, int ctas_per_sm, cudaStream_t stream) {
+                             const FwdTileOut& out, int ns, int tile, int stage, bool fast, int pair,
+                             const uint32_t* order, uint32_t* counter, int ctas_per_sm, cudaStream_t stream) {
   if (n_items <= 0) return;
   ensure_fwd_batch_attributes();
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
   const FwdBatchArgs args{views, n_items, ranges, vals, va, P, rgb_view_stride, out, order, counter};
+  if (pair && batch_pair_supported(tile, stage)) {
+    if (tile == 8 && stage == 32) launch_fwd_pair_cfg<PairCfg<8, 32>>(args, ns, fast, ctas_per_sm, stream);
+    else if (tile == 8) launch_fwd_pair_cfg<PairCfg<8, 64>>(args, ns, fast, ctas_per_sm, stream);
+    else if (stage == 128) launch_fwd_pair_cfg<PairCfg<16, 128>>(args, ns, fast, ctas_per_sm, stream);
+    else launch_fwd_pair_cfg<PairCfg<16, 256>>(args, ns, fast, ctas_per_sm, stream);
+    return;
+  }
   if (tile == 8 && stage == 32) launch_fwd_batch_cfg<TileCfg<8, 32>>(args, ns, fast, ctas_per_sm, stream);
   else if (tile == 8 && stage == 128) launch_fwd_batch_cfg<TileCfg<8, 128>>(args, ns, fast, ctas_per_sm, stream);
   else if (tile == 8) launch_fwd_batch_cfg<TileCfg<8, 64>>(args, ns, fast, ctas_per_sm, stream);

@@ -30,6 +30,9 @@ class FakeRaster:
     def set_binning(self, b):
         self.binning = b
 
+    def set_pixels_per_thread(self, n):
+        self.pixels_per_thread = n
+
     def set_schedule(self, fwd_ordered=True, bwd_ordered=True, fwd_ctas_per_sm=0, bwd_ctas_per_sm=0):
         self.schedule = (int(fwd_ordered) | (int(bwd_ordered) << 1), fwd_ctas_per_sm, bwd_ctas_per_sm)
 
@@ -61,6 +64,7 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
         t -= 0.5 * (r.schedule[2] == 3)
         t -= 0.25 * (getattr(r, "atomic_lanes", 1) == 4)
         t -= 0.125 * (getattr(r, "binning", 1) == 0)
+        t -= 0.0625 * (getattr(r, "pixels_per_thread", 1) == 2)
         return t
 
     geos = torch.zeros(r.P, 8)
@@ -77,7 +81,8 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
     assert r.schedule == (2, 0, 3)
     assert res["choice"]["reduce"] == 4 and r.atomic_lanes == 4
     assert res["choice"]["bin"] == 0 and r.binning == 0
-    assert set(res["timings"]) == {"tile", "bin", "sort", "fwd", "bwd", "reduce"}
+    assert res["choice"]["ppt"] == 2 and r.pixels_per_thread == 2
+    assert set(res["timings"]) == {"tile", "ppt", "bin", "sort", "fwd", "bwd", "reduce"}
     # second call: served from the cache, applied, no timing
     r2 = FakeRaster()
     res2 = autotune.tune_batched(r2, geos, sh0, shs, 3, timer=lambda *a: 1 / 0)

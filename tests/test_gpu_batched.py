@@ -53,15 +53,18 @@ def _raster(C, max_level=None, views=(0, 1, 2), **kw):
     return r, cams
 
 
-@pytest.mark.parametrize("binning", [1, 0])
+@pytest.mark.parametrize("binning,ppt", [(1, 1), (0, 1), (1, 2)])
 @pytest.mark.parametrize("max_key_bits", [None, 40])
-def test_batched_forward_equals_plain(c1, max_key_bits, binning, monkeypatch):
+def test_batched_forward_equals_plain(c1, max_key_bits, binning, ppt, monkeypatch):
     """Counting sort by tile (binning 1) and radix passes over the tile bits
-    (0, with one or several sort groups) give the plain path's tile lists."""
+    (0, with one or several sort groups) give the plain path's tile lists;
+    with the exact arithmetic images, T and contributor counts are the plain
+    path's with one or two pixels per compositing thread."""
     if max_key_bits:
         # 32 position bits + 8 bits for one view's tiles: one sort group per view
         monkeypatch.setenv("SVR_MAX_KEY_BITS", str(max_key_bits))
     r, _ = _raster(c1, exact=True)
+    r.set_pixels_per_thread(ppt)
     r.set_binning(binning)
     if max_key_bits:
         assert r.n_groups == 3
@@ -347,18 +350,23 @@ def _render_and_grads(r, C, wC, wT):
     return color.clone(), T.clone(), dgeo.clone(), sub.clone(), dsh0.clone(), dshs.clone(), total
 
 
-@pytest.mark.parametrize("tile,stage,order,ctas,buckets,lanes,binning", [
-    (8, 64, (True, True), (0, 0), (512, 4096), 4, 1),
-    (8, 32, (True, False), (0, 0), (256, 4096), 1, 0),
-    (8, 128, (False, True), (0, 0), (1024, 2048), 2, 1),
-    (32, 256, (True, True), (0, 0), (512, 4096), 1, 0),
-    (16, 128, (True, True), (0, 0), (256, 2048), 8, 1),
-    (16, 512, (False, False), (0, 0), (1024, 4096), 2, 0),
-    (16, 256, (False, True), (3, 2), (512, 2048), 32, 0),
+@pytest.mark.parametrize("tile,stage,order,ctas,buckets,lanes,binning,ppt", [
+    (8, 64, (True, True), (0, 0), (512, 4096), 4, 1, 1),
+    (8, 32, (True, False), (0, 0), (256, 4096), 1, 0, 1),
+    (8, 128, (False, True), (0, 0), (1024, 2048), 2, 1, 1),
+    (32, 256, (True, True), (0, 0), (512, 4096), 1, 0, 1),
+    (16, 128, (True, True), (0, 0), (256, 2048), 8, 1, 1),
+    (16, 512, (False, False), (0, 0), (1024, 4096), 2, 0, 1),
+    (16, 256, (False, True), (3, 2), (512, 2048), 32, 0, 1),
+    (8, 64, (True, True), (0, 0), (512, 4096), 1, 1, 2),
+    (8, 32, (False, True), (0, 0), (512, 4096), 4, 1, 2),
+    (16, 256, (True, False), (0, 0), (512, 4096), 1, 0, 2),
+    (16, 128, (True, True), (0, 0), (512, 4096), 32, 1, 2),
 ])
-def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas, buckets, lanes, binning):
-    """Every tile size, staging depth, compositing schedule and sort-bucket
-    setting the autotuner may pick renders bit-identical images and T (a pixel
+def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas, buckets, lanes, binning, ppt):
+    """Every tile size, staging depth, compositing schedule, sort-bucket
+    setting and pixels per thread the autotuner may pick renders
+    bit-identical images and T (a pixel
     sees the same instances in the same order) and the same gradients up to
     the order of the atomic additions."""
     g = torch.Generator(device="cuda").manual_seed(11)
@@ -373,6 +381,7 @@ def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas,
     r.set_sort_buckets(*buckets)
     r.set_reduction(lanes)
     r.set_binning(binning)
+    r.set_pixels_per_thread(ppt)
     got = _render_and_grads(r, c1, wC, wT)
     assert torch.equal(got[0], base[0]), "colour differs"
     assert torch.equal(got[1], base[1]), "T differs"
@@ -394,7 +403,7 @@ def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
     base = _render_and_grads(r0, c1, wC, wT)
     r, _ = _raster(c1)
     res = tune_batched(r, c1.geos, c1.sh0, c1.shs, 3, reps=2, warmup=1)
-    assert not res["cached"] and set(res["choice"]) == {"tile", "bin", "sort", "fwd", "bwd", "reduce"}
+    assert not res["cached"] and set(res["choice"]) == {"tile", "ppt", "bin", "sort", "fwd", "bwd", "reduce"}
     got = _render_and_grads(r, c1, wC, wT)
     assert torch.equal(got[0], base[0])
     assert rel_err(got[2], base[2]) < 1e-5

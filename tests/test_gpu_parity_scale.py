@@ -130,8 +130,8 @@ class _DevCam:
         self.c2w = torch.from_numpy(c.c2w).cuda()
 
 
-@pytest.mark.parametrize("exact", [True, False])
-def test_batched_bf16_c4_view_matches_reference_on_rounded_inputs(ref, exact):
+@pytest.mark.parametrize("exact,ppt", [(True, 1), (False, 1), (True, 2), (False, 2)])
+def test_batched_bf16_c4_view_matches_reference_on_rounded_inputs(ref, exact, ppt):
     """The batched step on one 1080p c4 view (bf16 storage, 8x8 tiles) against
     the reference run on the bf16-rounded parameters upcast to fp32.  With the
     exact arithmetic images and T are bitwise the reference's; with the fast
@@ -144,6 +144,7 @@ def test_batched_bf16_c4_view_matches_reference_on_rounded_inputs(ref, exact):
     sh016, shs16 = C.sh0.to(torch.bfloat16).contiguous(), C.shs.to(torch.bfloat16).contiguous()
     r = BatchedRasterizer([_DevCam(cam)], C.octpath, C.centers, C.lengths, max_level=sc.max_level, tile_size=8,
                           exact=exact)
+    r.set_pixels_per_thread(ppt)
     r.fit_capacity(sh016, shs16, 3)
     r.prepare(sh016, shs16, 3)
     color, T = r.render(geos16)
@@ -181,7 +182,7 @@ def test_batched_bf16_c4_view_matches_reference_on_rounded_inputs(ref, exact):
     rsh0, rshs = ref.sh_compute_bw(3, 16, vis, C.centers, pos, rgbs, g[1])
     errs = {"dL_dgeos": rel_err(dgeo, g[0]), "subdiv_p_bw": rel_err(sub, g[2].reshape(-1)),
             "dL_dsh0": rel_err(dsh0, rsh0), "dL_dshs": rel_err(dshs, rshs)}
-    print(f"batched c4 view 0 ({'exact' if exact else 'fast'}) vs reference (bf16-rounded inputs): rgb bitwise "
+    print(f"batched c4 view 0 ({'exact' if exact else 'fast'}, {ppt} px/thread) vs reference (bf16-rounded inputs): rgb bitwise "
           f"{rgb_bitwise}, image max err {img_max:.2e} rel {img_rel:.2e}, T max err {t_max:.2e}, bitwise {bitwise}; "
           + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
     assert rgb_bitwise
