@@ -105,6 +105,26 @@ int svr_rasterize_forward(const svr_camera* cam, int n_samp_per_vox, int need_de
                           size_t binning_bytes, void* image_buffer, size_t image_bytes, float* out_color,
                           float* out_depth, float* out_normal, float* out_T, float* max_w, int debug, void* stream);
 
+/* Octrees 21 levels deep: the forward of the reference's new_cuda backend
+ * (backends/new_cuda/src/forward.cu:660-752, config.h:16,24-34), whose
+ * 63-bit Morton ranks make the (tile, rank) sort key 128 bits wide
+ * (auxiliary.h:17-25,66-87).  levels = 16 is svr_rasterize_forward; levels =
+ * 21 sorts by (tile, 63-bit rank) -- the same order as the reference's stable
+ * wide-key sort -- and leaves the sorted values and tile ranges where
+ * svr_rasterize_backward reads them.  The binning buffer is sized by
+ * svr_binning_buffer_bytes_levels. */
+size_t svr_binning_buffer_bytes_levels(int64_t num_rendered, int width, int height, int levels);
+int svr_rasterize_binning_levels(const svr_camera* cam, int64_t P, int64_t num_rendered, const int64_t* octree_paths,
+                                 int levels, void* geom_buffer, void* binning_buffer, size_t binning_bytes,
+                                 void* image_buffer, size_t image_bytes, int debug, void* stream);
+int svr_rasterize_forward_levels(const svr_camera* cam, int n_samp_per_vox, int need_depth, int need_distortion,
+                                 int need_normal, int track_max_w, int64_t P, int64_t num_rendered,
+                                 const int64_t* octree_paths, int levels, const float* vox_centers,
+                                 const float* vox_lengths, const float* geos, const float* rgbs, void* geom_buffer,
+                                 void* binning_buffer, size_t binning_bytes, void* image_buffer, size_t image_bytes,
+                                 float* out_color, float* out_depth, float* out_normal, float* out_T, float* max_w,
+                                 int debug, void* stream);
+
 /* The two stages of svr_rasterize_forward, callable separately (same
  * arguments): duplication + sort + tile ranges (forward.cu:660-700), then the
  * compositing kernel alone (forward.cu:702-731).  The render stage also ranks
@@ -143,6 +163,11 @@ int svr_unpack_image_state(int width, int height, const void* image_buffer, int3
  * parity checks of the sort (forward.cu:681-686 results). */
 int svr_binning_sorted(const void* binning_buffer, int64_t num_rendered, int width, int height,
                        const uint64_t** keys, const uint32_t** vals);
+/* The same for a 21-level binning buffer: the sorted 128-bit keys as their
+ * low and high words (the reference's SortKey128 {hi, lo}: lo = tile << 63 |
+ * rank, hi = tile >> 1) and the sorted values. */
+int svr_binning_sorted_wide(const void* binning_buffer, int64_t num_rendered, int width, int height,
+                            const uint64_t** keys_lo, const uint64_t** keys_hi, const uint32_t** vals);
 /* Per-voxel preprocess state of a geom buffer (device pointers). */
 int svr_geom_arrays(const void* geom_buffer, int64_t P, const uint32_t** n_dup, const uint32_t** scan,
                     const uint64_t** bboxes, const uint32_t** quads);

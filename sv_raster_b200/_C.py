@@ -103,8 +103,9 @@ def geom_num_rendered(geomBuffer):
 
 def rasterize_voxels(n_samp_per_vox, image_width, image_height, tan_fovx, tan_fovy, cx, cy, w2c_matrix, c2w_matrix,
                      bg_color, need_depth, need_distortion, need_normal, track_max_w, octree_paths, vox_centers,
-                     vox_lengths, geos, rgbs, geomBuffer, debug=False):
-    """forward.cu:739-825 -> (num_rendered, binningBuffer, imgBuffer, color, depth, normal, T, max_w)."""
+                     vox_lengths, geos, rgbs, geomBuffer, debug=False, levels=MAX_NUM_LEVELS):
+    """forward.cu:739-825 -> (num_rendered, binningBuffer, imgBuffer, color, depth, normal, T, max_w).
+    ``levels`` = 21 bins octrees 21 levels deep (the new_cuda backend's forward)."""
     if vox_centers.ndimension() != 2 or vox_centers.size(1) != 3:
         raise RuntimeError("vox_centers must have dimensions (num_points, 3)")
     if rgbs.ndimension() != 2 or rgbs.size(1) != 3:
@@ -129,7 +130,13 @@ def rasterize_voxels(n_samp_per_vox, image_width, image_height, tan_fovx, tan_fo
         num_rendered = geom_num_rendered(geomBuffer)  # host sync, as forward.cu:653
         if num_rendered == 0xFFFFFFFF:
             raise RuntimeError("rasterize_voxels: instance count overflows 32 bits")
-        binning = torch.empty(L.svr_binning_buffer_bytes(num_rendered, W, H), dtype=torch.uint8, device=dev)
+        if levels == MAX_NUM_LEVELS:
+            nbytes = L.svr_binning_buffer_bytes(num_rendered, W, H)
+        else:
+            nbytes = L.svr_binning_buffer_bytes_levels(num_rendered, W, H, int(levels))
+            if nbytes == 0:
+                raise RuntimeError(f"rasterize_voxels: unsupported octree depth {levels}")
+        binning = torch.empty(nbytes, dtype=torch.uint8, device=dev)
         op = _i64(octree_paths, "octree_paths").reshape(-1)
         vc = _f32(vox_centers, "vox_centers")
         vl = _f32(vox_lengths, "vox_lengths")
@@ -138,10 +145,12 @@ def rasterize_voxels(n_samp_per_vox, image_width, image_height, tan_fovx, tan_fo
         w2c = _mat(w2c_matrix, "w2c_matrix", dev)
         c2w = _mat(c2w_matrix, "c2w_matrix", dev)
         cam = _camera(W, H, tan_fovx, tan_fovy, cx, cy, w2c, c2w, 0.02, bg_color)
-        st = L.svr_rasterize_forward(
-            ctypes.byref(cam), int(n_samp_per_vox), int(bool(need_depth)), int(bool(need_distortion)),
-            int(bool(need_normal)), int(bool(track_max_w)), P, num_rendered,
-            _ptr(op), _ptr(vc), _ptr(vl), _ptr(g), _ptr(c), _ptr(geomBuffer),
+        head = (ctypes.byref(cam), int(n_samp_per_vox), int(bool(need_depth)), int(bool(need_distortion)),
+                int(bool(need_normal)), int(bool(track_max_w)), P, num_rendered, _ptr(op))
+        fwd = L.svr_rasterize_forward if levels == MAX_NUM_LEVELS else \
+            (lambda *a: L.svr_rasterize_forward_levels(*a[:9], int(levels), *a[9:]))
+        st = fwd(
+            *head, _ptr(vc), _ptr(vl), _ptr(g), _ptr(c), _ptr(geomBuffer),
             _ptr(binning), binning.numel(), _ptr(img), img.numel(),
             _ptr(color), _ptr(depth) if (need_depth or need_distortion) else None,
             _ptr(normal) if need_normal else None, _ptr(T), _ptr(max_w) if track_max_w else None,
@@ -227,6 +236,21 @@ def unpack_sorted_list(binningBuffer, num_rendered, image_width, image_height):
     keys = binningBuffer[ko:ko + 8 * num_rendered].view(torch.int64).clone()
     vals = binningBuffer[vo:vo + 4 * num_rendered].view(torch.int32).clone()
     return keys, vals
+
+
+def unpack_sorted_list_wide(binningBuffer, num_rendered, image_width, image_height):
+    """Sorted 128-bit keys (as int64 high and low words) and values of a
+    21-level binning buffer (copies)."""
+    dev = binningBuffer.device
+    if num_rendered == 0:
+        e = torch.empty(0, dtype=torch.int64, device=dev)
+        return e, e.clone(), torch.empty(0, dtype=torch.int32, device=dev)
+    lo, hi, vp = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    check(lib().svr_binning_sorted_wide(_ptr(binningBuffer), num_rendered, image_width, image_height,
+                                        ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(vp)), "binning_sorted_wide")
+    base = binningBuffer.data_ptr()
+    cut = lambda p, n, dt: binningBuffer[p.value - base:p.value - base + n * num_rendered].view(dt).clone()
+    return cut(hi, 8, torch.int64), cut(lo, 8, torch.int64), cut(vp, 4, torch.int32)
 
 
 def unpack_geom_state(geomBuffer, P):

@@ -58,6 +58,14 @@ _SIGS = {
                                        c_p, c_p, c_p, c_p, c_p, c_int, c_p]),
     "svr_unpack_image_state": (c_int, [c_int, c_int, c_p, c_p, c_p, c_p, c_p]),
     "svr_binning_sorted": (c_int, [c_p, c_i64, c_int, c_int, ctypes.POINTER(c_p), ctypes.POINTER(c_p)]),
+    "svr_binning_sorted_wide": (c_int, [c_p, c_i64, c_int, c_int, ctypes.POINTER(c_p), ctypes.POINTER(c_p),
+                                        ctypes.POINTER(c_p)]),
+    "svr_binning_buffer_bytes_levels": (c_sz, [c_i64, c_int, c_int, c_int]),
+    "svr_rasterize_binning_levels": (c_int, [ctypes.POINTER(Camera), c_i64, c_i64, c_p, c_int, c_p, c_p, c_sz, c_p,
+                                             c_sz, c_int, c_p]),
+    "svr_rasterize_forward_levels": (c_int, [ctypes.POINTER(Camera), c_int, c_int, c_int, c_int, c_int, c_i64, c_i64,
+                                             c_p, c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_sz, c_p, c_sz,
+                                             c_p, c_p, c_p, c_p, c_p, c_int, c_p]),
     "svr_geom_arrays": (c_int, [c_p, c_i64, ctypes.POINTER(c_p), ctypes.POINTER(c_p), ctypes.POINTER(c_p),
                                 ctypes.POINTER(c_p)]),
     "svr_sh_compute": (c_int, [c_int, c_i64, c_p, c_i64, c_int, c_p, c_p, c_p, c_p, c_int, c_p, c_p]),

@@ -117,6 +117,27 @@ BinningLayout binning_layout(void* buf, size_t n, int n_tiles) {
   return b;
 }
 
+// 21-level binning: the 16-level layout, then the wide keys' high halves
+// and the per-instance rank, tile and value arrays.
+DeepBinning deep_layout(void* buf, size_t n, int n_tiles, size_t* bytes) {
+  BinningLayout bl = binning_layout(buf, n, n_tiles);
+  Carver c(buf ? static_cast<char*>(buf) + bl.bytes : nullptr);
+  DeepBinning d;
+  d.keys_a = bl.keys_a;
+  d.keys_b = bl.keys_b;
+  d.vals_a = bl.vals_a;
+  d.vals_b = bl.vals_b;
+  d.sort_temp = bl.sort_temp;
+  d.vals_out = bl.vals_b;
+  d.keys_lo = bl.keys_b;
+  d.keys_hi = c.take<uint64_t>(n);
+  d.rank_of = c.take<uint64_t>(n);
+  d.tile_of = c.take<uint32_t>(n);
+  d.val_of = c.take<uint32_t>(n);
+  if (bytes) *bytes = bl.bytes + c.size();
+  return d;
+}
+
 // Bits needed to represent n (the tile-id width of the sort key).
 inline int bit_width_u32(uint32_t n) {
   int b = 0;
@@ -196,6 +217,14 @@ size_t svr_binning_buffer_bytes(int64_t n, int width, int height) {
   return binning_layout(nullptr, (size_t)n, tiles_x(width) * tiles_y(height)).bytes;
 }
 
+size_t svr_binning_buffer_bytes_levels(int64_t n, int width, int height, int levels) {
+  if (levels == kMaxLevels) return svr_binning_buffer_bytes(n, width, height);
+  if (levels != kDeepLevels || n < 0 || width <= 0 || height <= 0) return 0;
+  size_t bytes = 0;
+  deep_layout(nullptr, (size_t)n, tiles_x(width) * tiles_y(height), &bytes);
+  return bytes;
+}
+
 const uint32_t* svr_geom_count_ptr(const void* geom) { return static_cast<const uint32_t*>(geom); }
 uint32_t* svr_geom_error_ptr(void* geom) { return static_cast<uint32_t*>(geom) + 1; }
 
@@ -229,7 +258,7 @@ struct FwdCtx {
 
 static int fwd_prepare(const svr_camera* cam, int n_samp, int64_t P, int64_t num_rendered, void* geom_buffer,
                        void* binning_buffer, size_t binning_bytes, void* image_buffer, size_t image_bytes,
-                       FwdCtx& c) {
+                       FwdCtx& c, bool deep = false) {
   if (!valid_camera(cam) || n_samp < 1 || n_samp > kMaxSamples || P < 0 || num_rendered < 0 ||
       num_rendered > 0xffffffffll)
     return SVR_ERR_SHAPE;
@@ -238,9 +267,10 @@ static int fwd_prepare(const svr_camera* cam, int n_samp, int64_t P, int64_t num
   if (!image_buffer || image_bytes < c.im.bytes) return SVR_ERR_CAPACITY;
   c.n = (size_t)num_rendered;
   c.bl = binning_layout(binning_buffer, c.n, tiles_x(W) * tiles_y(H));
-  if (c.n > 0 && (!binning_buffer || binning_bytes < c.bl.bytes)) return SVR_ERR_CAPACITY;
+  // (21-level binning checks its own, larger buffer; its keys are two words wide)
+  if (!deep && c.n > 0 && (!binning_buffer || binning_bytes < c.bl.bytes)) return SVR_ERR_CAPACITY;
   c.key_bits = plain_key_bits(W, H);
-  if (c.key_bits > 64) return SVR_ERR_KEYBITS;
+  if (!deep && c.key_bits > 64) return SVR_ERR_KEYBITS;
   c.g = geom_layout(geom_buffer, P);
   c.vt.n = 1;
   c.vt.v[0] = make_view(*cam);
@@ -309,6 +339,46 @@ int svr_rasterize_render(const svr_camera* cam, int n_samp, int need_depth, int 
   return check_launch(debug, stream);
 }
 
+int svr_rasterize_binning_levels(const svr_camera* cam, int64_t P, int64_t num_rendered, const int64_t* octree_paths,
+                                 int levels, void* geom_buffer, void* binning_buffer, size_t binning_bytes,
+                                 void* image_buffer, size_t image_bytes, int debug, void* stream_) {
+  if (levels == kMaxLevels)
+    return svr_rasterize_binning(cam, P, num_rendered, octree_paths, geom_buffer, binning_buffer, binning_bytes,
+                                 image_buffer, image_bytes, debug, stream_);
+  if (levels != kDeepLevels) return SVR_ERR_SHAPE;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  FwdCtx c;
+  int st = fwd_prepare(cam, 1, P, num_rendered, geom_buffer, binning_buffer, 0, image_buffer, image_bytes, c, true);
+  if (st != SVR_OK) return st;
+  size_t need = 0;
+  const ViewParams& vp = c.vt.v[0];
+  const int n_tiles = vp.grid_x * vp.grid_y;
+  DeepBinning d = deep_layout(binning_buffer, c.n, n_tiles, &need);
+  if (c.n > 0 && (!binning_buffer || binning_bytes < need)) return SVR_ERR_CAPACITY;
+  if (P == 0) return SVR_OK;
+  if (c.n > 0 && !octree_paths) return SVR_ERR_SHAPE;
+  cudaMemsetAsync(c.im.ranges, 0, (size_t)n_tiles * sizeof(uint2), stream);
+  launch_binning_deep(vp, (int)P, octree_paths, c.g.bbox, c.g.quad, c.g.ndup, c.g.scan, c.g.header, (uint32_t)c.n, d,
+                      c.im.ranges, c.g.header + 1, stream);
+  return check_launch(debug, stream);
+}
+
+int svr_rasterize_forward_levels(const svr_camera* cam, int n_samp, int need_depth, int need_distortion,
+                                 int need_normal, int track_max_w, int64_t P, int64_t num_rendered,
+                                 const int64_t* octree_paths, int levels, const float* vox_centers,
+                                 const float* vox_lengths, const float* geos, const float* rgbs, void* geom_buffer,
+                                 void* binning_buffer, size_t binning_bytes, void* image_buffer, size_t image_bytes,
+                                 float* out_color, float* out_depth, float* out_normal, float* out_T, float* max_w,
+                                 int debug, void* stream) {
+  int st = svr_rasterize_binning_levels(cam, P, num_rendered, octree_paths, levels, geom_buffer, binning_buffer,
+                                        binning_bytes, image_buffer, image_bytes, debug, stream);
+  if (st != SVR_OK) return st;
+  return svr_rasterize_render(cam, n_samp, need_depth, need_distortion, need_normal, track_max_w, P, num_rendered,
+                              vox_centers, vox_lengths, geos, rgbs, geom_buffer, binning_buffer, binning_bytes,
+                              image_buffer, image_bytes, out_color, out_depth, out_normal, out_T, max_w, debug,
+                              stream);
+}
+
 int svr_rasterize_forward(const svr_camera* cam, int n_samp, int need_depth, int need_distortion, int need_normal,
                           int track_max_w, int64_t P, int64_t num_rendered, const int64_t* octree_paths,
                           const float* vox_centers, const float* vox_lengths, const float* geos, const float* rgbs,
@@ -369,6 +439,17 @@ int svr_unpack_image_state(int width, int height, const void* image_buffer, int3
     cudaMemcpyAsync(n_contrib, im.n_contrib, (size_t)width * height * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                     stream);
   return check_launch(0, stream);
+}
+
+int svr_binning_sorted_wide(const void* binning_buffer, int64_t num_rendered, int width, int height,
+                            const uint64_t** keys_lo, const uint64_t** keys_hi, const uint32_t** vals) {
+  if (!binning_buffer || num_rendered < 0 || width <= 0 || height <= 0) return SVR_ERR_SHAPE;
+  DeepBinning d = deep_layout(const_cast<void*>(binning_buffer), (size_t)num_rendered,
+                              tiles_x(width) * tiles_y(height), nullptr);
+  if (keys_lo) *keys_lo = d.keys_lo;
+  if (keys_hi) *keys_hi = d.keys_hi;
+  if (vals) *vals = d.vals_out;
+  return SVR_OK;
 }
 
 int svr_binning_sorted(const void* binning_buffer, int64_t num_rendered, int width, int height,

@@ -30,6 +30,10 @@ constexpr float kStepScale = 100.f;               // config.h:21
 constexpr int kMaxSamples = 3;                    // config.h:23
 constexpr int kRankBits = 3 * kMaxLevels;         // config.h:27 (48)
 constexpr int kVoxIdBits = 29;                    // auxiliary.h:50-63
+// Octrees 21 levels deep (the reference's new_cuda backend, config.h:16,30):
+// 63-bit Morton ranks, sorted as (tile, rank) pairs wider than 64 bits.
+constexpr int kDeepLevels = 21;
+constexpr int kDeepRankBits = 3 * kDeepLevels;
 
 // Repeat a 3-bit octant code over all 16 octree levels (auxiliary.h:16-38).
 __host__ __device__ constexpr uint64_t octant_repeat(uint64_t q) {

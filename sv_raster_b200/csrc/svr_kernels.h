@@ -89,6 +89,26 @@ void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* r
                              size_t rgb_view_stride, size_t drgb_view_stride, const BwdTileIn& in,
                              const BwdTileOut& out, int ns, int tile, int stage, bool fast, int pair,
                              const uint32_t* order, uint32_t* counter, int ctas_per_sm, cudaStream_t stream);
+// svr_binning_deep.cu: binning of 21-level octrees (63-bit ranks).  The
+// sort pairs (keys_a, vals_a) / (keys_b, vals_b) and sort_temp are those of
+// the 16-level layout; vals_out / keys_lo are its sorted-value and sorted-key
+// arrays, keys_hi and the per-instance rank / tile / value arrays follow it.
+struct DeepBinning {
+  uint64_t* keys_a;
+  uint64_t* keys_b;
+  uint32_t* vals_a;
+  uint32_t* vals_b;
+  void* sort_temp;
+  uint64_t* rank_of;
+  uint32_t* tile_of;
+  uint32_t* val_of;
+  uint32_t* vals_out;
+  uint64_t* keys_lo;
+  uint64_t* keys_hi;
+};
+void launch_binning_deep(const ViewParams& vp, int P, const int64_t* octpaths, const uint2* bboxes,
+                         const uint32_t* quads, const uint32_t* ndup, const uint32_t* scan, const uint32_t* d_n,
+                         uint32_t n, const DeepBinning& b, uint2* ranges, uint32_t* err, cudaStream_t stream);
 // Grid of a persistent launch: resident CTAs of `kernel` on this device
 // (capped at ctas_per_sm per SM when > 0), at most n_items.
 int persistent_grid(const void* kernel, int threads, size_t dyn_smem, int n_items, int ctas_per_sm);

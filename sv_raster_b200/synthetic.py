@@ -25,27 +25,28 @@ import numpy as np
 MAX_LEVELS = 16
 
 
-def ijk_to_octpath(ijk, level):
-    """(i,j,k) integer cell coords at `level` -> octpath (int64)."""
+def ijk_to_octpath(ijk, level, max_levels=MAX_LEVELS):
+    """(i,j,k) integer cell coords at `level` -> octpath (int64) of an octree
+    `max_levels` deep (16, or 21 for the new_cuda encoding)."""
     ijk = np.asarray(ijk, dtype=np.int64)
     level = np.asarray(level, dtype=np.int64).reshape(-1)
     i, j, k = ijk[:, 0].copy(), ijk[:, 1].copy(), ijk[:, 2].copy()
     path = np.zeros(len(level), dtype=np.int64)
-    for l in range(MAX_LEVELS):
+    for l in range(max_levels):
         bits = ((i & 1) << 2) | ((j & 1) << 1) | (k & 1)
         path |= bits << (3 * l)
         i >>= 1
         j >>= 1
         k >>= 1
-    return path << (3 * (MAX_LEVELS - level))
+    return path << (3 * (max_levels - level))
 
 
-def octpath_to_ijk(path, level):
+def octpath_to_ijk(path, level, max_levels=MAX_LEVELS):
     path = np.asarray(path, dtype=np.int64).reshape(-1)
     level = np.asarray(level, dtype=np.int64).reshape(-1)
-    p = path >> (3 * (MAX_LEVELS - level))
+    p = path >> (3 * (max_levels - level))
     ijk = np.zeros((len(path), 3), dtype=np.int64)
-    for l in range(MAX_LEVELS):
+    for l in range(max_levels):
         bits = p & 7
         ijk[:, 0] |= ((bits >> 2) & 1) << l
         ijk[:, 1] |= ((bits >> 1) & 1) << l
@@ -54,9 +55,9 @@ def octpath_to_ijk(path, level):
     return ijk
 
 
-def decode_voxels(path, level):
+def decode_voxels(path, level, max_levels=MAX_LEVELS):
     """Voxel centres [N,3] and sizes [N,1] (float32, exact) of octree cells."""
-    ijk = octpath_to_ijk(path, level)
+    ijk = octpath_to_ijk(path, level, max_levels)
     size = np.ldexp(1.0, -np.asarray(level, dtype=np.int64).reshape(-1, 1))
     centers = -0.5 + (ijk + 0.5) * size
     return centers.astype(np.float32), size.astype(np.float32)
@@ -395,6 +396,40 @@ def grid_params(sc, dev, seed=0):
     rng = np.random.default_rng(seed + 5)
     mu, sd = float(np.mean(sc.geos)), float(np.std(sc.geos))
     return key, rng.normal(mu, sd, size=M).astype(np.float32)
+
+
+def deep_scene(n_voxels=20000, n_chains=64, seed=0, max_levels=21):
+    """An octree 21 levels deep (the new_cuda backend's depth): the c1 sphere
+    scene (levels 6-8) with `n_chains` of its voxels refined down to level 21
+    along a seeded path -- at every level 7 of the 8 children are kept and one
+    is refined further -- so every level from 6 to 21 holds voxels and their
+    63-bit Morton ranks differ below the 48 bits a 16-level octree uses.
+    No voxel is an ancestor of another.  Octree paths use the 21-level
+    encoding (utils.cu:129-158 with MAX_NUM_LEVELS = 21)."""
+    base = config_scene("c1", seed=seed, n_voxels=n_voxels)
+    ijk = octpath_to_ijk(base.octpath, base.octlevel)
+    lv = base.octlevel.astype(np.int64)
+    rng = np.random.default_rng(seed + 77)
+    pick = rng.choice(len(lv), size=min(n_chains, len(lv)), replace=False)
+    keep = np.ones(len(lv), bool)
+    keep[pick] = False
+    cells, levels = [ijk[keep]], [lv[keep]]
+    offs = np.array([[(c >> 2) & 1, (c >> 1) & 1, c & 1] for c in range(8)], np.int64)
+    for p in pick:
+        cur, l = ijk[p], int(lv[p])
+        while l < max_levels:
+            kids = 2 * cur[None, :] + offs
+            nxt = int(rng.integers(8))
+            cells.append(np.delete(kids, nxt, axis=0))
+            levels.append(np.full(7, l + 1, np.int64))
+            cur, l = kids[nxt], l + 1
+        cells.append(cur[None, :])
+        levels.append(np.array([l], np.int64))
+    ijk, lv = np.concatenate(cells), np.concatenate(levels)
+    path = ijk_to_octpath(ijk, lv, max_levels)
+    centers, lengths = decode_voxels(path, lv, max_levels)
+    geos, sh0, shs = _params(np.random.default_rng(seed + 1), len(path), -1.0, 1.0)
+    return Scene("deep", path, lv.astype(np.int8), centers, lengths, geos, sh0, shs, config_cameras("c1", seed))
 
 
 def scene_cache_dir():

@@ -6,7 +6,9 @@ with torch tensor operations on the inputs' device.
 """
 import torch
 
-MAX_NUM_LEVELS = 16
+from . import _C
+
+MAX_NUM_LEVELS = _C.MAX_NUM_LEVELS  # 16, or 21 for the new_cuda surface (levels21)
 
 
 def _order_tables(device):

@@ -108,15 +108,20 @@ def test_bf16_storage_precision_c4_full_view():
     # PSNR against the target within 0.01 dB of the FP64 oracle's
     assert abs(b["psnr_delta_db"]) <= 0.01
     assert abs(f["psnr_delta_db"]) <= 1e-3
-    # fp32 compositing: the fp32 path is within fp32 accumulation error of FP64
-    assert f["image_max_abs_err"] <= 1e-4
+    # fp32 compositing: within fp32 accumulation error of FP64 norm-wise; a
+    # pixel whose transmittance lands on the 1e-4 early-stop threshold may
+    # take one voxel more or less in fp32 than in FP64 (at most T * alpha *
+    # rgb < 2e-4 of colour; measured 1.0e-4 on this view)
+    assert f["image_rel_err"] <= 1e-5 and f["image_max_abs_err"] <= 2e-4
     assert f["dL_dgeos_rel_err"] <= 1e-4 and f["dL_dsh0_rel_err"] <= 1e-4 and f["dL_dshs_rel_err"] <= 1e-4
-    # bf16 storage: 8-bit mantissas of the stored densities and SH bound the error
-    assert b["image_max_abs_err"] <= 0.05
+    # bf16 storage: the 8-bit mantissas of the stored densities and SH
+    # coefficients bound the error (measured: image 2.8e-4 norm-wise, 1.2e-3
+    # at worst; gradients 1.3e-3 and 8.8e-4)
+    assert b["image_rel_err"] <= 1e-3 and b["image_max_abs_err"] <= 5e-3
     assert b["dL_dgeos_rel_err"] <= BF16_GRAD_TOL
     assert b["dL_dsh0_rel_err"] <= BF16_GRAD_TOL and b["dL_dshs_rel_err"] <= BF16_GRAD_TOL
 
 
 # Relative error of bf16-storage gradients against the FP64 oracle on the fp32
 # master parameters.
-BF16_GRAD_TOL = 0.05
+BF16_GRAD_TOL = 5e-3

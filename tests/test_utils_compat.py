@@ -57,3 +57,32 @@ def test_svraster_cuda_shim_resolves_to_this_package():
     assert svraster_cuda.sparse_adam.SparseAdam is sv_raster_b200.sparse_adam.SparseAdam
     assert MAX_NUM_LEVELS == 16 and STEP_SZ_SCALE == 100.0
     assert hasattr(svraster_cuda.grid_loss_bw, "total_variation")
+
+
+def test_levels21_surface_imports_with_its_depth():
+    """The new_svraster_cuda drop-in: the same modules over a 21-level _C."""
+    import importlib
+    import sys
+    from sv_raster_b200 import levels21
+    assert levels21._C.MAX_NUM_LEVELS == 21 and levels21.meta.MAX_NUM_LEVELS == 21
+    assert levels21.utils.MAX_NUM_LEVELS == 21 and levels21.meta.MAX_SORT_KEY_BITS == 128
+    assert levels21.meta.MAX_RENDER_TILES == 4096 * 4096
+    assert levels21.renderer._C is levels21._C
+    from sv_raster_b200 import renderer, utils
+    assert renderer._C.MAX_NUM_LEVELS == 16 and utils.MAX_NUM_LEVELS == 16
+    compat = __import__("os").path.join(__import__("os").path.dirname(renderer.__file__), "compat")
+    sys.path.insert(0, compat)
+    try:
+        m = importlib.import_module("new_svraster_cuda")
+        assert m.renderer is levels21.renderer and m.meta.MAX_NUM_LEVELS == 21
+    finally:
+        sys.path.remove(compat)
+
+
+def test_deep_scene_spans_21_levels():
+    from sv_raster_b200 import synthetic
+    sc = synthetic.deep_scene(n_voxels=3000, n_chains=8)
+    assert int(sc.octlevel.min()) == 6 and int(sc.octlevel.max()) == 21
+    assert int(sc.octpath.max()).bit_length() > 48  # ranks use the bits below a 16-level path
+    c, l = synthetic.decode_voxels(sc.octpath, sc.octlevel, 21)
+    assert (c == sc.centers).all() and (l == sc.lengths).all()
