@@ -447,8 +447,10 @@ def comparator_leg(args, sc, dev, batched_ms_per_view):
 def cpu_baseline(sc, budget_s=15.0, view=0, seed=0):
     """The CPU oracle (fp32 mimic, all host threads) on a bounded sample of one
     view: its full SH, projection and binning, then forward + backward of
-    seeded runs of 8 tiles spread over the image until the budget is spent;
-    reported as ms/view = setup + mean time per sampled tile x tile count."""
+    seeded runs of 128 tiles spread over the image until the budget is spent;
+    reported as ms/view = setup + mean time per sampled tile x tile count.
+    (Each oracle call allocates full-view images and per-voxel gradients, so
+    runs are long enough for the compositing to dominate the sample.)"""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     cam = sc.cameras[view % len(sc.cameras)]
@@ -462,8 +464,8 @@ def cpu_baseline(sc, budget_s=15.0, view=0, seed=0):
     t_setup = time.perf_counter() - t0
     gx, gy = (cam.width + 15) // 16, (cam.height + 15) // 16
     T = gx * gy
-    run = 8
-    order = np.random.default_rng(seed + view).permutation(max(1, T // run))
+    run = 128
+    order = np.random.default_rng(seed + view).permutation(max(1, -(-T // run)))
     spent, done = 0.0, 0
     for slot in order:
         lo, hi = int(slot) * run, min(T, int(slot) * run + run)
