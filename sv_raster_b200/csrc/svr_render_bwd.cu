@@ -23,7 +23,8 @@ struct BwdArgs {
 template <class CFG>
 struct BwdSmem {
   StageSmem<CFG::SB> s;
-  float grad[CFG::SB * kGradStride];
+  float grad[GradAcc<CFG>::kFloats];
+  uint32_t hit[GradAcc<CFG>::kWords];
   float c2w[12];
   uint32_t item;
 };
@@ -40,7 +41,7 @@ render_bwd_kernel(const __grid_constant__ BwdArgs a) {
   const int tile = a.order ? (int)a.order[b] : b;
   const int tile_x = (tile % a.vp.grid_x) * 2 + (sub & 1), tile_y = (tile / a.vp.grid_x) * 2 + (sub >> 1);
   render_tile_bwd<PlainTile, NS, DEPTH, DIST, NORMAL>(a.vp, sm.c2w, tile_x, tile_y, a.ranges[tile], a.tile_last[tile],
-                                                      a.vals, a.va, a.in, a.out, sm.s, sm.grad);
+                                                      a.vals, a.va, a.in, a.out, sm.s, sm.grad, sm.hit);
 }
 
 // Multi-view form: a persistent grid over all views' tiles, in the order of
@@ -90,7 +91,7 @@ render_bwd_batch_kernel(const __grid_constant__ BwdBatchArgs a) {
     BwdTileOut o = a.out;
     o.dL_drgbs = a.out.dL_drgbs + (size_t)view * a.drgb_view_stride;
     render_tile_bwd<CFG, NS, false, false, false, FAST, true>(vp, sm.c2w, tile_x, tile_y, a.ranges[item],
-                                                              a.tile_last[item], a.vals, va, in, o, sm.s, sm.grad);
+                                                              a.tile_last[item], a.vals, va, in, o, sm.s, sm.grad, sm.hit);
     __syncthreads();  // shared state (item, camera, staging) is free for the next tile
   }
 }
@@ -125,7 +126,7 @@ render_bwd_batch_pair_kernel(const __grid_constant__ BwdBatchArgs a) {
     BwdTileOut o = a.out;
     o.dL_drgbs = a.out.dL_drgbs + (size_t)view * a.drgb_view_stride;
     render_tile_bwd_pair<CFG, NS, FAST>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.tile_last[item], a.vals, va,
-                                        in, o, sm.s, sm.grad);
+                                        in, o, sm.s, sm.grad, sm.hit);
     __syncthreads();
   }
 }

@@ -8,9 +8,9 @@
 // ascending / colour-concentration terms (:344-510) and the 12-float
 // gradient pack (:515-522).  The reference issues 12 global atomics per
 // contributing (pixel, voxel); here each warp reduces its lanes' gradients
-// with shuffles into a shared-memory accumulator per staged record, and each
-// record is flushed once per tile (16-byte vector reductions where the
-// gradient rows are aligned).
+// with shuffles into a shared-memory accumulator per staged record
+// (GradAcc), and each record is flushed once per tile (16-byte vector
+// reductions where the gradient rows are aligned).
 #pragma once
 
 #include "svr_render.cuh"
@@ -91,12 +91,103 @@ __device__ __forceinline__ int warp_reduce_scatter12(float v[12], int lane) {
 // FAST selects the arithmetic of the per-(pixel, voxel) loop (exp_f, div_f in
 // svr_common.cuh); RGB4 the [P,4] colour-gradient layout whose rows, like the
 // density rows, are flushed with one 16-byte vector reduction each.
+// Per-record gradient accumulators of one staging round.  With at most two
+// warps per CTA each warp owns a slot per staged record: a warp visits a
+// record at most once per round, so the record's warp total is stored with
+// plain stores, a bitmask per 32-record group marks the slots written this
+// round, and the flush adds the (at most two) slots -- no shared-memory
+// atomics and no zeroing.  Larger CTAs share one slot per record and add into
+// it with shared-memory atomics.
+template <class CFG>
+struct GradAcc {
+  static constexpr bool kPerWarp = CFG::NW <= 2;
+  static constexpr int kStride = kPerWarp ? 12 : kGradStride;  // 48-byte rows: 16-byte vector access
+  static constexpr int kFloats = (kPerWarp ? CFG::NW : 1) * CFG::SB * kStride;
+  static constexpr int kWords = kPerWarp ? CFG::NW * CFG::GROUPS : 1;
+
+  __device__ static void init(float* s_grad, int tid) {
+    if (!kPerWarp)
+      for (int i = tid; i < CFG::SB * kStride; i += CFG::NT) s_grad[i] = 0.f;
+  }
+
+  // The warp's gradients of staged record j (gp: this lane's 12 values,
+  // meaningful where `contrib`; act_mask: the contributing lanes).
+  __device__ static void add(float* s_grad, int warp, int j, float gp[12], int lane, uint32_t act_mask,
+                             bool contrib, int atomic_lanes) {
+    const bool reduce = kPerWarp ? __popc(act_mask) > 1 : __popc(act_mask) > atomic_lanes;
+    if (reduce && !contrib) {
+#pragma unroll
+      for (int c = 0; c < 12; ++c) gp[c] = 0.f;
+    }
+    if (kPerWarp) {
+      float* acc = s_grad + (warp * CFG::SB + j) * kStride;
+      if (!reduce) {
+        if (contrib) {
+          float4* a4 = reinterpret_cast<float4*>(acc);
+          a4[0] = make_float4(gp[0], gp[1], gp[2], gp[3]);
+          a4[1] = make_float4(gp[4], gp[5], gp[6], gp[7]);
+          a4[2] = make_float4(gp[8], gp[9], gp[10], gp[11]);
+        }
+      } else {
+        const int slot = warp_reduce_scatter12(gp, lane);
+        if (slot >= 0) acc[slot] = gp[0];
+      }
+    } else {
+      float* acc = s_grad + j * kStride;
+      if (!reduce) {  // few lanes: add their values directly
+        if (contrib) {
+#pragma unroll
+          for (int c = 0; c < 12; ++c) atomicAdd(acc + c, gp[c]);
+        }
+      } else {
+        const int slot = warp_reduce_scatter12(gp, lane);
+        if (slot >= 0) atomicAdd(acc + slot, gp[0]);
+      }
+    }
+  }
+
+  // End of group g of a warp's hit loop: `wrote` marks the records it stored.
+  __device__ static void mark(uint32_t* s_hit, int warp, int g, uint32_t wrote, int lane) {
+    if (kPerWarp && lane == 0) s_hit[warp * CFG::GROUPS + g] = wrote;
+  }
+
+  // Record t's total over the CTA this round; false when no warp wrote it.
+  __device__ static bool gather(float* s_grad, const uint32_t* s_hit, int t, float a[12]) {
+    if (kPerWarp) {
+      bool any = false;
+#pragma unroll
+      for (int c = 0; c < 12; ++c) a[c] = 0.f;
+#pragma unroll
+      for (int w = 0; w < CFG::NW; ++w) {
+        if (!((s_hit[w * CFG::GROUPS + (t >> 5)] >> (t & 31)) & 1u)) continue;
+        any = true;
+        const float4* a4 = reinterpret_cast<const float4*>(s_grad + (w * CFG::SB + t) * kStride);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const float4 v = a4[q];
+          a[4 * q] += v.x; a[4 * q + 1] += v.y; a[4 * q + 2] += v.z; a[4 * q + 3] += v.w;
+        }
+      }
+      return any;
+    }
+    float* acc = s_grad + t * kStride;
+#pragma unroll
+    for (int c = 0; c < 12; ++c) {
+      a[c] = acc[c];
+      acc[c] = 0.f;
+    }
+    return true;
+  }
+};
+
 template <class CFG, int NS, bool DEPTH, bool DIST, bool NORMAL, bool FAST = false, bool RGB4 = false>
 __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const float* __restrict__ c2w_s, int tile_x,
                                                 int tile_y, uint2 range_raw, uint32_t tile_last,
                                                 const uint32_t* __restrict__ vals, const VoxelArrays& va,
                                                 const BwdTileIn& in, const BwdTileOut& out, StageSmem<CFG::SB>& s,
-                                                float* s_grad /*[SB*kGradStride]*/) {
+                                                float* s_grad /*[GradAcc::kFloats]*/,
+                                                uint32_t* s_hit /*[GradAcc::kWords]*/) {
+  using Acc = GradAcc<CFG>;
   constexpr int SB = CFG::SB;
   const int W = vp.W, H = vp.H;
   const int tid = threadIdx.x, lane = tid & 31;
@@ -153,7 +244,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
     prefix_w = 1.f - T_final;
   }
 
-  for (int i = tid; i < SB * kGradStride; i += CFG::NT) s_grad[i] = 0.f;
+  Acc::init(s_grad, tid);
   // Largest contributor count of this warp: records at or beyond it are skipped by every lane.
   const uint32_t warp_lc = __reduce_max_sync(0xffffffffu, last_contrib);
   const uint32_t quad_mask = __reduce_or_sync(0xffffffffu, inside ? (1u << ray.quad) : 0u);
@@ -173,6 +264,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
       const uint32_t pos = (uint32_t)(todo_total - base - slot - 1);
       const bool hit = slot < n_here && pos < warp_lc && record_hits_warp(s, slot, wx0, wy0, quad_mask);
       uint32_t m = __ballot_sync(0xffffffffu, hit);
+      uint32_t wrote = 0u;
       while (m) {
         const int j = g * 32 + __ffs(m) - 1;
         m &= m - 1;
@@ -342,29 +434,19 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
             }
           }
         }
-        // Warp reduction of this record's gradients into its shared accumulator.
+        // Warp reduction of this record's gradients into its accumulator.
         const uint32_t act_mask = __ballot_sync(0xffffffffu, contrib);
         if (act_mask == 0u) continue;
-        float* acc = s_grad + j * kGradStride;
-        if (__popc(act_mask) <= in.atomic_lanes) {  // few lanes: add their values directly
-          if (contrib) {
-#pragma unroll
-            for (int c = 0; c < 12; ++c) atomicAdd(acc + c, gp[c]);
-          }
-        } else {
-          if (!contrib) {
-#pragma unroll
-            for (int c = 0; c < 12; ++c) gp[c] = 0.f;
-          }
-          const int slot = warp_reduce_scatter12(gp, lane);
-          if (slot >= 0) atomicAdd(acc + slot, gp[0]);
-        }
+        Acc::add(s_grad, warp, j, gp, lane, act_mask, contrib, in.atomic_lanes);
+        wrote |= 1u << (j & 31);
       }
+      Acc::mark(s_hit, warp, g, wrote, lane);
     }
     __syncthreads();
     // Flush this batch's accumulators: one set of reductions per (voxel, tile).
     for (int t = tid; t < n_here; t += CFG::NT) {
-      float* acc = s_grad + t * kGradStride;
+      float acc[12];
+      if (!Acc::gather(s_grad, s_hit, t, acc)) continue;
       float gsum = 0.f;
 #pragma unroll
       for (int c = 0; c < 12; ++c) gsum += fabsf(acc[c]);
@@ -386,8 +468,6 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
           atomicAdd(out.subdiv + vid, acc[11]);
         }
       }
-#pragma unroll
-      for (int c = 0; c < 12; ++c) acc[c] = 0.f;
     }
   }
 }

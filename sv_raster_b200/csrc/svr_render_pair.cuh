@@ -182,7 +182,9 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
                                                      int tile_x, int tile_y, uint2 range_raw, uint32_t tile_last,
                                                      const uint32_t* __restrict__ vals, const VoxelArrays& va,
                                                      const BwdTileIn& in, const BwdTileOut& out,
-                                                     StageSmem<CFG::SB>& s, float* s_grad /*[SB*kGradStride]*/) {
+                                                     StageSmem<CFG::SB>& s, float* s_grad /*[GradAcc::kFloats]*/,
+                                                     uint32_t* s_hit /*[GradAcc::kWords]*/) {
+  using Acc = GradAcc<CFG>;
   constexpr int SB = CFG::SB;
   const int W = vp.W, H = vp.H;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -219,7 +221,7 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
     }
   }
 
-  for (int i = tid; i < SB * kGradStride; i += CFG::NT) s_grad[i] = 0.f;
+  Acc::init(s_grad, tid);
   const uint32_t warp_lc = __reduce_max_sync(0xffffffffu, max(last_contrib[0], last_contrib[1]));
   const uint32_t quad_mask = __reduce_or_sync(
       0xffffffffu, (inside[0] ? (1u << ray[0].quad) : 0u) | (inside[1] ? (1u << ray[1].quad) : 0u));
@@ -238,6 +240,7 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
       const uint32_t pos = (uint32_t)(todo_total - base - slot - 1);
       const bool hit = slot < n_here && pos < warp_lc && record_hits_block8(s, slot, wx0, wy0, quad_mask);
       uint32_t m = __ballot_sync(0xffffffffu, hit);
+      uint32_t wrote = 0u;
       while (m) {
         const int j = g * 32 + __ffs(m) - 1;
         m &= m - 1;
@@ -307,22 +310,16 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
         // One warp reduction for both pixels' gradients of this record.
         const uint32_t act_mask = __ballot_sync(0xffffffffu, contrib);
         if (act_mask == 0u) continue;
-        float* acc = s_grad + j * kGradStride;
-        if (__popc(act_mask) <= in.atomic_lanes) {
-          if (contrib) {
-#pragma unroll
-            for (int c = 0; c < 12; ++c) atomicAdd(acc + c, gp[c]);
-          }
-        } else {
-          const int slot_out = warp_reduce_scatter12(gp, lane);
-          if (slot_out >= 0) atomicAdd(acc + slot_out, gp[0]);
-        }
+        Acc::add(s_grad, warp, j, gp, lane, act_mask, contrib, in.atomic_lanes);
+        wrote |= 1u << (j & 31);
       }
+      Acc::mark(s_hit, warp, g, wrote, lane);
     }
     __syncthreads();
     // Flush this batch's accumulators: one set of vector reductions per (voxel, tile).
     for (int t = tid; t < n_here; t += CFG::NT) {
-      float* acc = s_grad + t * kGradStride;
+      float acc[12];
+      if (!Acc::gather(s_grad, s_hit, t, acc)) continue;
       float gsum = 0.f;
 #pragma unroll
       for (int c = 0; c < 12; ++c) gsum += fabsf(acc[c]);
@@ -333,8 +330,6 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
         atomicAdd(g4 + 1, make_float4(acc[4], acc[5], acc[6], acc[7]));
         atomicAdd(reinterpret_cast<float4*>(out.dL_drgbs) + vid, make_float4(acc[8], acc[9], acc[10], acc[11]));
       }
-#pragma unroll
-      for (int c = 0; c < 12; ++c) acc[c] = 0.f;
     }
   }
 }
