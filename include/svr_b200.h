@@ -289,8 +289,11 @@ int svr_batch_plan_set_staging(svr_batch_plan* plan, int records);
 int svr_batch_plan_tile_size(const svr_batch_plan* plan);
 /* Backward gradient reduction inside a warp: a staged record's 12 gradient
  * values from at most atomic_lanes (1-32, default 1) contributing lanes are
- * added to its shared accumulator with atomics, from more lanes through a
- * 13-shuffle reduce-scatter.  Only the order of additions changes. */
+ * added to its shared accumulator with atomics, from up to 8 lanes by a
+ * transposition through shared memory, from more lanes through a 13-shuffle
+ * reduce-scatter.  Configurations that keep a slot per warp (at most two
+ * warps, 32 staged records) store one lane's values directly whatever the
+ * setting.  Only the order of additions changes. */
 int svr_batch_plan_set_reduction(svr_batch_plan* plan, int atomic_lanes);
 /* Arithmetic of the compositing loops of svr_batch_render / svr_batch_backward.
  * exact = 1: the reference's operations (forward.cu:243-253, backward.cu:309-333:

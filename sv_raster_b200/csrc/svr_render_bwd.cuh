@@ -92,17 +92,29 @@ __device__ __forceinline__ int warp_reduce_scatter12(float v[12], int lane) {
 // svr_common.cuh); RGB4 the [P,4] colour-gradient layout whose rows, like the
 // density rows, are flushed with one 16-byte vector reduction each.
 // Per-record gradient accumulators of one staging round.  With at most two
-// warps per CTA each warp owns a slot per staged record: a warp visits a
-// record at most once per round, so the record's warp total is stored with
-// plain stores, a bitmask per 32-record group marks the slots written this
-// round, and the flush adds the (at most two) slots -- no shared-memory
-// atomics and no zeroing.  Larger CTAs share one slot per record and add into
-// it with shared-memory atomics.
+// warps per CTA and 32 records staged per round, each warp owns a slot per
+// staged record: a warp visits a record at most once per round, so the
+// record's warp total is stored with plain stores, a bitmask per 32-record
+// group marks the slots written this round, and the flush adds the (at most
+// two) slots -- no shared-memory atomics and no zeroing.  Other
+// configurations share one slot per record and add into it with
+// shared-memory atomics (per-warp slots for 64 records would cost the 64-
+// thread CTAs their 16th resident CTA per SM: measured slower).
+//
+// A record reached by few lanes (2 to kFewLanes, a third of the records a
+// warp contributes to at 1080p over the c4 scene) is summed by transposing
+// through a small per-warp area instead of the 13-shuffle reduce-scatter:
+// each contributing lane stores its 12 values as one row, then lanes 0-11
+// each add one column over the rows.
 template <class CFG>
 struct GradAcc {
-  static constexpr bool kPerWarp = CFG::NW <= 2;
+  static constexpr bool kPerWarp = CFG::NW <= 2 && CFG::SB <= 32;
   static constexpr int kStride = kPerWarp ? 12 : kGradStride;  // 48-byte rows: 16-byte vector access
-  static constexpr int kFloats = (kPerWarp ? CFG::NW : 1) * CFG::SB * kStride;
+  static constexpr int kFewLanes = 8;
+  static constexpr int kSlots = (kPerWarp ? CFG::NW : 1) * CFG::SB * kStride;
+  // accumulators, then the transposition rows (16-byte aligned)
+  static constexpr int kRowsAt = (kSlots + 3) / 4 * 4;
+  static constexpr int kFloats = kRowsAt + CFG::NW * kFewLanes * 12;
   static constexpr int kWords = kPerWarp ? CFG::NW * CFG::GROUPS : 1;
 
   __device__ static void init(float* s_grad, int tid) {
@@ -114,36 +126,44 @@ struct GradAcc {
   // meaningful where `contrib`; act_mask: the contributing lanes).
   __device__ static void add(float* s_grad, int warp, int j, float gp[12], int lane, uint32_t act_mask,
                              bool contrib, int atomic_lanes) {
-    const bool reduce = kPerWarp ? __popc(act_mask) > 1 : __popc(act_mask) > atomic_lanes;
-    if (reduce && !contrib) {
-#pragma unroll
-      for (int c = 0; c < 12; ++c) gp[c] = 0.f;
-    }
-    if (kPerWarp) {
-      float* acc = s_grad + (warp * CFG::SB + j) * kStride;
-      if (!reduce) {
-        if (contrib) {
-          float4* a4 = reinterpret_cast<float4*>(acc);
-          a4[0] = make_float4(gp[0], gp[1], gp[2], gp[3]);
-          a4[1] = make_float4(gp[4], gp[5], gp[6], gp[7]);
-          a4[2] = make_float4(gp[8], gp[9], gp[10], gp[11]);
-        }
-      } else {
-        const int slot = warp_reduce_scatter12(gp, lane);
-        if (slot >= 0) acc[slot] = gp[0];
-      }
-    } else {
-      float* acc = s_grad + j * kStride;
-      if (!reduce) {  // few lanes: add their values directly
-        if (contrib) {
+    const int k = __popc(act_mask);
+    float* acc = s_grad + ((kPerWarp ? warp * CFG::SB : 0) + j) * kStride;
+    if (kPerWarp ? k == 1 : k <= atomic_lanes) {
+      if (contrib) {  // one (or, shared slots, a few) lane(s): their values go straight in
+        if (kPerWarp) store_row(acc, gp);
+        else
 #pragma unroll
           for (int c = 0; c < 12; ++c) atomicAdd(acc + c, gp[c]);
-        }
-      } else {
-        const int slot = warp_reduce_scatter12(gp, lane);
-        if (slot >= 0) atomicAdd(acc + slot, gp[0]);
+      }
+    } else if (k <= kFewLanes) {
+      float* rows = s_grad + kRowsAt + warp * kFewLanes * 12;
+      if (contrib) store_row(rows + 12 * __popc(act_mask & ((1u << lane) - 1u)), gp);
+      __syncwarp();
+      if (lane < 12) {
+        float sum = rows[lane];
+        for (int r = 1; r < k; ++r) sum += rows[12 * r + lane];
+        if (kPerWarp) acc[lane] = sum;
+        else atomicAdd(acc + lane, sum);
+      }
+      __syncwarp();  // the rows are reused by the warp's next record
+    } else {
+      if (!contrib) {
+#pragma unroll
+        for (int c = 0; c < 12; ++c) gp[c] = 0.f;
+      }
+      const int slot = warp_reduce_scatter12(gp, lane);
+      if (slot >= 0) {
+        if (kPerWarp) acc[slot] = gp[0];
+        else atomicAdd(acc + slot, gp[0]);
       }
     }
+  }
+
+  __device__ static void store_row(float* row, const float gp[12]) {
+    float4* a4 = reinterpret_cast<float4*>(row);
+    a4[0] = make_float4(gp[0], gp[1], gp[2], gp[3]);
+    a4[1] = make_float4(gp[4], gp[5], gp[6], gp[7]);
+    a4[2] = make_float4(gp[8], gp[9], gp[10], gp[11]);
   }
 
   // End of group g of a warp's hit loop: `wrote` marks the records it stored.

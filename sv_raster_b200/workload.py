@@ -593,13 +593,16 @@ class BatchedTrainWorkload:
         self.loss = torch.zeros((), device=dev)
         # one flat buffer for the exchanged gradients: densities (per-voxel corners or grid
         # points), sh0, shs; the subdivision priority is not exchanged
+        # (each part starts 256-byte aligned: the fused Adam reads 16-byte vectors)
         P = self.P
-        self.n_dens = 8 * P if self.grid is None else self.grid.numel()
-        nd = self.n_dens
-        self.flat_grad = torch.zeros(nd + P * (3 + 45), device=dev)
+        pad = lambda n: (n + 63) // 64 * 64
+        nd = 8 * P if self.grid is None else self.grid.numel()
+        self.n_dens = pad(nd)  # the density bucket, padding included
+        o_shs = self.n_dens + pad(3 * P)
+        self.flat_grad = torch.zeros(o_shs + 45 * P, device=dev)
         dgeo = self.flat_grad[:nd].view(P, 8) if self.grid is None else torch.zeros(P, 8, device=dev)
-        self.grads = (dgeo, torch.zeros(P, device=dev), self.flat_grad[nd:nd + 3 * P].view(P, 3),
-                      self.flat_grad[nd + 3 * P:].view(P, 15, 3))
+        self.grads = (dgeo, torch.zeros(P, device=dev), self.flat_grad[self.n_dens:self.n_dens + 3 * P].view(P, 3),
+                      self.flat_grad[o_shs:].view(P, 15, 3))
         dens = self.geos if self.grid is None else self.grid
         self.adam_grads = [self.flat_grad[:nd].view(dens.shape), self.grads[2], self.grads[3]]
         self.adam = DeviceAdam([dens, self.sh0, self.shs], [lr_geo, lr_sh, lr_sh], betas, eps)
@@ -621,7 +624,7 @@ class BatchedTrainWorkload:
         self.grads[0].zero_()
         r.backward_render(self.geos, self.T, self.dC, self.dT, self.grads[0])
         if self.grid is not None:
-            dgrid = self.flat_grad[:self.n_dens]
+            dgrid = self.flat_grad[:self.grid.numel()]
             dgrid.zero_()
             scatter_grid_grad(self.vox_key, self.grads[0], dgrid)
 
