@@ -286,6 +286,10 @@ int svr_batch_plan_set_binning(svr_batch_plan* plan, int binning);
  * 128, 256 (default) or 512 with 16x16 tiles, 32, 64 (default) or 128 with
  * 8x8, 256 with 32x32. */
 int svr_batch_plan_set_staging(svr_batch_plan* plan, int records);
+/* The backward's staging depth alone (same values; set_staging sets both):
+ * the backward keeps more per-record state in shared memory than the forward,
+ * so its best depth can be smaller. */
+int svr_batch_plan_set_backward_staging(svr_batch_plan* plan, int records);
 int svr_batch_plan_tile_size(const svr_batch_plan* plan);
 /* Backward gradient reduction inside a warp: a staged record's 12 gradient
  * values from at most atomic_lanes (1-32, default 1) contributing lanes are

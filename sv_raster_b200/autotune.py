@@ -18,6 +18,11 @@ gradients agree up to the order of floating-point additions):
 * ``reduce`` -- backward gradient reduction threshold: records touched by at
   most this many lanes of a warp add their gradients with shared-memory
   atomics instead of a warp reduce-scatter (``set_reduction``).
+* ``bstage`` -- the backward's own staging depth (0: the forward's), tuned
+  with the backward after the tile (``set_backward_staging``): the backward
+  holds more per-record state in shared memory, so a shallower staging round
+  can keep more CTAs resident.  Depths the tile size does not support are
+  skipped.
 * ``ppt`` -- pixels per compositing thread, 1 or 2 (two pixels of an 8x8
   warp block share each record's loads and, in the backward, its warp
   reduction; ``BatchedRasterizer.set_pixels_per_thread``), tuned with the
@@ -46,6 +51,7 @@ DEFAULT_SPACE = {
     "bwd": [(True, 0), (False, 0)],
     "reduce": [1, 2, 4, 8],
     "ppt": [1, 2],
+    "bstage": [0, 32, 64, 128, 256],
 }
 
 
@@ -75,7 +81,7 @@ def _store_cache(path, data):
 
 # Bumped whenever the search space or the kernels behind it change, so that
 # choices cached by an older build are measured again rather than reused.
-CACHE_SCHEMA = 4
+CACHE_SCHEMA = 5
 
 
 def cache_key(raster, geos, sh0):
@@ -117,6 +123,8 @@ def apply(raster, choice):
         raster.set_reduction(int(choice["reduce"]))
     if "ppt" in choice:
         raster.set_pixels_per_thread(int(choice["ppt"]))
+    if "bstage" in choice:
+        raster.set_backward_staging(int(choice["bstage"]) or None)
     f = choice.get("fwd", (True, 0))
     b = choice.get("bwd", (True, 0))
     raster.set_schedule(fwd_ordered=bool(f[0]), bwd_ordered=bool(b[0]), fwd_ctas_per_sm=int(f[1]),
@@ -172,18 +180,21 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
         dC, dT = upstream()
         state["grads"] = raster.backward(geos, state["out"][1], dC, dT, sh_degree, M, state.get("grads"))
 
-    stages = [("tile", step), ("ppt", step), ("bin", prepare), ("sort", prepare), ("fwd", render),
-              ("bwd", backward), ("reduce", backward)]
+    stages = [("tile", step), ("ppt", step), ("bstage", backward), ("bin", prepare), ("sort", prepare),
+              ("fwd", render), ("bwd", backward), ("reduce", backward)]
     for name, fn in stages:
         cands = space.get(name)
         if not cands:
             continue
         res = []
         for cand in cands:
-            apply(raster, dict(choice, **{name: cand}))
+            try:
+                apply(raster, dict(choice, **{name: cand}))
+            except RuntimeError:  # a value this tile configuration does not support
+                continue
             if name == "tile":
                 raster.fit_capacity(sh0, shs, sh_degree)
-            if name in ("fwd", "bwd", "reduce"):
+            if name in ("fwd", "bwd", "reduce", "bstage"):
                 raster.prepare(sh0, shs, sh_degree)
                 render()
             t = timer(fn, reps, warmup)

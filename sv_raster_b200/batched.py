@@ -59,6 +59,7 @@ class BatchedRasterizer:
         self.binning = 1
         self.exact = bool(exact)
         self.pixels_per_thread = 1
+        self.staging_bwd = None  # None: the forward's staging depth
         self._make_plan(0 if capacity is None else int(capacity))
         self.capacity_auto = capacity is None
 
@@ -86,6 +87,8 @@ class BatchedRasterizer:
         check(L.svr_batch_plan_set_arithmetic(plan, int(self.exact)), "batch_plan_set_arithmetic")
         check(L.svr_batch_plan_set_pixels_per_thread(plan, self.pixels_per_thread),
               "batch_plan_set_pixels_per_thread")
+        if self.staging_bwd is not None:
+            check(L.svr_batch_plan_set_backward_staging(plan, self.staging_bwd), "batch_plan_set_backward_staging")
 
     def set_binning(self, binning=1):
         """How prepare groups the instances by tile before the per-tile sort:
@@ -125,14 +128,23 @@ class BatchedRasterizer:
         if tile_size != self.tile_size:
             self.tile_size = tile_size
             self.staging = staging
+            self.staging_bwd = None
             self._make_plan(self.capacity)
         else:
             self.set_staging(staging)
 
     def set_staging(self, records):
-        """Records staged into shared memory per round (see svr_batch_plan_set_staging)."""
+        """Records staged into shared memory per round, forward and backward
+        (see svr_batch_plan_set_staging)."""
         check(lib().svr_batch_plan_set_staging(self.plan, int(records)), "batch_plan_set_staging")
         self.staging = int(records)
+        self.staging_bwd = None
+
+    def set_backward_staging(self, records=None):
+        """The backward's staging depth alone (None: the forward's)."""
+        r = self.staging if records is None else int(records)
+        check(lib().svr_batch_plan_set_backward_staging(self.plan, r), "batch_plan_set_backward_staging")
+        self.staging_bwd = None if records is None else r
 
     def set_sort_buckets(self, small_n=512, chunk=4096):
         """Segment-size buckets of the per-tile segment sort (small_n in

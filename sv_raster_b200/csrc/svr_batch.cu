@@ -383,6 +383,7 @@ struct svr_batch_plan {
   int seg_small_n, seg_chunk;  // segment-sort buckets (svr_batch_plan_set_sort_buckets)
   int tile_size;               // compositing tile size (8, 16 or 32), fixed at creation
   int stage;                   // records staged per round (svr_batch_plan_set_staging)
+  int stage_bwd;               // the backward's, when set apart (svr_batch_plan_set_backward_staging)
   int atomic_lanes;            // backward reduction threshold (svr_batch_plan_set_reduction)
   int exact;                   // compositing arithmetic (svr_batch_plan_set_arithmetic): 1 exact, 0 fast
   int pair;                    // two pixels per compositing thread (svr_batch_plan_set_pixels_per_thread)
@@ -478,6 +479,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   memset(&p->vt, 0, sizeof(p->vt));
   p->tile_size = tile_size;
   p->stage = tile_size == 8 ? 64 : 256;
+  p->stage_bwd = p->stage;
   p->V = n_views;
   p->P = P;
   p->cap = (size_t)capacity;
@@ -623,6 +625,13 @@ int svr_batch_plan_set_schedule(svr_batch_plan* p, int order_flags, int fwd_ctas
 int svr_batch_plan_set_staging(svr_batch_plan* p, int stage) {
   if (!p || !batch_tile_supported(p->tile_size, stage)) return SVR_ERR_SHAPE;
   p->stage = stage;
+  p->stage_bwd = stage;
+  return SVR_OK;
+}
+
+int svr_batch_plan_set_backward_staging(svr_batch_plan* p, int stage) {
+  if (!p || !batch_tile_supported(p->tile_size, stage)) return SVR_ERR_SHAPE;
+  p->stage_bwd = stage;
   return SVR_OK;
 }
 
@@ -820,7 +829,7 @@ int svr_batch_backward(svr_batch_plan* p, void* ws, const float* vox_centers, co
   if (ordered) build_tile_order(p, q, q.tile_last, q.order_bwd, stream);
   launch_render_bwd_batch(p->vt, (int)p->total_tiles, q.ranges, q.tile_last, p->cap > 0 ? q.vb : nullptr, va,
                           (int)p->P, (size_t)p->P * 3, (size_t)p->P * 4, in, out, p->n_samp, p->tile_size,
-                          p->stage, !p->exact, p->pair, ordered ? q.order_bwd : nullptr, q.header + 3,
+                          p->stage_bwd, !p->exact, p->pair, ordered ? q.order_bwd : nullptr, q.header + 3,
                           p->bwd_ctas_per_sm, stream);
   return check_last();
 }

@@ -33,6 +33,11 @@ class FakeRaster:
     def set_pixels_per_thread(self, n):
         self.pixels_per_thread = n
 
+    def set_backward_staging(self, n=None):
+        if n is not None and n not in ((32, 64, 128) if self.tile_size == 8 else (128, 256, 512)):
+            raise RuntimeError("staging depth not supported by this tile size")
+        self.staging_bwd = n
+
     def set_schedule(self, fwd_ordered=True, bwd_ordered=True, fwd_ctas_per_sm=0, bwd_ctas_per_sm=0):
         self.schedule = (int(fwd_ordered) | (int(bwd_ordered) << 1), fwd_ctas_per_sm, bwd_ctas_per_sm)
 
@@ -65,6 +70,7 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
         t -= 0.25 * (getattr(r, "atomic_lanes", 1) == 4)
         t -= 0.125 * (getattr(r, "binning", 1) == 0)
         t -= 0.0625 * (getattr(r, "pixels_per_thread", 1) == 2)
+        t -= 0.03125 * (getattr(r, "staging_bwd", None) == 32)
         return t
 
     geos = torch.zeros(r.P, 8)
@@ -82,7 +88,9 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
     assert res["choice"]["reduce"] == 4 and r.atomic_lanes == 4
     assert res["choice"]["bin"] == 0 and r.binning == 0
     assert res["choice"]["ppt"] == 2 and r.pixels_per_thread == 2
-    assert set(res["timings"]) == {"tile", "ppt", "bin", "sort", "fwd", "bwd", "reduce"}
+    assert res["choice"]["bstage"] == 32 and r.staging_bwd == 32
+    assert [c for c, _ in res["timings"]["bstage"]] == [0, 32, 64, 128]  # 256 needs 16x16 tiles
+    assert set(res["timings"]) == {"tile", "ppt", "bstage", "bin", "sort", "fwd", "bwd", "reduce"}
     # second call: served from the cache, applied, no timing
     r2 = FakeRaster()
     res2 = autotune.tune_batched(r2, geos, sh0, shs, 3, timer=lambda *a: 1 / 0)

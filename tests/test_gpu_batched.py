@@ -393,6 +393,25 @@ def test_tiling_and_schedule_do_not_change_results(c1, tile, stage, order, ctas,
         assert got[6] < base[6]
 
 
+@pytest.mark.parametrize("tile,stage,bstage", [(8, 64, 32), (8, 32, 128), (16, 256, 128)])
+def test_backward_staging_depth_does_not_change_results(c1, tile, stage, bstage):
+    """The backward's own staging depth (32 records: per-warp accumulators)
+    gives the same gradients up to the order of additions."""
+    g = torch.Generator(device="cuda").manual_seed(17)
+    r0, _ = _raster(c1, tile_size=tile)
+    r0.set_staging(stage)
+    wC = torch.randn(3 * r0.n_pixels, device="cuda", generator=g)
+    wT = torch.randn(r0.n_pixels, device="cuda", generator=g)
+    base = _render_and_grads(r0, c1, wC, wT)
+    r, _ = _raster(c1, tile_size=tile)
+    r.set_staging(stage)
+    r.set_backward_staging(bstage)
+    got = _render_and_grads(r, c1, wC, wT)
+    assert torch.equal(got[0], base[0])
+    for a, b, name in zip(got[2:6], base[2:6], ("dL_dgeos", "subdiv", "dL_dsh0", "dL_dshs")):
+        assert rel_err(a, b) < 1e-5, name
+
+
 def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
     from sv_raster_b200.autotune import tune_batched
     monkeypatch.setenv("SVR_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
@@ -403,7 +422,8 @@ def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
     base = _render_and_grads(r0, c1, wC, wT)
     r, _ = _raster(c1)
     res = tune_batched(r, c1.geos, c1.sh0, c1.shs, 3, reps=2, warmup=1)
-    assert not res["cached"] and set(res["choice"]) == {"tile", "ppt", "bin", "sort", "fwd", "bwd", "reduce"}
+    assert not res["cached"] and set(res["choice"]) == {"tile", "ppt", "bstage", "bin", "sort", "fwd", "bwd",
+                                                        "reduce"}
     got = _render_and_grads(r, c1, wC, wT)
     assert torch.equal(got[0], base[0])
     assert rel_err(got[2], base[2]) < 1e-5
