@@ -54,8 +54,8 @@ def parse():
     ap.add_argument("--no-tune", action="store_true",
                     help="batched mode: default launch parameters instead of the autotuner's choice")
     ap.add_argument("--tile", default=None,
-                    help="batched mode: fixed compositing tile 'TS' or 'TS,SB' (8,64 | 16,128|256|512 | 32,256); "
-                         "no autotuning")
+                    help="batched mode: fixed compositing tile 'TS', 'TS,SB' or 'TS,SB,SB_backward' (8,64 | "
+                         "16,128|256|512 | 32,256; the backward's staging depth apart); no autotuning")
     ap.add_argument("--exact", action="store_true",
                     help="batched mode: the exact compositing arithmetic (bit-identical to the plain path) instead "
                          "of the default fast form")
@@ -183,7 +183,7 @@ def main():
         tile = None
         if args.tile:
             parts = [int(x) for x in args.tile.split(",")]
-            tile = (parts[0], parts[1] if len(parts) > 1 else (64 if parts[0] == 8 else 256))
+            tile = (parts[0], parts[1] if len(parts) > 1 else (64 if parts[0] == 8 else 256)) + tuple(parts[2:3])
         wl = workload.BatchedWorkload(sc, dev, tune=not (args.no_tune or tile), tile=tile, exact=args.exact)
     n_views = len(sc.cameras)
 
@@ -235,7 +235,10 @@ def main():
         e2e = wl.e2e(args.steps, args.warmup)
         e2e["ms_total"] = workload.max_over_ranks(e2e["ms_total"], device=dev)
     r = getattr(wl, "raster", None)
-    tile_key = f"{r.tile_size},{r.staging}" if r is not None else "16,256"
+    # committed-capture lookup keys of the compositing kernels: tile size and staging depth
+    tile_keys = ({"render_fwd": f"{r.tile_size},{r.staging}",
+                  "render_bwd": f"{r.tile_size},{r.staging_bwd or r.staging}"} if r is not None else
+                 {"render_fwd": "16,256", "render_bwd": "16,256"})
     inst_per_view = wl.instances_per_view()
     launches = wl.launches_per_step()
     tuned = getattr(wl, "tuned", None)
@@ -267,7 +270,7 @@ def main():
         issue = None
         tf = os.path.join(ROOT, "profiles", "render_traffic.json")
         if os.path.exists(tf) and dom["name"] in ("render_fwd", "render_bwd"):
-            t = json.load(open(tf))["tiles"].get(tile_key)
+            t = json.load(open(tf))["tiles"].get(tile_keys[dom["name"]])
             if t is not None:
                 inst = inst_per_view * (n_views if args.mode == "batched" else 1)
                 traffic = round(t[dom["name"]]["dram_bytes"] / t["instances_per_launch"] * inst)

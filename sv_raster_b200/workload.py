@@ -266,7 +266,9 @@ class BatchedWorkload:
                                         max_level=scene.max_level, exact=exact)
         self.tuned = None
         if tile is not None:
-            self.raster.set_tile_size(*tile)
+            self.raster.set_tile_size(*tile[:2])
+            if len(tile) > 2:
+                self.raster.set_backward_staging(tile[2])
             self.tuned = {"tile": list(tile), "fixed": True}
         self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
         if tune:
