@@ -23,6 +23,10 @@ gradients agree up to the order of floating-point additions):
   holds more per-record state in shared memory, so a shallower staging round
   can keep more CTAs resident.  Depths the tile size does not support are
   skipped.
+* ``fstage`` -- the forward's staging depth once the backward's is set apart
+  (0: the tile's own), timed with the forward alone; the tile stage times
+  both kernels with one depth, and the two kernels prefer different ones
+  (c4: forward 64, backward 32 records).
 * ``ppt`` -- pixels per compositing thread, 1 or 2 (two pixels of an 8x8
   warp block share each record's loads and, in the backward, its warp
   reduction; ``BatchedRasterizer.set_pixels_per_thread``), tuned with the
@@ -52,6 +56,7 @@ DEFAULT_SPACE = {
     "reduce": [1, 2, 4, 8],
     "ppt": [1, 2],
     "bstage": [0, 32, 64, 128, 256],
+    "fstage": [0, 32, 64, 128, 256, 512],
 }
 
 
@@ -81,7 +86,7 @@ def _store_cache(path, data):
 
 # Bumped whenever the search space or the kernels behind it change, so that
 # choices cached by an older build are measured again rather than reused.
-CACHE_SCHEMA = 5
+CACHE_SCHEMA = 6
 
 
 def cache_key(raster, geos, sh0):
@@ -123,6 +128,8 @@ def apply(raster, choice):
         raster.set_reduction(int(choice["reduce"]))
     if "ppt" in choice:
         raster.set_pixels_per_thread(int(choice["ppt"]))
+    if int(choice.get("fstage", 0)):
+        raster.set_staging(int(choice["fstage"]))  # (resets the backward's; set again below)
     if "bstage" in choice:
         raster.set_backward_staging(int(choice["bstage"]) or None)
     f = choice.get("fwd", (True, 0))
@@ -180,8 +187,8 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
         dC, dT = upstream()
         state["grads"] = raster.backward(geos, state["out"][1], dC, dT, sh_degree, M, state.get("grads"))
 
-    stages = [("tile", step), ("ppt", step), ("bstage", backward), ("bin", prepare), ("sort", prepare),
-              ("fwd", render), ("bwd", backward), ("reduce", backward)]
+    stages = [("tile", step), ("ppt", step), ("bstage", backward), ("fstage", render), ("bin", prepare),
+              ("sort", prepare), ("fwd", render), ("bwd", backward), ("reduce", backward)]
     for name, fn in stages:
         cands = space.get(name)
         if not cands:
@@ -194,13 +201,15 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
                 continue
             if name == "tile":
                 raster.fit_capacity(sh0, shs, sh_degree)
-            if name in ("fwd", "bwd", "reduce", "bstage"):
+            if name in ("fwd", "bwd", "reduce", "bstage", "fstage"):
                 raster.prepare(sh0, shs, sh_degree)
                 render()
             t = timer(fn, reps, warmup)
             res.append((t, cand))
         timings[name] = [[c if not isinstance(c, tuple) else list(c), round(t, 4)] for t, c in res]
         choice[name] = min(res, key=lambda x: x[0])[1]
+        if name in ("bstage", "fstage") and not choice[name]:
+            choice[name] = raster.staging  # "as the tile's" made concrete: later stages may change it
         apply(raster, choice)
         if name == "tile":
             raster.fit_capacity(sh0, shs, sh_degree)

@@ -20,6 +20,12 @@ class FakeRaster:
 
     def set_tile_size(self, t, s=None):
         self.tile_size, self.staging = t, s
+        self.staging_bwd = None
+
+    def set_staging(self, s):
+        if s not in ((32, 64, 128) if self.tile_size == 8 else (128, 256, 512)):
+            raise RuntimeError("staging depth not supported by this tile size")
+        self.staging, self.staging_bwd = s, None
 
     def set_sort_buckets(self, a, b):
         self.sort_buckets = (a, b)
@@ -71,6 +77,7 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
         t -= 0.125 * (getattr(r, "binning", 1) == 0)
         t -= 0.0625 * (getattr(r, "pixels_per_thread", 1) == 2)
         t -= 0.03125 * (getattr(r, "staging_bwd", None) == 32)
+        t -= 0.015625 * (r.staging == 128 and getattr(r, "staging_bwd", None) == 32)
         return t
 
     geos = torch.zeros(r.P, 8)
@@ -83,14 +90,16 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
     assert res["choice"]["fwd"] == (False, 0)
     assert res["choice"]["bwd"] == (True, 3)
     # the chosen parameters are left applied
-    assert (r.tile_size, r.staging, r.sort_buckets) == (8, 64, (256, 4096))
+    assert (r.tile_size, r.staging, r.sort_buckets) == (8, 128, (256, 4096))  # forward depth re-tuned
     assert r.schedule == (2, 0, 3)
     assert res["choice"]["reduce"] == 4 and r.atomic_lanes == 4
     assert res["choice"]["bin"] == 0 and r.binning == 0
     assert res["choice"]["ppt"] == 2 and r.pixels_per_thread == 2
     assert res["choice"]["bstage"] == 32 and r.staging_bwd == 32
     assert [c for c, _ in res["timings"]["bstage"]] == [0, 32, 64, 128]  # 256 needs 16x16 tiles
-    assert set(res["timings"]) == {"tile", "ppt", "bstage", "bin", "sort", "fwd", "bwd", "reduce"}
+    # the forward's own depth, re-tuned with the backward's kept
+    assert res["choice"]["fstage"] == 128 and r.staging == 128 and r.staging_bwd == 32
+    assert set(res["timings"]) == {"tile", "ppt", "bstage", "fstage", "bin", "sort", "fwd", "bwd", "reduce"}
     # second call: served from the cache, applied, no timing
     r2 = FakeRaster()
     res2 = autotune.tune_batched(r2, geos, sh0, shs, 3, timer=lambda *a: 1 / 0)
