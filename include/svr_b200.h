@@ -309,6 +309,18 @@ int svr_batch_plan_set_reduction(svr_batch_plan* plan, int atomic_lanes);
  * form to fp32 accumulation error (a pixel may stop one voxel earlier or later
  * where its transmittance lands on the 1e-4 early-stop threshold). */
 int svr_batch_plan_set_arithmetic(svr_batch_plan* plan, int exact);
+/* Pixel bbox of each (view, voxel) pair written by svr_batch_prepare.
+ * culling = 0: the reference's bbox, each side of the projected corners'
+ * extent rounded to the nearest pixel (preprocess.cu:98-113); tile lists and
+ * contributor counts are the plain path's.  culling = 1: the pixels of that
+ * bbox whose centre lies within 0.05 pixel of the unrounded extent, for voxels
+ * with all 8 corners in front of the near plane -- every other pixel's ray
+ * provably misses the cube, so the lists lose instances that contribute
+ * nothing; a voxel left with no pixel centre is culled for that view (n_dup 0).
+ * Images, T and gradients are unchanged; contributor counts (list positions)
+ * shrink.  culling = -1 (default): 1 with the fast arithmetic, 0 with the
+ * exact one. */
+int svr_batch_plan_set_culling(svr_batch_plan* plan, int culling);
 /* Pixels per thread of the compositing kernels: 1 (default) or 2 (a warp
  * covers an 8x8 block, each lane two pixels four rows apart; a record's
  * shared-memory fields are read once for both and, in the backward, one warp

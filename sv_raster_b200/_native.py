@@ -94,6 +94,7 @@ _SIGS = {
     "svr_batch_plan_tile_size": (c_int, [c_p]),
     "svr_batch_plan_set_reduction": (c_int, [c_p, c_int]),
     "svr_batch_plan_set_arithmetic": (c_int, [c_p, c_int]),
+    "svr_batch_plan_set_culling": (c_int, [c_p, c_int]),
     "svr_batch_plan_set_backward_staging": (c_int, [c_p, c_int]),
     "svr_batch_plan_set_pixels_per_thread": (c_int, [c_p, c_int]),
     "svr_batch_plan_set_binning": (c_int, [c_p, c_int]),

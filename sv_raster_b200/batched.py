@@ -59,6 +59,7 @@ class BatchedRasterizer:
         self.binning = 1
         self.exact = bool(exact)
         self.pixels_per_thread = 1
+        self.culling = -1  # -1: tight bbox with the fast arithmetic, the rounded one with the exact
         self.staging_bwd = None  # None: the forward's staging depth
         self._make_plan(0 if capacity is None else int(capacity))
         self.capacity_auto = capacity is None
@@ -85,6 +86,7 @@ class BatchedRasterizer:
         check(L.svr_batch_plan_set_reduction(plan, self.atomic_lanes), "batch_plan_set_reduction")
         check(L.svr_batch_plan_set_binning(plan, self.binning), "batch_plan_set_binning")
         check(L.svr_batch_plan_set_arithmetic(plan, int(self.exact)), "batch_plan_set_arithmetic")
+        check(L.svr_batch_plan_set_culling(plan, self.culling), "batch_plan_set_culling")
         check(L.svr_batch_plan_set_pixels_per_thread(plan, self.pixels_per_thread),
               "batch_plan_set_pixels_per_thread")
         if self.staging_bwd is not None:
@@ -111,6 +113,16 @@ class BatchedRasterizer:
         loops (see svr_batch_plan_set_arithmetic)."""
         check(lib().svr_batch_plan_set_arithmetic(self.plan, int(bool(exact))), "batch_plan_set_arithmetic")
         self.exact = bool(exact)
+
+    def set_culling(self, culling=-1):
+        """Pixel bbox of each (view, voxel) pair: 0 the reference's rounded
+        bbox (the plain path's tile lists), 1 only the pixels whose centre ray
+        can meet the cube (fewer instances, same images and gradients), -1
+        tight with the fast arithmetic and rounded with the exact one (see
+        svr_batch_plan_set_culling).  Re-fit the capacity after switching from
+        tight to rounded."""
+        check(lib().svr_batch_plan_set_culling(self.plan, int(culling)), "batch_plan_set_culling")
+        self.culling = int(culling)
 
     def set_pixels_per_thread(self, pixels=1):
         """Pixels per compositing thread, 1 or 2 (see

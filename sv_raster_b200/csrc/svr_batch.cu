@@ -62,7 +62,7 @@ template <int DEG, typename TS>
 __global__ void __launch_bounds__(128)
 project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* __restrict__ centers,
                   const float* __restrict__ lengths, const TS* __restrict__ sh0, const TS* __restrict__ shs, int M,
-                  const int64_t* __restrict__ octpaths, int level_low_bits, uint32_t* __restrict__ ndup,
+                  const int64_t* __restrict__ octpaths, int level_low_bits, int tight, uint32_t* __restrict__ ndup,
                   uint2* __restrict__ bboxes, uint32_t* __restrict__ quads, float* __restrict__ rgbs,
                   uint32_t* __restrict__ err) {
   constexpr int NB = (DEG + 1) * (DEG + 1) - 1;  // rest coefficients per channel
@@ -85,7 +85,8 @@ project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* _
   for (int v = 0; v < views.n; ++v) {
     const size_t o = (size_t)v * P + i;
     const float* m = s_m[v];
-    const Projection pr = project_voxel(views.v[v], m, m + 12, cx, cy, cz, len);
+    Projection pr = project_voxel(views.v[v], m, m + 12, cx, cy, cz, len);
+    if (tight) tighten_bbox(views.v[v], pr);
     ndup[o] = pr.n;
     bboxes[o] = pr.bbox;
     quads[o] = pr.quads;
@@ -387,6 +388,7 @@ struct svr_batch_plan {
   int atomic_lanes;            // backward reduction threshold (svr_batch_plan_set_reduction)
   int exact;                   // compositing arithmetic (svr_batch_plan_set_arithmetic): 1 exact, 0 fast
   int pair;                    // two pixels per compositing thread (svr_batch_plan_set_pixels_per_thread)
+  int culling;                 // pixel bbox (svr_batch_plan_set_culling): -1 follows exact, 0 rounded, 1 tight
   int binning;                 // 1: counting sort by tile, 0: radix over the tile bits (svr_batch_plan_set_binning)
   // workspace layout (byte offsets)
   size_t o_header, o_ndup, o_scan, o_bbox, o_quad, o_scan_tmp, o_rgbs, o_drgbs;
@@ -595,6 +597,7 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->atomic_lanes = 1;
   p->exact = 0;
   p->pair = 0;
+  p->culling = -1;
   p->binning = 1;
   ensure_segsort_attributes();
   ensure_fwd_batch_attributes();
@@ -646,6 +649,12 @@ int svr_batch_plan_set_pixels_per_thread(svr_batch_plan* p, int pixels) {
 int svr_batch_plan_set_arithmetic(svr_batch_plan* p, int exact) {
   if (!p || (exact != 0 && exact != 1)) return SVR_ERR_SHAPE;
   p->exact = exact;
+  return SVR_OK;
+}
+
+int svr_batch_plan_set_culling(svr_batch_plan* p, int culling) {
+  if (!p || culling < -1 || culling > 1) return SVR_ERR_SHAPE;
+  p->culling = culling;
   return SVR_OK;
 }
 
@@ -711,16 +720,17 @@ int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, 
   cudaMemsetAsync(q.header, 0, kHeaderWords * sizeof(uint32_t), stream);
   const dim3 pgrid((P + 127) / 128);
   const int level_low = (p->rank_bits == kRankBits) ? 0 : kRankBits - (p->rank_bits - 3);  // 3*(16-L)
+  const int tight = p->culling < 0 ? !p->exact : p->culling;
 #define SVR_PROJ(D)                                                                                           \
   if (sh_bf16)                                                                                                \
     project_sh_kernel<D, __nv_bfloat16><<<pgrid, 128, 0, stream>>>(                                           \
         p->vt, P, vox_centers, vox_lengths, (const __nv_bfloat16*)sh0, (const __nv_bfloat16*)shs, M,         \
-        octree_paths, level_low, q.ndup, q.bbox, q.quad, q.rgbs, q.header + 1);                               \
+        octree_paths, level_low, tight, q.ndup, q.bbox, q.quad, q.rgbs, q.header + 1);                        \
   else                                                                                                        \
     project_sh_kernel<D, float><<<pgrid, 128, 0, stream>>>(p->vt, P, vox_centers, vox_lengths,               \
                                                            (const float*)sh0, (const float*)shs, M,          \
-                                                           octree_paths, level_low, q.ndup, q.bbox, q.quad,  \
-                                                           q.rgbs, q.header + 1);
+                                                           octree_paths, level_low, tight, q.ndup, q.bbox,   \
+                                                           q.quad, q.rgbs, q.header + 1);
   const dim3 grid((P + 255) / 256, p->V);
   switch (sh_degree) {
     case 0: SVR_PROJ(0) break;

@@ -183,8 +183,10 @@ def test_fast_arithmetic_matches_exact(c1, views):
     approximate division) against the exact form that is bit-identical to the
     plain path: images within 1e-5 norm-wise (a pixel whose transmittance
     lands on the early-stop threshold may take one voxel more or less, at most
-    about 1e-4 of colour), contributor counts equal almost everywhere, and
-    gradients within 1e-5."""
+    about 1e-4 of colour), contributor counts equal almost everywhere (on the
+    reference's rounded bbox; the default tight bbox of the fast form shortens
+    the lists, so its counts are compared by the culling test), and gradients
+    within 1e-5."""
     if views == "c3":
         C = SceneTensors(synthetic.cached_config_scene("c3"))
         cams = [DevCam(C.scene.cameras[i]) for i in (0, 5)]
@@ -193,19 +195,22 @@ def test_fast_arithmetic_matches_exact(c1, views):
         cams = [DevCam(C.scene.cameras[i]) for i in views]
     out = {}
     g = torch.Generator(device="cuda").manual_seed(13)
-    for exact in (True, False):
+    for exact, culling in ((True, -1), (False, -1), (False, 0)):
         r = BatchedRasterizer(cams, C.octpath, C.centers, C.lengths, max_level=C.scene.max_level, tile_size=8,
                               exact=exact)
+        r.set_culling(culling)
         if "wC" not in out:
             out["wC"] = torch.randn(3 * r.n_pixels, device="cuda", generator=g) * 1e-3
             out["wT"] = torch.randn(r.n_pixels, device="cuda", generator=g) * 1e-3
         res = _render_and_grads(r, C, out["wC"], out["wT"])
-        out[exact] = res + (r.arrays()["n_contrib"].clone(),)
+        out[exact, culling] = res + (r.arrays()["n_contrib"].clone(),)
         del r
-    e, f = out[True], out[False]
+    e, f, f0 = out[True, -1], out[False, -1], out[False, 0]
     img_rel = rel_err(f[0], e[0])
     img_max = (f[0] - e[0]).abs().max().item()
-    nc_mism = (f[7] != e[7]).float().mean().item()
+    nc_mism = (f0[7] != e[7]).float().mean().item()
+    assert f[6] < f0[6] == e[6]  # the tight bbox drops instances
+    assert rel_err(f0[0], e[0]) < 1e-5
     grads = {name: rel_err(a, b) for a, b, name in zip(f[2:6], e[2:6], ("dL_dgeos", "subdiv", "dL_dsh0", "dL_dshs"))}
     print(f"fast vs exact ({views}): image rel {img_rel:.2e}, max {img_max:.2e}, n_contrib mismatch {nc_mism:.2e}, "
           + ", ".join(f"{k} {v:.2e}" for k, v in grads.items()))
@@ -214,6 +219,46 @@ def test_fast_arithmetic_matches_exact(c1, views):
     assert nc_mism < 1e-3
     for k, v in grads.items():
         assert v < 1e-5, k
+
+
+@pytest.mark.parametrize("views,tile,exact", [((0, 1, 2), 8, True), ((0, 1, 2), 8, False), ((0, 1, 2), 16, True),
+                                              ("c3", 8, False)])
+def test_tight_bbox_culls_only_missing_rays(c1, views, tile, exact):
+    """The tight pixel bbox (pixel centres within 0.05 pixel of the projected
+    corners' extent) against the reference's rounded bbox, with the same
+    arithmetic: the dropped (tile, voxel) instances are ones whose rays all
+    miss the cube, so images and T are bit-identical, gradients agree up to
+    the order of additions, every voxel's duplicate count can only shrink,
+    and each pixel's last contributor sits no later in its shorter list."""
+    if views == "c3":
+        C = SceneTensors(synthetic.cached_config_scene("c3"))
+        cams = [DevCam(C.scene.cameras[i]) for i in (0, 5)]
+    else:
+        C = c1
+        cams = [DevCam(C.scene.cameras[i]) for i in views]
+    g = torch.Generator(device="cuda").manual_seed(19)
+    out = {}
+    for culling in (0, 1):
+        r = BatchedRasterizer(cams, C.octpath, C.centers, C.lengths, max_level=C.scene.max_level, tile_size=tile,
+                              exact=exact)
+        r.set_culling(culling)
+        if "wC" not in out:
+            out["wC"] = torch.randn(3 * r.n_pixels, device="cuda", generator=g)
+            out["wT"] = torch.randn(r.n_pixels, device="cuda", generator=g)
+        res = _render_and_grads(r, C, out["wC"], out["wT"])
+        arr = r.arrays()
+        out[culling] = res + (arr["n_contrib"].clone(), arr["ndup"].clone())
+        del r
+    ref, tight = out[0], out[1]
+    print(f"tight bbox ({views}, {tile}x{tile}, {'exact' if exact else 'fast'}): {tight[6]} of {ref[6]} instances "
+          f"({1 - tight[6] / ref[6]:.1%} dropped)")
+    assert tight[6] < ref[6]
+    assert torch.equal(tight[0], ref[0]), "colour differs"
+    assert torch.equal(tight[1], ref[1]), "T differs"
+    for a, b, name in zip(tight[2:6], ref[2:6], ("dL_dgeos", "subdiv", "dL_dsh0", "dL_dshs")):
+        assert rel_err(a, b) < 1e-5, name
+    assert bool((tight[7] <= ref[7]).all())
+    assert bool((tight[8] <= ref[8]).all())
 
 
 def _psnr(a, b):

@@ -5,7 +5,8 @@ that do not depend on the size (the oracle is too slow at these sizes):
   the instances into per-tile ranges, every tile list is strictly increasing
   in Morton rank and holds only instances whose bbox touches the tile; the
   counting sort and the radix grouping produce the same instance array;
-  images and T are bit-identical between 8x8 and 16x16 tiles; the backward is
+  images and T are bit-identical between 8x8 and 16x16 tiles and between the
+  tight and the rounded pixel bbox; the backward is
   linear in the upstream gradient; no device error flag is raised.
 * c3 (2M voxels, 16 uneven views): every view of the batched path (exact
   arithmetic) is bit-identical to the plain per-view path (fp32 storage).
@@ -130,6 +131,16 @@ def test_c4_fullsize_binning_tiling_and_linearity(c4):
     assert r16.header()[1] == 0
     assert torch.equal(color16, color8)
     assert torch.equal(T16, T8)
+    # the reference's rounded pixel bbox: more instances, the same images
+    r16.set_culling(0)
+    r16.fit_capacity(c4["sh0"], c4["shs"], 3)
+    r16.prepare(c4["sh0"], c4["shs"], 3)
+    color16r, T16r = r16.render(c4["geos"])
+    torch.cuda.synchronize()
+    total16r, err = r16.header()
+    assert err == 0
+    assert torch.equal(color16r, color8)
+    assert torch.equal(T16r, T8)
 
 
 def test_c3_fullsize_batched_views_equal_plain():

@@ -166,7 +166,11 @@ def test_batched_bf16_c4_view_matches_reference_on_rounded_inputs(ref, exact, pp
                                False, False, False, False, C.octpath, C.centers, C.lengths, geos32, rgbs, geom, False)
     rcolor, rT = out[3], out[6]
     brgbs = r.arrays()["rgbs"][0]
-    rgb_bitwise = bool(torch.equal(brgbs[vis], rgbs[vis]))
+    # the fast arithmetic's tight pixel bbox culls a voxel whose rays all miss
+    # (no colour computed); every voxel it keeps is one the reference keeps
+    bvis = torch.where(r.arrays()["ndup"][0] > 0)[0]
+    assert bool((ndup[bvis] > 0).all()) and (len(bvis) == len(vis) if exact else len(bvis) <= len(vis))
+    rgb_bitwise = bool(torch.equal(brgbs[bvis], rgbs[bvis]))
     img_max = (color - rcolor).abs().max().item()
     img_rel = rel_err(color, rcolor)
     t_max = (T - rT).abs().max().item()
