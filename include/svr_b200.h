@@ -328,6 +328,11 @@ int svr_batch_plan_set_culling(svr_batch_plan* plan, int culling);
  * 16x16 tiles staging 128 or 256; other tile configurations run one pixel
  * per thread.  Images, T and contributor counts do not depend on it. */
 int svr_batch_plan_set_pixels_per_thread(svr_batch_plan* plan, int pixels);
+/* Pixels per thread of svr_batch_backward alone: 1 or 2, or 0 to follow
+ * svr_batch_plan_set_pixels_per_thread (default).  The forward walks each
+ * pixel's own records with one pixel per thread, while the backward's warp
+ * reduction favours two, so the best choices can differ. */
+int svr_batch_plan_set_backward_pixels_per_thread(svr_batch_plan* plan, int pixels);
 int64_t svr_batch_plan_pixels(const svr_batch_plan* plan);
 int64_t svr_batch_plan_tiles(const svr_batch_plan* plan);
 int svr_batch_plan_groups(const svr_batch_plan* plan);

@@ -29,8 +29,12 @@ gradients agree up to the order of floating-point additions):
   (c4: forward 64, backward 32 records).
 * ``ppt`` -- pixels per compositing thread, 1 or 2 (two pixels of an 8x8
   warp block share each record's loads and, in the backward, its warp
-  reduction; ``BatchedRasterizer.set_pixels_per_thread``), tuned with the
-  full step after the tile.
+  reduction; ``BatchedRasterizer.set_pixels_per_thread``), timed with the
+  forward after the tile.
+* ``bppt`` -- the backward's own pixels per thread (0: as ``ppt``), timed
+  with the backward: the forward walks each pixel's own records, which two
+  pixels per thread cannot, while the backward's warp reduction favours two
+  (``set_backward_pixels_per_thread``).
 * ``tile`` -- compositing tile size of the batched path (8, 16 or 32 pixels)
   with the voxel-staging depth (records staged into shared memory per round)
   (``BatchedRasterizer.set_tile_size``; the tile size changes the binning, so
@@ -55,6 +59,7 @@ DEFAULT_SPACE = {
     "bwd": [(True, 0), (False, 0)],
     "reduce": [1, 2, 4, 8],
     "ppt": [1, 2],
+    "bppt": [0, 1, 2],
     "bstage": [0, 32, 64, 128, 256],
     "fstage": [0, 32, 64, 128, 256, 512],
 }
@@ -86,7 +91,7 @@ def _store_cache(path, data):
 
 # Bumped whenever the search space or the kernels behind it change, so that
 # choices cached by an older build are measured again rather than reused.
-CACHE_SCHEMA = 6
+CACHE_SCHEMA = 7
 
 
 def cache_key(raster, geos, sh0):
@@ -128,6 +133,8 @@ def apply(raster, choice):
         raster.set_reduction(int(choice["reduce"]))
     if "ppt" in choice:
         raster.set_pixels_per_thread(int(choice["ppt"]))
+    if "bppt" in choice:
+        raster.set_backward_pixels_per_thread(int(choice["bppt"]) or None)
     if int(choice.get("fstage", 0)):
         raster.set_staging(int(choice["fstage"]))  # (resets the backward's; set again below)
     if "bstage" in choice:
@@ -187,7 +194,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
         dC, dT = upstream()
         state["grads"] = raster.backward(geos, state["out"][1], dC, dT, sh_degree, M, state.get("grads"))
 
-    stages = [("tile", step), ("ppt", step), ("bstage", backward), ("fstage", render), ("bin", prepare),
+    stages = [("tile", step), ("ppt", render), ("bppt", backward), ("bstage", backward), ("fstage", render), ("bin", prepare),
               ("sort", prepare), ("fwd", render), ("bwd", backward), ("reduce", backward)]
     for name, fn in stages:
         cands = space.get(name)
@@ -201,7 +208,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
                 continue
             if name == "tile":
                 raster.fit_capacity(sh0, shs, sh_degree)
-            if name in ("fwd", "bwd", "reduce", "bstage", "fstage"):
+            if name in ("ppt", "bppt", "fwd", "bwd", "reduce", "bstage", "fstage"):
                 raster.prepare(sh0, shs, sh_degree)
                 render()
             t = timer(fn, reps, warmup)
@@ -210,6 +217,8 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
         choice[name] = min(res, key=lambda x: x[0])[1]
         if name in ("bstage", "fstage") and not choice[name]:
             choice[name] = raster.staging  # "as the tile's" made concrete: later stages may change it
+        if name == "bppt" and not choice[name]:
+            choice[name] = choice["ppt"]
         apply(raster, choice)
         if name == "tile":
             raster.fit_capacity(sh0, shs, sh_degree)

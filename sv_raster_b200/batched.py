@@ -59,6 +59,7 @@ class BatchedRasterizer:
         self.binning = 1
         self.exact = bool(exact)
         self.pixels_per_thread = 1
+        self.pixels_per_thread_bwd = None  # None: as pixels_per_thread
         self.culling = -1  # -1: tight bbox with the fast arithmetic, the rounded one with the exact
         self.staging_bwd = None  # None: the forward's staging depth
         self._make_plan(0 if capacity is None else int(capacity))
@@ -89,6 +90,8 @@ class BatchedRasterizer:
         check(L.svr_batch_plan_set_culling(plan, self.culling), "batch_plan_set_culling")
         check(L.svr_batch_plan_set_pixels_per_thread(plan, self.pixels_per_thread),
               "batch_plan_set_pixels_per_thread")
+        check(L.svr_batch_plan_set_backward_pixels_per_thread(plan, self.pixels_per_thread_bwd or 0),
+              "batch_plan_set_backward_pixels_per_thread")
         if self.staging_bwd is not None:
             check(L.svr_batch_plan_set_backward_staging(plan, self.staging_bwd), "batch_plan_set_backward_staging")
 
@@ -130,6 +133,13 @@ class BatchedRasterizer:
         beyond the order of gradient additions."""
         check(lib().svr_batch_plan_set_pixels_per_thread(self.plan, int(pixels)), "batch_plan_set_pixels_per_thread")
         self.pixels_per_thread = int(pixels)
+
+    def set_backward_pixels_per_thread(self, pixels=None):
+        """Pixels per thread of the backward alone, 1 or 2 (None: as
+        set_pixels_per_thread)."""
+        check(lib().svr_batch_plan_set_backward_pixels_per_thread(self.plan, int(pixels or 0)),
+              "batch_plan_set_backward_pixels_per_thread")
+        self.pixels_per_thread_bwd = int(pixels) if pixels else None
 
     def set_tile_size(self, tile_size, staging=None):
         """Compositing tile size (8, 16 or 32 pixels) and records staged per

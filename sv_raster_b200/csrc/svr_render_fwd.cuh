@@ -7,8 +7,9 @@
 // distortion / normal accumulation (:256-313), early stop at T < 1e-4
 // (:315-316), median-depth refinement (:328-364) and outputs (:368-391).
 // Differences are in scheduling only: SoA staging, warp-ballot culling of the
-// staged batch, a single pass per pixel instead of the collect-then-process
-// two-pass with a 256-entry local array, and a CTA reduction for tile_last.
+// staged batch, each lane walking its own pixel's records of the batch, a
+// single pass per pixel instead of the collect-then-process two-pass with a
+// 256-entry local array, and a CTA reduction for tile_last.
 #pragma once
 
 #include "svr_render.cuh"
@@ -74,11 +75,21 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
       const int slot = g * 32 + (tid & 31);
       const bool hit = slot < n_here && record_hits_warp(s, slot, wx0, wy0, quad_mask);
       uint32_t m = __ballot_sync(0xffffffffu, hit);
-      while (m) {
-        const int j = g * 32 + __ffs(m) - 1;
-        m &= m - 1;
-        if (done) continue;
-        if (!record_hits_pixel(s, j, px, py, ray.quad)) continue;
+      // This pixel's records among those: each lane then walks its own list
+      // in order, so one warp iteration serves a different record per lane
+      // (a warp takes as many iterations as its busiest pixel has records,
+      // not one per record that touches it).
+      uint32_t mine = 0u;
+      if (!done) {
+        while (m) {
+          const int bit = __ffs(m) - 1;
+          m &= m - 1;
+          if (record_hits_pixel(s, g * 32 + bit, px, py, ray.quad)) mine |= 1u << bit;
+        }
+      }
+      while (mine) {
+        const int j = g * 32 + __ffs(mine) - 1;
+        mine &= mine - 1;
         const float4 slo = s.slab_lo[j], shi = s.slab_hi[j];
         const float2 ab = staged_ray_box(slo, shi, ray);
         const float a = ab.x, b = ab.y;
@@ -150,9 +161,12 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
           Nz = Nz + pt_w * rl * nz;
         }
         T *= (1.f - alpha);
-        done |= (T < kEarlyStopT);
         last_contrib = (uint32_t)(base + j + 1);
         if (MAXW) atomicMax(reinterpret_cast<int*>(out.max_w) + vid, __float_as_int(pt_w));
+        if (T < kEarlyStopT) {
+          done = true;
+          mine = 0u;
+        }
       }
     }
   }

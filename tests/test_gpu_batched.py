@@ -457,6 +457,26 @@ def test_backward_staging_depth_does_not_change_results(c1, tile, stage, bstage)
         assert rel_err(a, b) < 1e-5, name
 
 
+@pytest.mark.parametrize("ppt,bppt", [(1, 2), (2, 1)])
+def test_backward_pixels_per_thread_apart(c1, ppt, bppt):
+    """The backward's own pixels per thread: the same images and the same
+    gradients up to the order of additions."""
+    g = torch.Generator(device="cuda").manual_seed(23)
+    r0, _ = _raster(c1, tile_size=8)
+    r0.set_staging(32)
+    wC = torch.randn(3 * r0.n_pixels, device="cuda", generator=g)
+    wT = torch.randn(r0.n_pixels, device="cuda", generator=g)
+    base = _render_and_grads(r0, c1, wC, wT)
+    r, _ = _raster(c1, tile_size=8)
+    r.set_staging(32)
+    r.set_pixels_per_thread(ppt)
+    r.set_backward_pixels_per_thread(bppt)
+    got = _render_and_grads(r, c1, wC, wT)
+    assert torch.equal(got[0], base[0]) and torch.equal(got[1], base[1])
+    for a, b, name in zip(got[2:6], base[2:6], ("dL_dgeos", "subdiv", "dL_dsh0", "dL_dshs")):
+        assert rel_err(a, b) < 1e-5, name
+
+
 def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
     from sv_raster_b200.autotune import tune_batched
     monkeypatch.setenv("SVR_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
