@@ -487,8 +487,8 @@ def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
     base = _render_and_grads(r0, c1, wC, wT)
     r, _ = _raster(c1)
     res = tune_batched(r, c1.geos, c1.sh0, c1.shs, 3, reps=2, warmup=1)
-    assert not res["cached"] and set(res["choice"]) == {"tile", "ppt", "bstage", "fstage", "bin", "sort", "fwd",
-                                                        "bwd", "reduce"}
+    assert not res["cached"] and set(res["choice"]) == {"tile", "ppt", "bppt", "bstage", "fstage", "bin", "sort",
+                                                        "fwd", "bwd", "reduce"}
     got = _render_and_grads(r, c1, wC, wT)
     assert torch.equal(got[0], base[0])
     assert rel_err(got[2], base[2]) < 1e-5
