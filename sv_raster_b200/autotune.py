@@ -35,6 +35,11 @@ gradients agree up to the order of floating-point additions):
   with the backward: the forward walks each pixel's own records, which two
   pixels per thread cannot, while the backward's warp reduction favours two
   (``set_backward_pixels_per_thread``).
+* ``bform`` -- how the backward walks a tile (``set_backward_form``): 0
+  every warp visits each record touching its pixels together, 1 each lane
+  walks its own pixel's records and the records' gradient rows are summed
+  afterwards; timed with the backward (form 1 serves 8x8 tiles with one
+  pixel per thread).
 * ``tile`` -- compositing tile size of the batched path (8, 16 or 32 pixels)
   with the voxel-staging depth (records staged into shared memory per round)
   (``BatchedRasterizer.set_tile_size``; the tile size changes the binning, so
@@ -60,6 +65,7 @@ DEFAULT_SPACE = {
     "reduce": [1, 2, 4, 8],
     "ppt": [1, 2],
     "bppt": [0, 1, 2],
+    "bform": [0, 1],
     "bstage": [0, 32, 64, 128, 256],
     "fstage": [0, 32, 64, 128, 256, 512],
 }
@@ -91,7 +97,7 @@ def _store_cache(path, data):
 
 # Bumped whenever the search space or the kernels behind it change, so that
 # choices cached by an older build are measured again rather than reused.
-CACHE_SCHEMA = 7
+CACHE_SCHEMA = 8
 
 
 def cache_key(raster, geos, sh0):
@@ -135,6 +141,8 @@ def apply(raster, choice):
         raster.set_pixels_per_thread(int(choice["ppt"]))
     if "bppt" in choice:
         raster.set_backward_pixels_per_thread(int(choice["bppt"]) or None)
+    if "bform" in choice:
+        raster.set_backward_form(int(choice["bform"]))
     if int(choice.get("fstage", 0)):
         raster.set_staging(int(choice["fstage"]))  # (resets the backward's; set again below)
     if "bstage" in choice:
@@ -194,7 +202,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
         dC, dT = upstream()
         state["grads"] = raster.backward(geos, state["out"][1], dC, dT, sh_degree, M, state.get("grads"))
 
-    stages = [("tile", step), ("ppt", render), ("bppt", backward), ("bstage", backward), ("fstage", render), ("bin", prepare),
+    stages = [("tile", step), ("ppt", render), ("bppt", backward), ("bform", backward), ("bstage", backward), ("fstage", render), ("bin", prepare),
               ("sort", prepare), ("fwd", render), ("bwd", backward), ("reduce", backward)]
     for name, fn in stages:
         cands = space.get(name)
@@ -208,7 +216,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
                 continue
             if name == "tile":
                 raster.fit_capacity(sh0, shs, sh_degree)
-            if name in ("ppt", "bppt", "fwd", "bwd", "reduce", "bstage", "fstage"):
+            if name in ("ppt", "bppt", "bform", "fwd", "bwd", "reduce", "bstage", "fstage"):
                 raster.prepare(sh0, shs, sh_degree)
                 render()
             t = timer(fn, reps, warmup)
