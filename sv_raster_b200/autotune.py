@@ -38,8 +38,9 @@ gradients agree up to the order of floating-point additions):
 * ``bform`` -- how the backward walks a tile (``set_backward_form``): 0
   every warp visits each record touching its pixels together, 1 each lane
   walks its own pixel's records and the records' gradient rows are summed
-  afterwards; timed with the backward (form 1 serves 8x8 tiles with one
-  pixel per thread).
+  afterwards; timed with the backward against the ``bppt`` choice (form 1
+  serves 8x8 tiles with one pixel per thread, so choosing it sets the
+  backward's pixels per thread to 1).
 * ``tile`` -- compositing tile size of the batched path (8, 16 or 32 pixels)
   with the voxel-staging depth (records staged into shared memory per round)
   (``BatchedRasterizer.set_tile_size``; the tile size changes the binning, so
@@ -143,6 +144,8 @@ def apply(raster, choice):
         raster.set_backward_pixels_per_thread(int(choice["bppt"]) or None)
     if "bform" in choice:
         raster.set_backward_form(int(choice["bform"]))
+        if int(choice["bform"]) == 1:
+            raster.set_backward_pixels_per_thread(1)  # the lane form walks one pixel per thread
     if int(choice.get("fstage", 0)):
         raster.set_staging(int(choice["fstage"]))  # (resets the backward's; set again below)
     if "bstage" in choice:
@@ -227,6 +230,8 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
             choice[name] = raster.staging  # "as the tile's" made concrete: later stages may change it
         if name == "bppt" and not choice[name]:
             choice[name] = choice["ppt"]
+        if name == "bform" and choice[name] == 1:
+            choice["bppt"] = 1
         apply(raster, choice)
         if name == "tile":
             raster.fit_capacity(sh0, shs, sh_degree)

@@ -103,8 +103,8 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
     assert res["choice"]["reduce"] == 4 and r.atomic_lanes == 4
     assert res["choice"]["bin"] == 0 and r.binning == 0
     assert res["choice"]["ppt"] == 2 and r.pixels_per_thread == 2
-    assert res["choice"]["bppt"] == 1 and r.pixels_per_thread_bwd == 1  # the backward's own
     assert res["choice"]["bform"] == 1 and r.backward_form == 1
+    assert res["choice"]["bppt"] == 1 and r.pixels_per_thread_bwd == 1  # the lane form's one pixel per thread
     assert res["choice"]["bstage"] == 32 and r.staging_bwd == 32
     assert [c for c, _ in res["timings"]["bstage"]] == [0, 32, 64, 128]  # 256 needs 16x16 tiles
     # the forward's own depth, re-tuned with the backward's kept
