@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--tile", default=None,
                     help="batched mode: fixed compositing tile 'TS', 'TS,SB' or 'TS,SB,SB_backward' (8,64 | "
                          "16,128|256|512 | 32,256; the backward's staging depth apart); no autotuning")
+    ap.add_argument("--bwd-walk", default=None, choices=["warp", "pair", "lanes"],
+                    help="batched mode with --tile: the backward's walk (warp-synchronous with one or two pixels "
+                         "per thread, or each lane walking its own pixel's records)")
     ap.add_argument("--exact", action="store_true",
                     help="batched mode: the exact compositing arithmetic (bit-identical to the plain path) instead "
                          "of the default fast form")
@@ -184,7 +187,8 @@ def main():
         if args.tile:
             parts = [int(x) for x in args.tile.split(",")]
             tile = (parts[0], parts[1] if len(parts) > 1 else (64 if parts[0] == 8 else 256)) + tuple(parts[2:3])
-        wl = workload.BatchedWorkload(sc, dev, tune=not (args.no_tune or tile), tile=tile, exact=args.exact)
+        wl = workload.BatchedWorkload(sc, dev, tune=not (args.no_tune or tile), tile=tile, exact=args.exact,
+                                      bwd_walk=args.bwd_walk if tile else None)
     n_views = len(sc.cameras)
 
     for _ in range(args.warmup):

@@ -250,7 +250,8 @@ class BatchedWorkload:
     fp32 compositing / gradients, no host sync inside a step (the step is
     also captured as a CUDA graph)."""
 
-    def __init__(self, scene, dev, storage=torch.bfloat16, graph=True, tune=True, tile=None, exact=False):
+    def __init__(self, scene, dev, storage=torch.bfloat16, graph=True, tune=True, tile=None, exact=False,
+                 bwd_walk=None):
         from .batched import BatchedRasterizer
         self.sc = scene
         self.dev = dev
@@ -270,6 +271,13 @@ class BatchedWorkload:
             if len(tile) > 2:
                 self.raster.set_backward_staging(tile[2])
             self.tuned = {"tile": list(tile), "fixed": True}
+        if bwd_walk is not None:
+            # the backward's walk: warp-synchronous with one or two pixels per thread, or the lane form
+            ppt, form = {"warp": (1, 0), "pair": (2, 0), "lanes": (1, 1)}[bwd_walk]
+            self.raster.set_backward_pixels_per_thread(ppt)
+            self.raster.set_backward_form(form)
+            if self.tuned is not None:
+                self.tuned["bwd_walk"] = bwd_walk
         self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)
         if tune:
             self.tuned = tune_raster(self.raster, self.geos, self.sh0, self.shs)
