@@ -56,9 +56,8 @@ def parse():
     ap.add_argument("--tile", default=None,
                     help="batched mode: fixed compositing tile 'TS', 'TS,SB' or 'TS,SB,SB_backward' (8,64 | "
                          "16,128|256|512 | 32,256; the backward's staging depth apart); no autotuning")
-    ap.add_argument("--bwd-walk", default=None, choices=["warp", "pair", "lanes"],
-                    help="batched mode with --tile: the backward's walk (warp-synchronous with one or two pixels "
-                         "per thread, or each lane walking its own pixel's records)")
+    ap.add_argument("--bwd-walk", default=None, choices=["warp", "pair"],
+                    help="batched mode with --tile: the backward with one or two pixels per thread")
     ap.add_argument("--exact", action="store_true",
                     help="batched mode: the exact compositing arithmetic (bit-identical to the plain path) instead "
                          "of the default fast form")

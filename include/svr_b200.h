@@ -333,16 +333,6 @@ int svr_batch_plan_set_pixels_per_thread(svr_batch_plan* plan, int pixels);
  * pixel's own records with one pixel per thread, while the backward's warp
  * reduction favours two, so the best choices can differ. */
 int svr_batch_plan_set_backward_pixels_per_thread(svr_batch_plan* plan, int pixels);
-/* How svr_batch_backward walks a tile's records.  form = 0 (default): each
- * warp visits every staged record touching its 8x4 pixels with all 32 lanes
- * and reduces the record's gradients across the warp.  form = 1: each lane
- * walks only its own pixel's records, writing each (record, pixel) pair's
- * gradients into a row of shared memory, and lanes then add the rows of
- * each record column by column -- fewer warp iterations where most records
- * reach a few pixels.  The form applies to 8x8 tiles staging 32 or 64
- * records with one pixel per thread; other configurations use form 0.
- * Gradients agree up to the order of additions. */
-int svr_batch_plan_set_backward_form(svr_batch_plan* plan, int form);
 int64_t svr_batch_plan_pixels(const svr_batch_plan* plan);
 int64_t svr_batch_plan_tiles(const svr_batch_plan* plan);
 int svr_batch_plan_groups(const svr_batch_plan* plan);

@@ -98,7 +98,6 @@ _SIGS = {
     "svr_batch_plan_set_backward_staging": (c_int, [c_p, c_int]),
     "svr_batch_plan_set_pixels_per_thread": (c_int, [c_p, c_int]),
     "svr_batch_plan_set_backward_pixels_per_thread": (c_int, [c_p, c_int]),
-    "svr_batch_plan_set_backward_form": (c_int, [c_p, c_int]),
     "svr_batch_plan_set_binning": (c_int, [c_p, c_int]),
     "svr_batch_plan_pixels": (c_i64, [c_p]),
     "svr_batch_plan_tiles": (c_i64, [c_p]),

@@ -35,12 +35,6 @@ gradients agree up to the order of floating-point additions):
   with the backward: the forward walks each pixel's own records, which two
   pixels per thread cannot, while the backward's warp reduction favours two
   (``set_backward_pixels_per_thread``).
-* ``bform`` -- how the backward walks a tile (``set_backward_form``): 0
-  every warp visits each record touching its pixels together, 1 each lane
-  walks its own pixel's records and the records' gradient rows are summed
-  afterwards; timed with the backward against the ``bppt`` choice (form 1
-  serves 8x8 tiles with one pixel per thread, so choosing it sets the
-  backward's pixels per thread to 1).
 * ``tile`` -- compositing tile size of the batched path (8, 16 or 32 pixels)
   with the voxel-staging depth (records staged into shared memory per round)
   (``BatchedRasterizer.set_tile_size``; the tile size changes the binning, so
@@ -66,7 +60,6 @@ DEFAULT_SPACE = {
     "reduce": [1, 2, 4, 8],
     "ppt": [1, 2],
     "bppt": [0, 1, 2],
-    "bform": [0, 1],
     "bstage": [0, 32, 64, 128, 256],
     "fstage": [0, 32, 64, 128, 256, 512],
 }
@@ -98,7 +91,7 @@ def _store_cache(path, data):
 
 # Bumped whenever the search space or the kernels behind it change, so that
 # choices cached by an older build are measured again rather than reused.
-CACHE_SCHEMA = 8
+CACHE_SCHEMA = 7
 
 
 def cache_key(raster, geos, sh0):
@@ -142,10 +135,6 @@ def apply(raster, choice):
         raster.set_pixels_per_thread(int(choice["ppt"]))
     if "bppt" in choice:
         raster.set_backward_pixels_per_thread(int(choice["bppt"]) or None)
-    if "bform" in choice:
-        raster.set_backward_form(int(choice["bform"]))
-        if int(choice["bform"]) == 1:
-            raster.set_backward_pixels_per_thread(1)  # the lane form walks one pixel per thread
     if int(choice.get("fstage", 0)):
         raster.set_staging(int(choice["fstage"]))  # (resets the backward's; set again below)
     if "bstage" in choice:
@@ -205,7 +194,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
         dC, dT = upstream()
         state["grads"] = raster.backward(geos, state["out"][1], dC, dT, sh_degree, M, state.get("grads"))
 
-    stages = [("tile", step), ("ppt", render), ("bppt", backward), ("bform", backward), ("bstage", backward), ("fstage", render), ("bin", prepare),
+    stages = [("tile", step), ("ppt", render), ("bppt", backward), ("bstage", backward), ("fstage", render), ("bin", prepare),
               ("sort", prepare), ("fwd", render), ("bwd", backward), ("reduce", backward)]
     for name, fn in stages:
         cands = space.get(name)
@@ -219,7 +208,7 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
                 continue
             if name == "tile":
                 raster.fit_capacity(sh0, shs, sh_degree)
-            if name in ("ppt", "bppt", "bform", "fwd", "bwd", "reduce", "bstage", "fstage"):
+            if name in ("ppt", "bppt", "fwd", "bwd", "reduce", "bstage", "fstage"):
                 raster.prepare(sh0, shs, sh_degree)
                 render()
             t = timer(fn, reps, warmup)
@@ -230,8 +219,6 @@ def tune_batched(raster, geos, sh0, shs, sh_degree=3, space=None, reps=5, warmup
             choice[name] = raster.staging  # "as the tile's" made concrete: later stages may change it
         if name == "bppt" and not choice[name]:
             choice[name] = choice["ppt"]
-        if name == "bform" and choice[name] == 1:
-            choice["bppt"] = 1
         apply(raster, choice)
         if name == "tile":
             raster.fit_capacity(sh0, shs, sh_degree)

@@ -60,7 +60,6 @@ class BatchedRasterizer:
         self.exact = bool(exact)
         self.pixels_per_thread = 1
         self.pixels_per_thread_bwd = None  # None: as pixels_per_thread
-        self.backward_form = 0
         self.culling = -1  # -1: tight bbox with the fast arithmetic, the rounded one with the exact
         self.staging_bwd = None  # None: the forward's staging depth
         self._make_plan(0 if capacity is None else int(capacity))
@@ -93,7 +92,6 @@ class BatchedRasterizer:
               "batch_plan_set_pixels_per_thread")
         check(L.svr_batch_plan_set_backward_pixels_per_thread(plan, self.pixels_per_thread_bwd or 0),
               "batch_plan_set_backward_pixels_per_thread")
-        check(L.svr_batch_plan_set_backward_form(plan, self.backward_form), "batch_plan_set_backward_form")
         if self.staging_bwd is not None:
             check(L.svr_batch_plan_set_backward_staging(plan, self.staging_bwd), "batch_plan_set_backward_staging")
 
@@ -135,14 +133,6 @@ class BatchedRasterizer:
         beyond the order of gradient additions."""
         check(lib().svr_batch_plan_set_pixels_per_thread(self.plan, int(pixels)), "batch_plan_set_pixels_per_thread")
         self.pixels_per_thread = int(pixels)
-
-    def set_backward_form(self, form=0):
-        """How the backward walks a tile: 0 every warp visits each record
-        touching its pixels together, 1 each lane walks its own pixel's
-        records (8x8 tiles staging 32 or 64 records, one pixel per thread;
-        see svr_batch_plan_set_backward_form)."""
-        check(lib().svr_batch_plan_set_backward_form(self.plan, int(form)), "batch_plan_set_backward_form")
-        self.backward_form = int(form)
 
     def set_backward_pixels_per_thread(self, pixels=None):
         """Pixels per thread of the backward alone, 1 or 2 (None: as

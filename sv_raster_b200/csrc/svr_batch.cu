@@ -389,7 +389,6 @@ struct svr_batch_plan {
   int exact;                   // compositing arithmetic (svr_batch_plan_set_arithmetic): 1 exact, 0 fast
   int pair;                    // two pixels per compositing thread (svr_batch_plan_set_pixels_per_thread)
   int pair_bwd;                // the backward's, when set apart (-1: as pair)
-  int bwd_form;                // backward walk (svr_batch_plan_set_backward_form): 0 warp, 1 lanes
   int culling;                 // pixel bbox (svr_batch_plan_set_culling): -1 follows exact, 0 rounded, 1 tight
   int binning;                 // 1: counting sort by tile, 0: radix over the tile bits (svr_batch_plan_set_binning)
   // workspace layout (byte offsets)
@@ -600,7 +599,6 @@ int svr_batch_plan_create(int n_views, const svr_camera* cams, int64_t P, int64_
   p->exact = 0;
   p->pair = 0;
   p->pair_bwd = -1;
-  p->bwd_form = 0;
   p->culling = -1;
   p->binning = 1;
   ensure_segsort_attributes();
@@ -647,12 +645,6 @@ int svr_batch_plan_tile_size(const svr_batch_plan* p) { return p ? p->tile_size 
 int svr_batch_plan_set_pixels_per_thread(svr_batch_plan* p, int pixels) {
   if (!p || (pixels != 1 && pixels != 2)) return SVR_ERR_SHAPE;
   p->pair = pixels == 2;
-  return SVR_OK;
-}
-
-int svr_batch_plan_set_backward_form(svr_batch_plan* p, int form) {
-  if (!p || (form != 0 && form != 1)) return SVR_ERR_SHAPE;
-  p->bwd_form = form;
   return SVR_OK;
 }
 
@@ -855,7 +847,7 @@ int svr_batch_backward(svr_batch_plan* p, void* ws, const float* vox_centers, co
   if (ordered) build_tile_order(p, q, q.tile_last, q.order_bwd, stream);
   launch_render_bwd_batch(p->vt, (int)p->total_tiles, q.ranges, q.tile_last, p->cap > 0 ? q.vb : nullptr, va,
                           (int)p->P, (size_t)p->P * 3, (size_t)p->P * 4, in, out, p->n_samp, p->tile_size,
-                          p->stage_bwd, !p->exact, p->pair_bwd < 0 ? p->pair : p->pair_bwd, p->bwd_form,
+                          p->stage_bwd, !p->exact, p->pair_bwd < 0 ? p->pair : p->pair_bwd,
                           ordered ? q.order_bwd : nullptr, q.header + 3,
                           p->bwd_ctas_per_sm, stream);
   return check_last();

@@ -74,8 +74,6 @@ void launch_render_fwd(const ViewParams& vp, const uint2* ranges, const uint32_t
 // (identity when null); ctas_per_sm caps the resident CTAs per SM (0 = as
 // many as fit).  (tile, stage) must satisfy batch_tile_supported.
 bool batch_pair_supported(int tile, int stage);
-// Backward configurations with a lane form (svr_render_bwd_lanes.cuh).
-inline bool batch_lanes_supported(int tile, int stage) { return tile == 8 && (stage == 32 || stage == 64); }
 bool batch_tile_supported(int tile, int stage);
 void ensure_fwd_batch_attributes();
 void ensure_bwd_batch_attributes();
@@ -89,7 +87,7 @@ void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t
 void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
                              size_t rgb_view_stride, size_t drgb_view_stride, const BwdTileIn& in,
-                             const BwdTileOut& out, int ns, int tile, int stage, bool fast, int pair, int form,
+                             const BwdTileOut& out, int ns, int tile, int stage, bool fast, int pair,
                              const uint32_t* order, uint32_t* counter, int ctas_per_sm, cudaStream_t stream);
 // svr_binning_deep.cu: binning of 21-level octrees (63-bit ranks).  The
 // sort pairs (keys_a, vals_a) / (keys_b, vals_b) and sort_temp are those of

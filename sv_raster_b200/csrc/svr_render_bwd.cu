@@ -5,7 +5,6 @@
 
 #include "svr_kernels.h"
 #include "svr_render_bwd.cuh"
-#include "svr_render_bwd_lanes.cuh"
 #include "svr_render_pair.cuh"
 
 namespace svr {
@@ -132,60 +131,6 @@ render_bwd_batch_pair_kernel(const __grid_constant__ BwdBatchArgs a) {
   }
 }
 
-// The same persistent form with each lane walking its own pixel's records
-// (svr_render_bwd_lanes.cuh).
-template <class CFG>
-struct BwdLaneKernelSmem {
-  StageSmem<CFG::SB> s;
-  LaneBwdSmem<CFG> L;
-  float c2w[12];
-  uint32_t item;
-};
-
-// Resident CTAs per SM that the lane form's shared memory allows (1 KB of
-// each CTA's share is reserved), at most 16: its launch bound, so that the
-// register budget follows the occupancy the shared memory permits.
-template <class CFG>
-constexpr int lane_min_blocks() {
-  constexpr int per = (int)sizeof(BwdLaneKernelSmem<CFG>) + 1024;
-  constexpr int n = (228 * 1024) / per;
-  return n > 16 ? 16 : (n < 1 ? 1 : n);
-}
-
-template <class CFG, int NS, bool FAST>
-__global__ void __launch_bounds__(CFG::NT, lane_min_blocks<CFG>())
-render_bwd_batch_lanes_kernel(const __grid_constant__ BwdBatchArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  BwdLaneKernelSmem<CFG>& sm = *reinterpret_cast<BwdLaneKernelSmem<CFG>*>(smem_raw);
-  for (;;) {
-    if (threadIdx.x == 0) sm.item = atomicAdd(a.counter, 1u);
-    __syncthreads();
-    const uint32_t k = sm.item;
-    if (k >= (uint32_t)a.n_items) break;
-    const int item = a.order ? (int)a.order[k] : (int)k;
-    const int view = view_of_tile(a.views, item);
-    const ViewParams& vp = a.views.v[view];
-    if (threadIdx.x < 12) sm.c2w[threadIdx.x] = vp.c2w[threadIdx.x];
-    __syncthreads();
-    const int local = item - (int)vp.tile_base;
-    const int tile_x = local % vp.grid_x, tile_y = local / vp.grid_x;
-    VoxelArrays va = a.va;
-    va.bboxes = a.va.bboxes + (size_t)view * a.P;
-    va.rgbs = a.va.rgbs + (size_t)view * a.rgb_view_stride;
-    BwdTileIn in = a.in;
-    const size_t pb = vp.pix_base;
-    in.T = a.in.T + pb;
-    in.n_contrib = a.in.n_contrib + pb;
-    in.dL_dcolor = a.in.dL_dcolor + 3 * pb;
-    in.dL_dT = a.in.dL_dT + pb;
-    BwdTileOut o = a.out;
-    o.dL_drgbs = a.out.dL_drgbs + (size_t)view * a.drgb_view_stride;
-    render_tile_bwd_lanes<CFG, NS, FAST, true>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.tile_last[item], a.vals,
-                                               va, in, o, sm.s, sm.L);
-    __syncthreads();
-  }
-}
-
 static_assert(sizeof(BwdSmem<PlainTile>) <= 48 * 1024, "plain backward staging must fit the default limit");
 
 #define SVR_BWD_CASE(KERNEL, NS_, D_, T_, N_)                                                     \
@@ -220,17 +165,6 @@ static void set_bwd_pair_attrs() {
   cudaFuncSetAttribute(render_bwd_batch_pair_kernel<CFG, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
-template <class CFG>
-static void set_bwd_lane_attrs() {
-  const int smem = (int)sizeof(BwdLaneKernelSmem<CFG>);
-  cudaFuncSetAttribute(render_bwd_batch_lanes_kernel<CFG, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(render_bwd_batch_lanes_kernel<CFG, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(render_bwd_batch_lanes_kernel<CFG, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(render_bwd_batch_lanes_kernel<CFG, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(render_bwd_batch_lanes_kernel<CFG, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(render_bwd_batch_lanes_kernel<CFG, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-}
-
 template <class CFG, int NS>
 static void set_bwd_batch_attr() {
   cudaFuncSetAttribute(render_bwd_batch_kernel<CFG, NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -262,8 +196,6 @@ void ensure_bwd_batch_attributes() {
     set_bwd_pair_attrs<PairCfg<8, 64>>();
     set_bwd_pair_attrs<PairCfg<16, 128>>();
     set_bwd_pair_attrs<PairCfg<16, 256>>();
-    set_bwd_lane_attrs<TileCfg<8, 32>>();
-    set_bwd_lane_attrs<TileCfg<8, 64>>();
   });
 }
 
@@ -297,24 +229,6 @@ static void launch_bwd_pair_cfg(const BwdBatchArgs& args, int ns, bool fast, int
   else launch_bwd_pair_arith<CFG, false>(args, ns, ctas_per_sm, stream);
 }
 
-template <class CFG, bool FAST>
-static void launch_bwd_lanes_arith(const BwdBatchArgs& args, int ns, int ctas_per_sm, cudaStream_t stream) {
-  const size_t smem = sizeof(BwdLaneKernelSmem<CFG>);
-  auto go = [&](auto kfn) {
-    const int grid = persistent_grid((const void*)kfn, CFG::NT, smem, args.n_items, ctas_per_sm);
-    kfn<<<grid, CFG::NT, smem, stream>>>(args);
-  };
-  if (ns == 1) go(render_bwd_batch_lanes_kernel<CFG, 1, FAST>);
-  else if (ns == 2) go(render_bwd_batch_lanes_kernel<CFG, 2, FAST>);
-  else go(render_bwd_batch_lanes_kernel<CFG, 3, FAST>);
-}
-
-template <class CFG>
-static void launch_bwd_lanes_cfg(const BwdBatchArgs& args, int ns, bool fast, int ctas_per_sm, cudaStream_t stream) {
-  if (fast) launch_bwd_lanes_arith<CFG, true>(args, ns, ctas_per_sm, stream);
-  else launch_bwd_lanes_arith<CFG, false>(args, ns, ctas_per_sm, stream);
-}
-
 template <class CFG>
 static void launch_bwd_batch_cfg(const BwdBatchArgs& args, int ns, bool fast, int ctas_per_sm, cudaStream_t stream) {
   if (fast) launch_bwd_batch_arith<CFG, true>(args, ns, ctas_per_sm, stream);
@@ -324,18 +238,13 @@ static void launch_bwd_batch_cfg(const BwdBatchArgs& args, int ns, bool fast, in
 void launch_render_bwd_batch(const ViewTable& views, int n_items, const uint2* ranges,
                              const uint32_t* tile_last, const uint32_t* vals, const VoxelArrays& va, int P,
                              size_t rgb_view_stride, size_t drgb_view_stride, const BwdTileIn& in,
-                             const BwdTileOut& out, int ns, int tile, int stage, bool fast, int pair, int form,
+                             const BwdTileOut& out, int ns, int tile, int stage, bool fast, int pair,
                              const uint32_t* order, uint32_t* counter, int ctas_per_sm, cudaStream_t stream) {
   if (n_items <= 0) return;
   ensure_bwd_batch_attributes();
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
   const BwdBatchArgs args{views, n_items, ranges, tile_last, vals, va, P, rgb_view_stride, drgb_view_stride, in, out,
                           order, counter};
-  if (form == 1 && !pair && batch_lanes_supported(tile, stage)) {
-    if (stage == 32) launch_bwd_lanes_cfg<TileCfg<8, 32>>(args, ns, fast, ctas_per_sm, stream);
-    else launch_bwd_lanes_cfg<TileCfg<8, 64>>(args, ns, fast, ctas_per_sm, stream);
-    return;
-  }
   if (pair && batch_pair_supported(tile, stage)) {
     if (tile == 8 && stage == 32) launch_bwd_pair_cfg<PairCfg<8, 32>>(args, ns, fast, ctas_per_sm, stream);
     else if (tile == 8) launch_bwd_pair_cfg<PairCfg<8, 64>>(args, ns, fast, ctas_per_sm, stream);

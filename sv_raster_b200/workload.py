@@ -272,10 +272,8 @@ class BatchedWorkload:
                 self.raster.set_backward_staging(tile[2])
             self.tuned = {"tile": list(tile), "fixed": True}
         if bwd_walk is not None:
-            # the backward's walk: warp-synchronous with one or two pixels per thread, or the lane form
-            ppt, form = {"warp": (1, 0), "pair": (2, 0), "lanes": (1, 1)}[bwd_walk]
-            self.raster.set_backward_pixels_per_thread(ppt)
-            self.raster.set_backward_form(form)
+            # the backward's pixels per thread: one ("warp") or two ("pair")
+            self.raster.set_backward_pixels_per_thread({"warp": 1, "pair": 2}[bwd_walk])
             if self.tuned is not None:
                 self.tuned["bwd_walk"] = bwd_walk
         self.total = self.raster.fit_capacity(self.sh0, self.shs, 3)

@@ -42,9 +42,6 @@ class FakeRaster:
     def set_backward_pixels_per_thread(self, n=None):
         self.pixels_per_thread_bwd = n
 
-    def set_backward_form(self, f=0):
-        self.backward_form = f
-
     def set_backward_staging(self, n=None):
         if n is not None and n not in ((32, 64, 128) if self.tile_size == 8 else (128, 256, 512)):
             raise RuntimeError("staging depth not supported by this tile size")
@@ -85,7 +82,6 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
         t -= 0.03125 * (getattr(r, "staging_bwd", None) == 32)
         t -= 0.015625 * (r.staging == 128 and getattr(r, "staging_bwd", None) == 32)
         t -= 0.0078125 * (getattr(r, "pixels_per_thread_bwd", None) == 1)
-        t -= 0.00390625 * (getattr(r, "backward_form", 0) == 1)
         return t
 
     geos = torch.zeros(r.P, 8)
@@ -103,14 +99,12 @@ def test_tuner_picks_fastest_per_stage_and_caches(tmp_path, monkeypatch):
     assert res["choice"]["reduce"] == 4 and r.atomic_lanes == 4
     assert res["choice"]["bin"] == 0 and r.binning == 0
     assert res["choice"]["ppt"] == 2 and r.pixels_per_thread == 2
-    assert res["choice"]["bform"] == 1 and r.backward_form == 1
-    assert res["choice"]["bppt"] == 1 and r.pixels_per_thread_bwd == 1  # the lane form's one pixel per thread
+    assert res["choice"]["bppt"] == 1 and r.pixels_per_thread_bwd == 1  # the backward's own
     assert res["choice"]["bstage"] == 32 and r.staging_bwd == 32
     assert [c for c, _ in res["timings"]["bstage"]] == [0, 32, 64, 128]  # 256 needs 16x16 tiles
     # the forward's own depth, re-tuned with the backward's kept
     assert res["choice"]["fstage"] == 128 and r.staging == 128 and r.staging_bwd == 32
-    assert set(res["timings"]) == {"tile", "ppt", "bppt", "bform", "bstage", "fstage", "bin", "sort", "fwd", "bwd",
-                                   "reduce"}
+    assert set(res["timings"]) == {"tile", "ppt", "bppt", "bstage", "fstage", "bin", "sort", "fwd", "bwd", "reduce"}
     # second call: served from the cache, applied, no timing
     r2 = FakeRaster()
     res2 = autotune.tune_batched(r2, geos, sh0, shs, 3, timer=lambda *a: 1 / 0)

@@ -477,41 +477,6 @@ def test_backward_pixels_per_thread_apart(c1, ppt, bppt):
         assert rel_err(a, b) < 1e-5, name
 
 
-@pytest.mark.parametrize("views,stage,exact", [((0, 1, 2), 32, False), ((0, 1, 2), 64, False), ((0, 1, 2), 32, True),
-                                               ("c3", 32, False), ("c3", 64, True)])
-def test_backward_lane_form_matches_warp_form(c1, views, stage, exact):
-    """The backward with each lane walking its own pixel's records (rows of
-    (record, pixel) gradients summed per record afterwards, in sub-groups
-    when a group's pairs exceed the row buffer) against the warp form: the
-    same gradients up to the order of additions."""
-    if views == "c3":
-        C = SceneTensors(synthetic.cached_config_scene("c3"))
-        cams = [DevCam(C.scene.cameras[i]) for i in (0, 5)]
-    else:
-        C = c1
-        cams = [DevCam(C.scene.cameras[i]) for i in views]
-    g = torch.Generator(device="cuda").manual_seed(29)
-    out = {}
-    for form in (0, 1):
-        r = BatchedRasterizer(cams, C.octpath, C.centers, C.lengths, max_level=C.scene.max_level, tile_size=8,
-                              exact=exact)
-        r.set_staging(stage)
-        r.set_backward_form(form)
-        if "wC" not in out:
-            out["wC"] = torch.randn(3 * r.n_pixels, device="cuda", generator=g)
-            out["wT"] = torch.randn(r.n_pixels, device="cuda", generator=g)
-        out[form] = _render_and_grads(r, C, out["wC"], out["wT"])
-        del r
-    warp, lanes = out[0], out[1]
-    assert torch.equal(lanes[0], warp[0]) and torch.equal(lanes[1], warp[1])
-    errs = {name: rel_err(a, b) for a, b, name in zip(lanes[2:6], warp[2:6],
-                                                       ("dL_dgeos", "subdiv", "dL_dsh0", "dL_dshs"))}
-    print(f"lane form ({views}, stage {stage}, {'exact' if exact else 'fast'}): "
-          + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
-    for k, v in errs.items():
-        assert v < 1e-5, k
-
-
 def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
     from sv_raster_b200.autotune import tune_batched
     monkeypatch.setenv("SVR_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
@@ -522,8 +487,8 @@ def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
     base = _render_and_grads(r0, c1, wC, wT)
     r, _ = _raster(c1)
     res = tune_batched(r, c1.geos, c1.sh0, c1.shs, 3, reps=2, warmup=1)
-    assert not res["cached"] and set(res["choice"]) == {"tile", "ppt", "bppt", "bform", "bstage", "fstage", "bin",
-                                                        "sort", "fwd", "bwd", "reduce"}
+    assert not res["cached"] and set(res["choice"]) == {"tile", "ppt", "bppt", "bstage", "fstage", "bin", "sort",
+                                                        "fwd", "bwd", "reduce"}
     got = _render_and_grads(r, c1, wC, wT)
     assert torch.equal(got[0], base[0])
     assert rel_err(got[2], base[2]) < 1e-5
