@@ -269,165 +269,179 @@ __device__ __forceinline__ bool bwd_pixel_record(const StageSmem<SB>& s, int j, 
   (void)dL_dD; (void)dNx; (void)dNy; (void)dNz; (void)weight_dist;
   (void)prefix_wm; (void)suffix_wm; (void)prefix_w; (void)suffix_w;
   bool contrib = false;
-const float4 slo = s.slab_lo[j], shi = s.slab_hi[j];
-const float2 ab = staged_ray_box(slo, shi, ray);
-const float a = ab.x, b = ab.y;
-if (!(a > b)) {
-  float geo[8];
-  load_geo(s, j, geo);
-  float dgeo[8];
+  // Fast arithmetic, one sample, no depth terms: keep the trilinear weights
+  // and scale them once by dL/dI * d(density)/d(sample) (8 multiplies fewer
+  // than forming dI/dgeo first; a different rounding order).
+  constexpr bool kFoldScale = FAST && NS == 1 && !DEPTH;
+  const float4 slo = s.slab_lo[j], shi = s.slab_hi[j];
+  const float2 ab = staged_ray_box(slo, shi, ray);
+  const float a = ab.x, b = ab.y;
+  if (!(a > b)) {
+    float geo[8];
+    load_geo(s, j, geo);
+    float dgeo[8];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) dgeo[c] = 0.f;
-  float vol_int = 0.f;
-  float dI_dgeo[8];
+    for (int c = 0; c < 8; ++c) dgeo[c] = 0.f;
+    float vol_int = 0.f;
+    float dI_dgeo[8];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) dI_dgeo[c] = 0.f;
-  float each_dI[NS][8];
-  float w[8];
-  float local_alpha[NS];
-  const float vox_l_inv = slo.w;
-  const float4 cr = s.corner[j];
-  const float step_sz = (b - a) * (1.f / NS);
-  const float stx = step_sz * ray.dx, sty = step_sz * ray.dy, stz = step_sz * ray.dz;
-  const float t0 = a + 0.5f * step_sz;
-  const float ptx = ray.ox + t0 * ray.dx, pty = ray.oy + t0 * ray.dy, ptz = ray.oz + t0 * ray.dz;
-  float qx = (ptx - cr.x) * vox_l_inv;
-  float qy = (pty - cr.y) * vox_l_inv;
-  float qz = (ptz - cr.z) * vox_l_inv;
-  const float qsx = stx * vox_l_inv, qsy = sty * vox_l_inv, qsz = stz * vox_l_inv;
+    for (int c = 0; c < 8; ++c) dI_dgeo[c] = 0.f;
+    float each_dI[NS][8];
+    float w[8];
+    float local_alpha[NS];
+    const float vox_l_inv = slo.w;
+    const float4 cr = s.corner[j];
+    const float step_sz = (b - a) * (1.f / NS);
+    const float stx = step_sz * ray.dx, sty = step_sz * ray.dy, stz = step_sz * ray.dz;
+    const float t0 = a + 0.5f * step_sz;
+    const float ptx = ray.ox + t0 * ray.dx, pty = ray.oy + t0 * ray.dy, ptz = ray.oz + t0 * ray.dz;
+    float qx = (ptx - cr.x) * vox_l_inv;
+    float qy = (pty - cr.y) * vox_l_inv;
+    float qz = (ptz - cr.z) * vox_l_inv;
+    const float qsx = stx * vox_l_inv, qsy = sty * vox_l_inv, qsz = stz * vox_l_inv;
 #pragma unroll
-  for (int k = 0; k < NS; ++k) {
-    trilinear_weights(qx, qy, qz, w);
-    float d = 0.f;
+    for (int k = 0; k < NS; ++k) {
+      trilinear_weights(qx, qy, qz, w);
+      float d = 0.f;
 #pragma unroll
-    for (int c = 0; c < 8; ++c) d += geo[c] * w[c];
-    float act, act_grad;
-    density_act_and_grad_f<FAST>(d, act, act_grad);
-    const float lvi = kStepScale * step_sz * act;
-    vol_int += lvi;
-    if (DEPTH && NS > 1) local_alpha[k] = fminf(kMaxAlpha, 1.f - exp_f<FAST>(-lvi));
-    const float dd_dd = kStepScale * step_sz * act_grad;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const float tmp = dd_dd * w[c];
-      dI_dgeo[c] += tmp;
-      if (DEPTH && NS > 1) each_dI[k][c] = tmp;
-    }
-    qx = qx + qsx; qy = qy + qsy; qz = qz + qsz;
-  }
-  const float exp_neg = exp_f<FAST>(-vol_int);
-  const float alpha = fminf(kMaxAlpha, 1.f - exp_neg);
-  if (!(alpha < kMinAlpha)) {
-    contrib = true;
-    T = div_f<FAST>(T, 1.f - alpha);
-    const float pt_w = alpha * T;
-    const float4 rgbv = s.rgb[j];
-    float dL_dpt_w = gx * rgbv.x + gy * rgbv.y + gz * rgbv.z;
-    if (DIST) {
-      const float adist = contract_depth(a), bdist = contract_depth(b);
-      const float now_m = 0.5f * (adist + bdist);
-      const float now_wm = now_m * pt_w;
-      prefix_wm -= now_wm;
-      prefix_w -= pt_w;
-      const float uni = 0.6666666f * pt_w * (bdist - adist);
-      const float bi = 2.f * (now_m * (prefix_w - suffix_w) - (prefix_wm - suffix_wm));
-      dL_dpt_w += weight_dist * (uni + bi);
-      suffix_wm += now_wm;
-      suffix_w += pt_w;
-    }
-    if (NORMAL) {
-      float nx, ny, nz;
-      field_normal(geo, nx, ny, nz);
-      const float rl = safe_rnorm3(nx, ny, nz);
-      const float sx = rl * nx, sy = rl * ny, sz = rl * nz;
-      dL_dpt_w += dNx * sx + dNy * sy + dNz * sz;
-      const float dsx = pt_w * dNx, dsy = pt_w * dNy, dsz = pt_w * dNz;
-      const float dot_ = dsx * nx + dsy * ny + dsz * nz;
-      const float lnx = rl * (dsx - dot_ * rl * sx);
-      const float lny = rl * (dsy - dot_ * rl * sy);
-      const float lnz = rl * (dsz - dot_ * rl * sz);
-      dgeo[0] += -lnx - lny - lnz;
-      dgeo[1] += -lnx - lny + lnz;
-      dgeo[2] += -lnx + lny - lnz;
-      dgeo[3] += -lnx + lny + lnz;
-      dgeo[4] += +lnx - lny - lnz;
-      dgeo[5] += +lnx - lny + lnz;
-      dgeo[6] += +lnx + lny - lnz;
-      dgeo[7] += +lnx + lny + lnz;
-    }
-    const float dL_dalpha = T * (dL_dpt_w - last_dL_dT);
-    last_dL_dT += alpha * (dL_dpt_w - last_dL_dT);
-    const float dL_dI = dL_dalpha * exp_neg;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) dgeo[c] += dL_dI * dI_dgeo[c];
-    if (DEPTH) {
-      float dval;
-      float dI[NS];
-      if (NS == 3) {
-        const float ss = 0.3333333f * (b - a);
-        const float a0 = local_alpha[0], a1 = local_alpha[NS > 1 ? 1 : 0], a2 = local_alpha[NS > 2 ? 2 : 0];
-        const float t0_ = a + 0.5f * ss, t1_ = a + 1.5f * ss, t2_ = a + 2.5f * ss;
-        dval = a0 * t0_ + (1.f - a0) * a1 * t1_ + (1.f - a0) * (1.f - a1) * a2 * t2_;
-        dI[0] = dL_dD * T * (t0_ + a1 * a2 * t2_ - a1 * t1_ - a2 * t2_) * (1.f - a0);
-        dI[NS > 1 ? 1 : 0] = dL_dD * T * (t1_ + a0 * a2 * t2_ - a0 * t1_ - a2 * t2_) * (1.f - a1);
-        dI[NS > 2 ? 2 : 0] = dL_dD * T * (t2_ + a0 * a1 * t2_ - a0 * t2_ - a1 * t2_) * (1.f - a2);
-      } else if (NS == 2) {
-        const float ss = 0.5f * (b - a);
-        const float a0 = local_alpha[0], a1 = local_alpha[NS > 1 ? 1 : 0];
-        const float t0_ = a + 0.5f * ss, t1_ = a + 1.5f * ss;
-        dval = a0 * t0_ + (1.f - a0) * a1 * t1_;
-        dI[0] = dL_dD * T * (t0_ - a1 * t1_) * (1.f - a0);
-        dI[NS > 1 ? 1 : 0] = dL_dD * T * (t1_ - a0 * t1_) * (1.f - a1);
-      } else {
-        const float t0_ = 0.5f * (a + b);
-        dval = alpha * t0_;
-        dI[0] = dL_dD * T * t0_ * (1.f - alpha);
-      }
-      last_dL_dT += dL_dD * dval;
-      if (NS == 3) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          dgeo[c] += dI[0] * each_dI[0][c] + dI[NS > 1 ? 1 : 0] * each_dI[NS > 1 ? 1 : 0][c] +
-                     dI[NS > 2 ? 2 : 0] * each_dI[NS > 2 ? 2 : 0][c];
-      } else if (NS == 2) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          dgeo[c] += dI[0] * each_dI[0][c] + dI[NS > 1 ? 1 : 0] * each_dI[NS > 1 ? 1 : 0][c];
+      for (int c = 0; c < 8; ++c) d += geo[c] * w[c];
+      float act, act_grad;
+      density_act_and_grad_f<FAST>(d, act, act_grad);
+      const float lvi = kStepScale * step_sz * act;
+      vol_int += lvi;
+      if (DEPTH && NS > 1) local_alpha[k] = fminf(kMaxAlpha, 1.f - exp_f<FAST>(-lvi));
+      const float dd_dd = kStepScale * step_sz * act_grad;
+      if (kFoldScale) {
+        dI_dgeo[0] = dd_dd;  // the weights stay in w: dL/dgeo = (dL/dI * dd_dd) * w below
       } else {
 #pragma unroll
-        for (int c = 0; c < 8; ++c) dgeo[c] += dI[0] * dI_dgeo[c];
+        for (int c = 0; c < 8; ++c) {
+          const float tmp = dd_dd * w[c];
+          dI_dgeo[c] += tmp;
+          if (DEPTH && NS > 1) each_dI[k][c] = tmp;
+        }
       }
+      qx = qx + qsx; qy = qy + qsy; qz = qz + qsz;
     }
-    if (in.lambda_ascending > 0) {
-      const float lo_x = cr.x, lo_y = cr.y, lo_z = cr.z;
-      const float pax = ray.ox + a * ray.dx, pay = ray.oy + a * ray.dy, paz = ray.oz + a * ray.dz;
-      const float pbx = ray.ox + b * ray.dx, pby = ray.oy + b * ray.dy, pbz = ray.oz + b * ray.dz;
-      float wa[8], wb[8];
-      trilinear_weights((pax - lo_x) * vox_l_inv, (pay - lo_y) * vox_l_inv, (paz - lo_z) * vox_l_inv, wa);
-      trilinear_weights((pbx - lo_x) * vox_l_inv, (pby - lo_y) * vox_l_inv, (pbz - lo_z) * vox_l_inv, wb);
-      float d_a = 0.f, d_b = 0.f;
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        d_a += geo[c] * wa[c];
-        d_b += geo[c] * wb[c];
+    const float exp_neg = exp_f<FAST>(-vol_int);
+    const float alpha = fminf(kMaxAlpha, 1.f - exp_neg);
+    if (!(alpha < kMinAlpha)) {
+      contrib = true;
+      T = div_f<FAST>(T, 1.f - alpha);
+      const float pt_w = alpha * T;
+      const float4 rgbv = s.rgb[j];
+      float dL_dpt_w = gx * rgbv.x + gy * rgbv.y + gz * rgbv.z;
+      if (DIST) {
+        const float adist = contract_depth(a), bdist = contract_depth(b);
+        const float now_m = 0.5f * (adist + bdist);
+        const float now_wm = now_m * pt_w;
+        prefix_wm -= now_wm;
+        prefix_w -= pt_w;
+        const float uni = 0.6666666f * pt_w * (bdist - adist);
+        const float bi = 2.f * (now_m * (prefix_w - suffix_w) - (prefix_wm - suffix_wm));
+        dL_dpt_w += weight_dist * (uni + bi);
+        suffix_wm += now_wm;
+        suffix_w += pt_w;
       }
-      const float reg_w = weight_asc * pt_w * static_cast<float>(d_a > d_b);
+      if (NORMAL) {
+        float nx, ny, nz;
+        field_normal(geo, nx, ny, nz);
+        const float rl = safe_rnorm3(nx, ny, nz);
+        const float sx = rl * nx, sy = rl * ny, sz = rl * nz;
+        dL_dpt_w += dNx * sx + dNy * sy + dNz * sz;
+        const float dsx = pt_w * dNx, dsy = pt_w * dNy, dsz = pt_w * dNz;
+        const float dot_ = dsx * nx + dsy * ny + dsz * nz;
+        const float lnx = rl * (dsx - dot_ * rl * sx);
+        const float lny = rl * (dsy - dot_ * rl * sy);
+        const float lnz = rl * (dsz - dot_ * rl * sz);
+        dgeo[0] += -lnx - lny - lnz;
+        dgeo[1] += -lnx - lny + lnz;
+        dgeo[2] += -lnx + lny - lnz;
+        dgeo[3] += -lnx + lny + lnz;
+        dgeo[4] += +lnx - lny - lnz;
+        dgeo[5] += +lnx - lny + lnz;
+        dgeo[6] += +lnx + lny - lnz;
+        dgeo[7] += +lnx + lny + lnz;
+      }
+      const float dL_dalpha = T * (dL_dpt_w - last_dL_dT);
+      last_dL_dT += alpha * (dL_dpt_w - last_dL_dT);
+      const float dL_dI = dL_dalpha * exp_neg;
+      if (kFoldScale) {
+        const float sI = dL_dI * dI_dgeo[0];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) dgeo[c] += reg_w * (wa[c] - wb[c]);
-    }
-    float drx = pt_w * gx, dry = pt_w * gy, drz = pt_w * gz;
-    if (in.lambda_R_concen > 0) {
-      const float sR = weight_R * pt_w * 2.0f;
-      drx += sR * (rgbv.x - gtx);
-      dry += sR * (rgbv.y - gty);
-      drz += sR * (rgbv.z - gtz);
-    }
+        for (int c = 0; c < 8; ++c) dgeo[c] += sI * w[c];
+      } else {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) gp[c] = dgeo[c];
-    gp[8] = drx; gp[9] = dry; gp[10] = drz;
-    gp[11] = fabsf(dL_dalpha * alpha);
+        for (int c = 0; c < 8; ++c) dgeo[c] += dL_dI * dI_dgeo[c];
+      }
+      if (DEPTH) {
+        float dval;
+        float dI[NS];
+        if (NS == 3) {
+          const float ss = 0.3333333f * (b - a);
+          const float a0 = local_alpha[0], a1 = local_alpha[NS > 1 ? 1 : 0], a2 = local_alpha[NS > 2 ? 2 : 0];
+          const float t0_ = a + 0.5f * ss, t1_ = a + 1.5f * ss, t2_ = a + 2.5f * ss;
+          dval = a0 * t0_ + (1.f - a0) * a1 * t1_ + (1.f - a0) * (1.f - a1) * a2 * t2_;
+          dI[0] = dL_dD * T * (t0_ + a1 * a2 * t2_ - a1 * t1_ - a2 * t2_) * (1.f - a0);
+          dI[NS > 1 ? 1 : 0] = dL_dD * T * (t1_ + a0 * a2 * t2_ - a0 * t1_ - a2 * t2_) * (1.f - a1);
+          dI[NS > 2 ? 2 : 0] = dL_dD * T * (t2_ + a0 * a1 * t2_ - a0 * t2_ - a1 * t2_) * (1.f - a2);
+        } else if (NS == 2) {
+          const float ss = 0.5f * (b - a);
+          const float a0 = local_alpha[0], a1 = local_alpha[NS > 1 ? 1 : 0];
+          const float t0_ = a + 0.5f * ss, t1_ = a + 1.5f * ss;
+          dval = a0 * t0_ + (1.f - a0) * a1 * t1_;
+          dI[0] = dL_dD * T * (t0_ - a1 * t1_) * (1.f - a0);
+          dI[NS > 1 ? 1 : 0] = dL_dD * T * (t1_ - a0 * t1_) * (1.f - a1);
+        } else {
+          const float t0_ = 0.5f * (a + b);
+          dval = alpha * t0_;
+          dI[0] = dL_dD * T * t0_ * (1.f - alpha);
+        }
+        last_dL_dT += dL_dD * dval;
+        if (NS == 3) {
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            dgeo[c] += dI[0] * each_dI[0][c] + dI[NS > 1 ? 1 : 0] * each_dI[NS > 1 ? 1 : 0][c] +
+                       dI[NS > 2 ? 2 : 0] * each_dI[NS > 2 ? 2 : 0][c];
+        } else if (NS == 2) {
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            dgeo[c] += dI[0] * each_dI[0][c] + dI[NS > 1 ? 1 : 0] * each_dI[NS > 1 ? 1 : 0][c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 8; ++c) dgeo[c] += dI[0] * dI_dgeo[c];
+        }
+      }
+      if (in.lambda_ascending > 0) {
+        const float lo_x = cr.x, lo_y = cr.y, lo_z = cr.z;
+        const float pax = ray.ox + a * ray.dx, pay = ray.oy + a * ray.dy, paz = ray.oz + a * ray.dz;
+        const float pbx = ray.ox + b * ray.dx, pby = ray.oy + b * ray.dy, pbz = ray.oz + b * ray.dz;
+        float wa[8], wb[8];
+        trilinear_weights((pax - lo_x) * vox_l_inv, (pay - lo_y) * vox_l_inv, (paz - lo_z) * vox_l_inv, wa);
+        trilinear_weights((pbx - lo_x) * vox_l_inv, (pby - lo_y) * vox_l_inv, (pbz - lo_z) * vox_l_inv, wb);
+        float d_a = 0.f, d_b = 0.f;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          d_a += geo[c] * wa[c];
+          d_b += geo[c] * wb[c];
+        }
+        const float reg_w = weight_asc * pt_w * static_cast<float>(d_a > d_b);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) dgeo[c] += reg_w * (wa[c] - wb[c]);
+      }
+      float drx = pt_w * gx, dry = pt_w * gy, drz = pt_w * gz;
+      if (in.lambda_R_concen > 0) {
+        const float sR = weight_R * pt_w * 2.0f;
+        drx += sR * (rgbv.x - gtx);
+        dry += sR * (rgbv.y - gty);
+        drz += sR * (rgbv.z - gtz);
+      }
+#pragma unroll
+      for (int c = 0; c < 8; ++c) gp[c] = dgeo[c];
+      gp[8] = drx; gp[9] = dry; gp[10] = drz;
+      gp[11] = fabsf(dL_dalpha * alpha);
+    }
   }
-}
   return contrib;
 }
 

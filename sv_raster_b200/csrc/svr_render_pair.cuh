@@ -285,8 +285,12 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
             const float lvi = kStepScale * step_sz * act;
             vol_int += lvi;
             const float dd_dd = kStepScale * step_sz * act_grad;
+            if (FAST && NS == 1) {
+              dI_dgeo[0] = dd_dd;  // the weights stay in w: dL/dgeo = (dL/dI * dd_dd) * w below
+            } else {
 #pragma unroll
-            for (int c = 0; c < 8; ++c) dI_dgeo[c] += dd_dd * w[c];
+              for (int c = 0; c < 8; ++c) dI_dgeo[c] += dd_dd * w[c];
+            }
             qx = qx + qsx; qy = qy + qsy; qz = qz + qsz;
           }
           const float exp_neg = exp_f<FAST>(-vol_int);
@@ -300,8 +304,14 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
           const float dL_dalpha = T[k] * (dL_dpt_w - last_dL_dT[k]);
           last_dL_dT[k] += alpha * (dL_dpt_w - last_dL_dT[k]);
           const float dL_dI = dL_dalpha * exp_neg;
+          if (FAST && NS == 1) {
+            const float sI = dL_dI * dI_dgeo[0];
 #pragma unroll
-          for (int c = 0; c < 8; ++c) gp[c] += dL_dI * dI_dgeo[c];
+            for (int c = 0; c < 8; ++c) gp[c] += sI * w[c];
+          } else {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) gp[c] += dL_dI * dI_dgeo[c];
+          }
           gp[8] += pt_w * gx[k];
           gp[9] += pt_w * gy[k];
           gp[10] += pt_w * gz[k];
