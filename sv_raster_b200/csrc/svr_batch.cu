@@ -79,8 +79,11 @@ project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* _
     atomicOr(err, SVR_DEVERR_LEVEL);
   const float cx = centers[3 * (size_t)i], cy = centers[3 * (size_t)i + 1], cz = centers[3 * (size_t)i + 2];
   const float len = lengths[i];
+  // The rest coefficients are read per visible view through the cache
+  // (holding 45 of them in registers across the views cost the kernel half
+  // its occupancy).
+  const TS* sh = shs + (size_t)i * (M - 1) * 3;
   float c0[3];
-  float shr[NB > 0 ? NB * 3 : 1];
   bool loaded = false;
   for (int v = 0; v < views.n; ++v) {
     const size_t o = (size_t)v * P + i;
@@ -94,9 +97,6 @@ project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* _
     if (!loaded) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) c0[c] = ldf(sh0, 3 * (size_t)i + c);
-      const TS* sh = shs + (size_t)i * (M - 1) * 3;
-#pragma unroll
-      for (int k = 0; k < NB * 3; ++k) shr[k] = ldf(sh, k);
       loaded = true;
     }
     // View-dependent colour of this visible voxel (sh_compute.cu:54-106).
@@ -104,7 +104,7 @@ project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* _
     const float rn = rnorm3df(dx, dy, dz);
     dx = dx * rn; dy = dy * rn; dz = dz * rn;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) rgbs[3 * o + c] = sh_channel<DEG>(dx, dy, dz, c0[c], shr, c);
+    for (int c = 0; c < 3; ++c) rgbs[3 * o + c] = sh_channel<DEG>(dx, dy, dz, c0[c], sh, c);
   }
 }
 
