@@ -177,97 +177,6 @@ __device__ __forceinline__ void render_tile_fwd_pair(const ViewParams& vp, const
   }
 }
 
-// Both pixels of a lane against staged record j, interleaved: used when
-// records reach both pixel rows of the warp, every step of the two pixels'
-// arithmetic is issued back to back without branches, and each pixel's
-// results are kept only where it is a candidate (cand) and the record
-// contributes, so the two dependency chains overlap instead of running one
-// after the other.  Each pixel's operations and their order are those of the
-// one-pixel step in render_tile_bwd_pair, so its values are unchanged; the
-// values computed for a pixel that does not take them (a missed slab, an
-// alpha under the threshold) are discarded by selects.
-template <int SB, int NS, bool FAST>
-__device__ __forceinline__ bool pair_bwd_both(const StageSmem<SB>& s, int j, const float4& slo, const float4& shi,
-                                              const PixelRay (&ray)[2], const bool (&cand)[2], float (&T)[2],
-                                              const float (&gx)[2], const float (&gy)[2], const float (&gz)[2],
-                                              float (&last_dL_dT)[2], float gp[12]) {
-  constexpr bool kFold = FAST && NS == 1;
-  float geo[8];
-  load_geo(s, j, geo);
-  const float vox_l_inv = slo.w;
-  const float4 cr = s.corner[j];
-  bool hit[2];
-  float vol_int[2], dI_dgeo[2][8], wk[2][8];
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const float2 ab = staged_ray_box(slo, shi, ray[k]);
-    const float a = ab.x, b = ab.y;
-    hit[k] = cand[k] && !(a > b);
-    vol_int[k] = 0.f;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) dI_dgeo[k][c] = 0.f;
-    const float step_sz = (b - a) * (1.f / NS);
-    const float stx = step_sz * ray[k].dx, sty = step_sz * ray[k].dy, stz = step_sz * ray[k].dz;
-    const float t0 = a + 0.5f * step_sz;
-    const float ptx = ray[k].ox + t0 * ray[k].dx, pty = ray[k].oy + t0 * ray[k].dy, ptz = ray[k].oz + t0 * ray[k].dz;
-    float qx = (ptx - cr.x) * vox_l_inv;
-    float qy = (pty - cr.y) * vox_l_inv;
-    float qz = (ptz - cr.z) * vox_l_inv;
-    const float qsx = stx * vox_l_inv, qsy = sty * vox_l_inv, qsz = stz * vox_l_inv;
-#pragma unroll
-    for (int n = 0; n < NS; ++n) {
-      float w[8];
-      trilinear_weights(qx, qy, qz, w);
-      float d = 0.f;
-#pragma unroll
-      for (int c = 0; c < 8; ++c) d += geo[c] * w[c];
-      float act, act_grad;
-      density_act_and_grad_f<FAST>(d, act, act_grad);
-      vol_int[k] += kStepScale * step_sz * act;
-      const float dd_dd = kStepScale * step_sz * act_grad;
-      if (kFold) {
-        dI_dgeo[k][0] = dd_dd;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) wk[k][c] = w[c];
-      } else {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) dI_dgeo[k][c] += dd_dd * w[c];
-      }
-      qx = qx + qsx; qy = qy + qsy; qz = qz + qsz;
-    }
-  }
-  const float4 rgbv = s.rgb[j];
-  bool contrib = false;
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const float exp_neg = exp_f<FAST>(-vol_int[k]);
-    const float alpha = fminf(kMaxAlpha, 1.f - exp_neg);
-    const bool c = hit[k] && !(alpha < kMinAlpha);
-    const float Tn = div_f<FAST>(T[k], 1.f - alpha);
-    const float pt_w = alpha * Tn;
-    const float dL_dpt_w = gx[k] * rgbv.x + gy[k] * rgbv.y + gz[k] * rgbv.z;
-    const float dL_dalpha = Tn * (dL_dpt_w - last_dL_dT[k]);
-    const float next_dL_dT = last_dL_dT[k] + alpha * (dL_dpt_w - last_dL_dT[k]);
-    const float dL_dI = dL_dalpha * exp_neg;
-    T[k] = c ? Tn : T[k];
-    last_dL_dT[k] = c ? next_dL_dT : last_dL_dT[k];
-    if (kFold) {
-      const float sI = dL_dI * dI_dgeo[k][0];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) gp[q] += c ? sI * wk[k][q] : 0.f;
-    } else {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) gp[q] += c ? dL_dI * dI_dgeo[k][q] : 0.f;
-    }
-    gp[8] += c ? pt_w * gx[k] : 0.f;
-    gp[9] += c ? pt_w * gy[k] : 0.f;
-    gp[10] += c ? pt_w * gz[k] : 0.f;
-    gp[11] += c ? fabsf(dL_dalpha * alpha) : 0.f;
-    contrib |= c;
-  }
-  return contrib;
-}
-
 template <class CFG, int NS, bool FAST>
 __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const float* __restrict__ c2w_s,
                                                      int tile_x, int tile_y, uint2 range_raw, uint32_t tile_last,
@@ -341,16 +250,9 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
         for (int c = 0; c < 12; ++c) gp[c] = 0.f;
         bool contrib = false;
         const float4 slo = s.slab_lo[j], shi = s.slab_hi[j];
-        bool cand[2];
-#pragma unroll
-        for (int k = 0; k < 2; ++k)
-          cand[k] = inside[k] && jpos < last_contrib[k] && record_hits_pixel(s, j, px, py[k], ray[k].quad);
-        if (__any_sync(0xffffffffu, cand[0]) && __any_sync(0xffffffffu, cand[1])) {
-          contrib = pair_bwd_both<SB, NS, FAST>(s, j, slo, shi, ray, cand, T, gx, gy, gz, last_dL_dT, gp);
-        } else {
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-          if (!cand[k]) continue;
+          if (!(inside[k] && jpos < last_contrib[k]) || !record_hits_pixel(s, j, px, py[k], ray[k].quad)) continue;
           const float2 ab = staged_ray_box(slo, shi, ray[k]);
           const float a = ab.x, b = ab.y;
           if (a > b) continue;
@@ -414,7 +316,6 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
           gp[9] += pt_w * gy[k];
           gp[10] += pt_w * gz[k];
           gp[11] += fabsf(dL_dalpha * alpha);
-        }
         }
         // One warp reduction for both pixels' gradients of this record.
         const uint32_t act_mask = __ballot_sync(0xffffffffu, contrib);
