@@ -364,6 +364,24 @@ int svr_batch_render(svr_batch_plan* plan, void* workspace, const float* vox_cen
 int svr_batch_backward(svr_batch_plan* plan, void* workspace, const float* vox_centers, const float* vox_lengths,
                        const void* geos, int geos_bf16, const float* out_T, const float* dL_dcolor,
                        const float* dL_dT, float* dL_dgeos, void* stream);
+/* svr_batch_render / svr_batch_backward with the densities as grid points:
+ * corner c of voxel p is grid[vox_key[8 p + c]] (vox_key int64 [P,8], grid
+ * fp32 or bf16 [M]), read while each record is staged, and the backward adds
+ * every record's corner gradients straight into dL_dgrid (fp32 [M],
+ * accumulated: zero it first) -- GatherGeoParams and its backward
+ * (renderer.py:319-345, geo_params_gather.cu:22-72) fused into the staging
+ * and the flush.  The results equal svr_gather_grid_geo_all + svr_batch_render
+ * / svr_batch_backward + svr_scatter_grid_geo_all (images bitwise; gradients
+ * to the order of additions).  The grid reads and atomics are per (voxel,
+ * tile) instead of per voxel, so the separate gather and scatter cost less
+ * once each voxel is staged several times per step (many views). */
+int svr_batch_render_grid(svr_batch_plan* plan, void* workspace, const float* vox_centers, const float* vox_lengths,
+                          const int64_t* vox_key, const void* grid, int grid_bf16, float* out_color, float* out_T,
+                          void* stream);
+int svr_batch_backward_grid(svr_batch_plan* plan, void* workspace, const float* vox_centers,
+                            const float* vox_lengths, const int64_t* vox_key, const void* grid, int grid_bf16,
+                            const float* out_T, const float* dL_dcolor, const float* dL_dT, float* dL_dgrid,
+                            void* stream);
 /* dL/dsh0 [P,3] and dL/dshs [P,M-1,3] summed over views (overwritten), and,
  * when subdiv is not null, the subdivision priority subdiv_p_bw [P] summed
  * over views (overwritten; backward.cu:514 per view). */

@@ -15,6 +15,10 @@ stream after warm-up, on the seeded 2M-voxel scene with one 1297x840 view
   distortion and normal outputs off and on (the regulariser inputs of
   backward.cu), showing what the extra outputs cost on top of the colour.
 
+``--grid-step c2,c4`` instead times the batched step with grid-point
+densities, gathered and scattered separately or fused into the compositing
+kernels (see ``grid_step``).
+
 Inputs of the gathers are larger than L2 (126 MB) only for their index
 arrays; the grid values themselves are read at random, so their figures are
 bounded by the gather pattern rather than by streaming bandwidth.
@@ -59,14 +63,84 @@ def _peak_gbs():
         return 6650.0, "fallback"
 
 
+class _DevCam:
+    def __init__(self, c, dev):
+        self.width, self.height, self.tanfovx, self.tanfovy = c.width, c.height, c.tanfovx, c.tanfovy
+        self.cx, self.cy, self.near = c.cx, c.cy, c.near
+        self.w2c = torch.from_numpy(c.w2c).to(dev)
+        self.c2w = torch.from_numpy(c.c2w).to(dev)
+
+
+def grid_step(configs, reps, warmup):
+    """Batched compositing of a configuration's views with grid-point
+    densities, two ways: the separate all-voxel gather + render + backward +
+    scatter, and the fused form whose staging reads the grid points and whose
+    flush adds into the grid gradient (svr_batch_render_grid /
+    svr_batch_backward_grid).  8x8 tiles, forward staging 64, backward
+    staging 32 with two pixels per thread, fp32 grid; prepare excluded."""
+    from sv_raster_b200.batched import BatchedRasterizer, gather_grid_geos, scatter_grid_grad
+    dev = torch.device("cuda")
+    t = lambda a, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(a)).to(dev, dt)
+    out = {}
+    for name in configs:
+        sc = synthetic.cached_config_scene(name)
+        key, grid_np = synthetic.grid_params(sc, dev)
+        key, grid = key.contiguous(), t(grid_np)
+        P, M = sc.n_voxels, grid.numel()
+        r = BatchedRasterizer([_DevCam(c, dev) for c in sc.cameras], t(sc.octpath.reshape(-1), torch.int64),
+                              t(sc.centers), t(sc.lengths), max_level=sc.max_level, tile_size=8)
+        r.set_staging(64)
+        r.set_backward_staging(32)
+        r.set_backward_pixels_per_thread(2)
+        sh0, shs = t(sc.sh0), t(sc.shs)
+        r.fit_capacity(sh0, shs, 3)
+        r.prepare(sh0, shs, 3)
+        g = torch.Generator(device=dev).manual_seed(3)
+        dC = torch.randn(3 * r.n_pixels, device=dev, generator=g) * 1e-3
+        dT = torch.zeros(r.n_pixels, device=dev)
+        geos, dgeos, dgrid = torch.empty(P, 8, device=dev), torch.zeros(P, 8, device=dev), torch.zeros(M, device=dev)
+        color, T = torch.empty(3 * r.n_pixels, device=dev), torch.empty(r.n_pixels, device=dev)
+
+        def separate():
+            gather_grid_geos(key, grid, geos)
+            r.render(geos, color, T)
+            dgeos.zero_()
+            r.backward_render(geos, T, dC, dT, dgeos)
+            scatter_grid_grad(key, dgeos, dgrid)
+
+        def fused():
+            r.render_grid(key, grid, color, T)
+            r.backward_render_grid(key, grid, T, dC, dT, dgrid)
+
+        ops = {"separate": separate, "fused": fused,
+               "gather": lambda: gather_grid_geos(key, grid, geos),
+               "render": lambda: r.render(geos, color, T),
+               "backward": lambda: r.backward_render(geos, T, dC, dT, dgeos),
+               "scatter": lambda: scatter_grid_grad(key, dgeos, dgrid),
+               "render_grid": lambda: r.render_grid(key, grid, color, T),
+               "backward_grid": lambda: r.backward_render_grid(key, grid, T, dC, dT, dgrid)}
+        out[name] = {"voxels": P, "grid_points": M, "views": len(sc.cameras), "instances": r.header()[0],
+                     "ms": {k: round(time_ms(fn, reps, warmup), 4) for k, fn in ops.items()}}
+        del r
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--voxels", type=int, default=None)
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--grid-step", default=None,
+                    help="comma-separated configurations (e.g. c2,c4): separate vs fused grid-point batched step")
     args = ap.parse_args()
     if not torch.cuda.is_available():
         raise SystemExit("opbench needs a CUDA device")
+    if args.grid_step:
+        res = grid_step(args.grid_step.split(","), args.reps, args.warmup)
+        res["device"] = torch.cuda.get_device_name(torch.device("cuda"))
+        print(json.dumps(res))
+        return
     dev = torch.device("cuda")
     sc = synthetic.cached_config_scene("c2", n_voxels=args.voxels)
     N = len(sc.octpath)

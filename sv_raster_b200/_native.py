@@ -109,6 +109,8 @@ _SIGS = {
     "svr_batch_prepare": (c_int, [c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_int, c_int, c_int, c_p]),
     "svr_batch_render": (c_int, [c_p, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_p]),
     "svr_batch_backward": (c_int, [c_p, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_p, c_p, c_p]),
+    "svr_batch_render_grid": (c_int, [c_p, c_p, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_p]),
+    "svr_batch_backward_grid": (c_int, [c_p, c_p, c_p, c_p, c_p, c_p, c_int, c_p, c_p, c_p, c_p, c_p]),
     "svr_batch_sh_backward": (c_int, [c_p, c_p, c_p, c_int, c_int, c_p, c_p, c_p, c_p]),
 }
 

@@ -254,6 +254,27 @@ class BatchedRasterizer:
                                        self._p(dL_dcolor), self._p(dL_dT), self._p(dL_dgeos), self._stream()),
               "batch_backward")
 
+    def render_grid(self, vox_key, grid_pts, out_color=None, out_T=None):
+        """render() with grid-point densities read while staging: corner c of
+        voxel p is grid_pts[vox_key[p, c]] (vox_key int64 [P,8], grid fp32 or
+        bf16).  Same outputs as gather_grid_geos + render."""
+        if out_color is None:
+            out_color = torch.empty(3 * self.n_pixels, device=self.dev)
+            out_T = torch.empty(self.n_pixels, device=self.dev)
+        check(lib().svr_batch_render_grid(self.plan, self._p(self.ws), self._p(self.centers), self._p(self.lengths),
+                                          self._p(vox_key), self._p(grid_pts), int(grid_pts.dtype == torch.bfloat16),
+                                          self._p(out_color), self._p(out_T), self._stream()), "batch_render_grid")
+        return out_color, out_T
+
+    def backward_render_grid(self, vox_key, grid_pts, out_T, dL_dcolor, dL_dT, dL_dgrid):
+        """backward_render() adding each record's corner gradients straight
+        into dL_dgrid [M] fp32 (accumulates; zero it first)."""
+        check(lib().svr_batch_backward_grid(self.plan, self._p(self.ws), self._p(self.centers), self._p(self.lengths),
+                                            self._p(vox_key), self._p(grid_pts),
+                                            int(grid_pts.dtype == torch.bfloat16), self._p(out_T),
+                                            self._p(dL_dcolor), self._p(dL_dT), self._p(dL_dgrid), self._stream()),
+              "batch_backward_grid")
+
     def backward_sh(self, sh_degree, M, dL_dsh0, dL_dshs, subdiv=None):
         """SH gradients (and the subdivision priority) summed over views, from
         the colour gradients of the last backward_render (overwritten)."""
@@ -343,26 +364,43 @@ class GridBatchedRender(torch.autograd.Function):
     (grid_pts [M], sh0, shs) -> (color flat, T flat) over all views.  The
     corner densities are gathered once per step for all views into a [P,8]
     buffer of the grid's dtype, and the density gradients are added back into
-    the grid gradient once per step."""
+    the grid gradient once per step.  With ``fused=True`` the compositing
+    kernels read the grid points while staging each record and add the
+    corner gradients into the grid gradient in their flush instead (no [P,8]
+    buffer; per (voxel, tile) grid accesses instead of per voxel -- measured
+    equal at one view per step and slower with many, see
+    svr_batch_render_grid)."""
 
     @staticmethod
-    def forward(ctx, raster, sh_degree, vox_key, grid_pts, sh0, shs):
-        geos = torch.empty(vox_key.shape[0], 8, dtype=grid_pts.dtype, device=grid_pts.device)
-        gather_grid_geos(vox_key, grid_pts, geos)
+    def forward(ctx, raster, sh_degree, vox_key, grid_pts, sh0, shs, fused=False):
         raster.prepare(sh0, shs, sh_degree)
-        color, T = raster.render(geos)
-        ctx.raster, ctx.sh_degree, ctx.M = raster, sh_degree, 1 + shs.shape[1]
+        if fused:
+            geos = None
+            color, T = raster.render_grid(vox_key, grid_pts)
+            ctx.save_for_backward(vox_key, grid_pts, T)
+        else:
+            geos = torch.empty(vox_key.shape[0], 8, dtype=grid_pts.dtype, device=grid_pts.device)
+            gather_grid_geos(vox_key, grid_pts, geos)
+            color, T = raster.render(geos)
+            ctx.save_for_backward(vox_key, geos, T)
+        ctx.raster, ctx.sh_degree, ctx.M, ctx.fused = raster, sh_degree, 1 + shs.shape[1], bool(fused)
         ctx.sh_dtype, ctx.grid_dtype, ctx.M_grid = sh0.dtype, grid_pts.dtype, grid_pts.shape[0]
-        ctx.save_for_backward(vox_key, geos, T)
         return color, T
 
     @staticmethod
     def backward(ctx, dL_dcolor, dL_dT):
-        vox_key, geos, T = ctx.saved_tensors
+        vox_key, dens, T = ctx.saved_tensors
         r = ctx.raster
         if dL_dT is None:
             dL_dT = torch.zeros_like(T)
-        dgeo, _sub, dsh0, dshs = r.backward(geos, T, dL_dcolor.contiguous(), dL_dT.contiguous(), ctx.sh_degree, ctx.M)
-        dgrid = torch.zeros(ctx.M_grid, dtype=torch.float32, device=dgeo.device)
-        scatter_grid_grad(vox_key, dgeo, dgrid)
-        return None, None, None, dgrid.to(ctx.grid_dtype), dsh0.to(ctx.sh_dtype), dshs.to(ctx.sh_dtype)
+        dgrid = torch.zeros(ctx.M_grid, dtype=torch.float32, device=T.device)
+        P, M = vox_key.shape[0], ctx.M
+        if ctx.fused:
+            r.backward_render_grid(vox_key, dens, T, dL_dcolor.contiguous(), dL_dT.contiguous(), dgrid)
+            dsh0 = torch.empty(P, 3, device=T.device)
+            dshs = torch.empty(P, M - 1, 3, device=T.device)
+            r.backward_sh(ctx.sh_degree, M, dsh0, dshs)
+        else:
+            dgeo, _sub, dsh0, dshs = r.backward(dens, T, dL_dcolor.contiguous(), dL_dT.contiguous(), ctx.sh_degree, M)
+            scatter_grid_grad(vox_key, dgeo, dgrid)
+        return (None, None, None, dgrid.to(ctx.grid_dtype), dsh0.to(ctx.sh_dtype), dshs.to(ctx.sh_dtype), None)

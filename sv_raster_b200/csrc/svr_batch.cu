@@ -811,14 +811,13 @@ int svr_batch_prepare(svr_batch_plan* p, void* ws, const int64_t* octree_paths, 
   return check_last();
 }
 
-int svr_batch_render(svr_batch_plan* p, void* ws, const float* vox_centers, const float* vox_lengths,
-                     const void* geos, int geos_bf16, float* out_color, float* out_T, void* stream_) {
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
-  if (!p || !ws || !vox_centers || !vox_lengths || !geos || !out_color || !out_T) return SVR_ERR_SHAPE;
-  if ((reinterpret_cast<uintptr_t>(geos) & 15u) != 0) return SVR_ERR_ALIGN;
+// Compositing of all views with the densities either per voxel (geos) or
+// as grid points read through the voxels' corner indices (va.key).
+static int batch_render(svr_batch_plan* p, void* ws, VoxelArrays va, float* out_color, float* out_T,
+                        cudaStream_t stream) {
   BatchPtrs q = ptrs(p, ws);
-  VoxelArrays va{q.bbox, vox_centers, vox_lengths, geos_bf16 ? nullptr : (const float*)geos,
-                 geos_bf16 ? (const __nv_bfloat16*)geos : nullptr, q.rgbs};
+  va.bboxes = q.bbox;
+  va.rgbs = q.rgbs;
   FwdTileOut out{q.tile_last, q.ncontrib, out_color, nullptr, nullptr, out_T, nullptr};
   const bool ordered = (p->order_flags & 1) != 0;
   if (ordered) build_tile_order(p, q, nullptr, q.order_fwd, stream);
@@ -828,21 +827,16 @@ int svr_batch_render(svr_batch_plan* p, void* ws, const float* vox_centers, cons
   return check_last();
 }
 
-int svr_batch_backward(svr_batch_plan* p, void* ws, const float* vox_centers, const float* vox_lengths,
-                       const void* geos, int geos_bf16, const float* out_T, const float* dL_dcolor,
-                       const float* dL_dT, float* dL_dgeos, void* stream_) {
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
-  if (!p || !ws || !vox_centers || !vox_lengths || !geos || !out_T || !dL_dcolor || !dL_dT || !dL_dgeos)
-    return SVR_ERR_SHAPE;
-  if ((reinterpret_cast<uintptr_t>(geos) & 15u) != 0 || (reinterpret_cast<uintptr_t>(dL_dgeos) & 15u) != 0)
-    return SVR_ERR_ALIGN;
+static int batch_backward(svr_batch_plan* p, void* ws, VoxelArrays va, const float* out_T, const float* dL_dcolor,
+                          const float* dL_dT, BwdTileOut out, cudaStream_t stream) {
   BatchPtrs q = ptrs(p, ws);
   cudaMemsetAsync(q.drgbs, 0, (size_t)p->V * p->P * 16, stream);
-  VoxelArrays va{q.bbox, vox_centers, vox_lengths, geos_bf16 ? nullptr : (const float*)geos,
-                 geos_bf16 ? (const __nv_bfloat16*)geos : nullptr, q.rgbs};
+  va.bboxes = q.bbox;
+  va.rgbs = q.rgbs;
   BwdTileIn in{out_T, q.ncontrib, dL_dcolor, nullptr, nullptr, dL_dT, nullptr, nullptr, 0.f, 0.f, 0.f,
                p->atomic_lanes};
-  BwdTileOut out{dL_dgeos, q.drgbs, nullptr, q.header + 1, 1};
+  out.dL_drgbs = q.drgbs;
+  out.err = q.header + 1;
   const bool ordered = (p->order_flags & 2) != 0;
   if (ordered) build_tile_order(p, q, q.tile_last, q.order_bwd, stream);
   launch_render_bwd_batch(p->vt, (int)p->total_tiles, q.ranges, q.tile_last, p->cap > 0 ? q.vb : nullptr, va,
@@ -851,6 +845,54 @@ int svr_batch_backward(svr_batch_plan* p, void* ws, const float* vox_centers, co
                           ordered ? q.order_bwd : nullptr, q.header + 3,
                           p->bwd_ctas_per_sm, stream);
   return check_last();
+}
+
+int svr_batch_render(svr_batch_plan* p, void* ws, const float* vox_centers, const float* vox_lengths,
+                     const void* geos, int geos_bf16, float* out_color, float* out_T, void* stream_) {
+  if (!p || !ws || !vox_centers || !vox_lengths || !geos || !out_color || !out_T) return SVR_ERR_SHAPE;
+  if ((reinterpret_cast<uintptr_t>(geos) & 15u) != 0) return SVR_ERR_ALIGN;
+  VoxelArrays va{nullptr, vox_centers, vox_lengths, geos_bf16 ? nullptr : (const float*)geos,
+                 geos_bf16 ? (const __nv_bfloat16*)geos : nullptr, nullptr};
+  return batch_render(p, ws, va, out_color, out_T, static_cast<cudaStream_t>(stream_));
+}
+
+int svr_batch_render_grid(svr_batch_plan* p, void* ws, const float* vox_centers, const float* vox_lengths,
+                          const int64_t* vox_key, const void* grid, int grid_bf16, float* out_color, float* out_T,
+                          void* stream_) {
+  if (!p || !ws || !vox_centers || !vox_lengths || !vox_key || !grid || !out_color || !out_T) return SVR_ERR_SHAPE;
+  VoxelArrays va{nullptr, vox_centers, vox_lengths, nullptr, nullptr, nullptr};
+  va.key = vox_key;
+  va.grid = grid_bf16 ? nullptr : (const float*)grid;
+  va.grid_bf16 = grid_bf16 ? (const __nv_bfloat16*)grid : nullptr;
+  return batch_render(p, ws, va, out_color, out_T, static_cast<cudaStream_t>(stream_));
+}
+
+int svr_batch_backward(svr_batch_plan* p, void* ws, const float* vox_centers, const float* vox_lengths,
+                       const void* geos, int geos_bf16, const float* out_T, const float* dL_dcolor,
+                       const float* dL_dT, float* dL_dgeos, void* stream_) {
+  if (!p || !ws || !vox_centers || !vox_lengths || !geos || !out_T || !dL_dcolor || !dL_dT || !dL_dgeos)
+    return SVR_ERR_SHAPE;
+  if ((reinterpret_cast<uintptr_t>(geos) & 15u) != 0 || (reinterpret_cast<uintptr_t>(dL_dgeos) & 15u) != 0)
+    return SVR_ERR_ALIGN;
+  VoxelArrays va{nullptr, vox_centers, vox_lengths, geos_bf16 ? nullptr : (const float*)geos,
+                 geos_bf16 ? (const __nv_bfloat16*)geos : nullptr, nullptr};
+  BwdTileOut out{dL_dgeos, nullptr, nullptr, nullptr, 1};
+  return batch_backward(p, ws, va, out_T, dL_dcolor, dL_dT, out, static_cast<cudaStream_t>(stream_));
+}
+
+int svr_batch_backward_grid(svr_batch_plan* p, void* ws, const float* vox_centers, const float* vox_lengths,
+                            const int64_t* vox_key, const void* grid, int grid_bf16, const float* out_T,
+                            const float* dL_dcolor, const float* dL_dT, float* dL_dgrid, void* stream_) {
+  if (!p || !ws || !vox_centers || !vox_lengths || !vox_key || !grid || !out_T || !dL_dcolor || !dL_dT || !dL_dgrid)
+    return SVR_ERR_SHAPE;
+  VoxelArrays va{nullptr, vox_centers, vox_lengths, nullptr, nullptr, nullptr};
+  va.key = vox_key;
+  va.grid = grid_bf16 ? nullptr : (const float*)grid;
+  va.grid_bf16 = grid_bf16 ? (const __nv_bfloat16*)grid : nullptr;
+  BwdTileOut out{nullptr, nullptr, nullptr, nullptr, 0};
+  out.key = vox_key;
+  out.grid_grad = dL_dgrid;
+  return batch_backward(p, ws, va, out_T, dL_dcolor, dL_dT, out, static_cast<cudaStream_t>(stream_));
 }
 
 int svr_batch_sh_backward(svr_batch_plan* p, void* ws, const float* vox_centers, int sh_degree, int M,

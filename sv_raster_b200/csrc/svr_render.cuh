@@ -74,6 +74,12 @@ struct VoxelArrays {
   const float* geos;          // [P,8] fp32, or nullptr when geos_bf16 is set
   const __nv_bfloat16* geos_bf16;  // [P,8] bf16 storage
   const float* rgbs;          // [P,3] (this view)
+  // Grid-point densities (batched grid entry points): when key is set, corner
+  // c of voxel v is grid[key[8 v + c]] (fp32 grid, or grid_bf16), read while
+  // staging the record, and geos / geos_bf16 are unused.
+  const int64_t* key = nullptr;
+  const float* grid = nullptr;
+  const __nv_bfloat16* grid_bf16 = nullptr;
 };
 
 // One staged record.  Besides the raw attributes it holds the per-record
@@ -105,7 +111,14 @@ __device__ __forceinline__ void stage_record(StageSmem<SB>& s, int slot, uint32_
   s.slab_lo[slot] = make_float4(dx - rad, dy - rad, dz - rad, 1.f / len);
   s.slab_hi[slot] = make_float4(dx + rad, dy + rad, dz + rad, len);
   s.corner[slot] = make_float4(cx - 0.5f * len, cy - 0.5f * len, cz - 0.5f * len, __int_as_float((int)vid));
-  if (va.geos_bf16) {
+  if (va.key) {
+    const int64_t* k = va.key + 8 * (size_t)vid;
+    float g[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) g[c] = va.grid_bf16 ? __bfloat162float(va.grid_bf16[k[c]]) : va.grid[k[c]];
+    s.geo[slot][0] = make_float4(g[0], g[1], g[2], g[3]);
+    s.geo[slot][1] = make_float4(g[4], g[5], g[6], g[7]);
+  } else if (va.geos_bf16) {
     const uint4 raw = *reinterpret_cast<const uint4*>(va.geos_bf16 + 8 * (size_t)vid);
     const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&raw);
     const float2 g0 = __bfloat1622float2(h[0]), g1 = __bfloat1622float2(h[1]);

@@ -38,7 +38,31 @@ struct BwdTileOut {
   float* subdiv;     // [P] (unused with RGB4)
   uint32_t* err;     // device error word
   int geo_vec4;      // dL_dgeos is 16-byte aligned: flush its rows with vector reductions
+  // Grid-point densities: when key is set, a record's 8 corner gradients are
+  // added into grid_grad[key[8 v + c]] instead of a dL_dgeos row.
+  const int64_t* key = nullptr;
+  float* grid_grad = nullptr;
 };
+
+// Density part of one record's flush: its 8 corner gradients into the
+// voxel's dL_dgeos row (two 16-byte reductions where the rows are aligned),
+// or into the grid points its corners index.
+__device__ __forceinline__ void flush_density(const BwdTileOut& out, uint32_t vid, const float acc[12], bool vec4) {
+  if (out.key) {
+    const int64_t* k = out.key + 8 * (size_t)vid;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) atomicAdd(out.grid_grad + k[c], acc[c]);
+    return;
+  }
+  float* g = out.dL_dgeos + 8 * (size_t)vid;
+  if (vec4) {
+    atomicAdd(reinterpret_cast<float4*>(g), make_float4(acc[0], acc[1], acc[2], acc[3]));
+    atomicAdd(reinterpret_cast<float4*>(g) + 1, make_float4(acc[4], acc[5], acc[6], acc[7]));
+  } else {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) atomicAdd(g + c, acc[c]);
+  }
+}
 
 constexpr int kGradStride = 13;  // 12 gradient floats + 1 pad (bank spread)
 
@@ -526,14 +550,7 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
       for (int c = 0; c < 12; ++c) gsum += fabsf(acc[c]);
       if (gsum != 0.f) {
         const uint32_t vid = (uint32_t)__float_as_int(s.corner[t].w);
-        float* g = out.dL_dgeos + 8 * (size_t)vid;
-        if (RGB4 || out.geo_vec4) {
-          atomicAdd(reinterpret_cast<float4*>(g), make_float4(acc[0], acc[1], acc[2], acc[3]));
-          atomicAdd(reinterpret_cast<float4*>(g) + 1, make_float4(acc[4], acc[5], acc[6], acc[7]));
-        } else {
-#pragma unroll
-          for (int c = 0; c < 8; ++c) atomicAdd(g + c, acc[c]);
-        }
+        flush_density(out, vid, acc, RGB4 || out.geo_vec4);
         if (RGB4) {
           atomicAdd(reinterpret_cast<float4*>(out.dL_drgbs) + vid, make_float4(acc[8], acc[9], acc[10], acc[11]));
         } else {

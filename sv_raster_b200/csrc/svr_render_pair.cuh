@@ -335,9 +335,7 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
       for (int c = 0; c < 12; ++c) gsum += fabsf(acc[c]);
       if (gsum != 0.f) {
         const uint32_t vid = (uint32_t)__float_as_int(s.corner[t].w);
-        float4* g4 = reinterpret_cast<float4*>(out.dL_dgeos + 8 * (size_t)vid);
-        atomicAdd(g4, make_float4(acc[0], acc[1], acc[2], acc[3]));
-        atomicAdd(g4 + 1, make_float4(acc[4], acc[5], acc[6], acc[7]));
+        flush_density(out, vid, acc, true);
         atomicAdd(reinterpret_cast<float4*>(out.dL_drgbs) + vid, make_float4(acc[8], acc[9], acc[10], acc[11]));
       }
     }

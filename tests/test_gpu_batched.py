@@ -477,6 +477,63 @@ def test_backward_pixels_per_thread_apart(c1, ppt, bppt):
         assert rel_err(a, b) < 1e-5, name
 
 
+@pytest.mark.parametrize("views,grid_dtype,ppt", [((0, 1, 2), torch.float32, 2), ((0, 1, 2), torch.bfloat16, 1),
+                                                  ("c3", torch.float32, 2)])
+def test_grid_fused_matches_separate(c1, views, grid_dtype, ppt):
+    """Grid-point densities read while staging and corner gradients added
+    into the grid in the flush (svr_batch_render_grid / _backward_grid)
+    against the separate all-voxel gather and scatter around render /
+    backward: images and T bitwise, grid gradient to the order of additions,
+    also through the autograd function (fused=True vs False)."""
+    if views == "c3":
+        C = SceneTensors(synthetic.cached_config_scene("c3"))
+        cams = [DevCam(C.scene.cameras[i]) for i in (0, 5)]
+    else:
+        C = c1
+        cams = [DevCam(C.scene.cameras[i]) for i in views]
+    from sv_raster_b200.batched import GridBatchedRender, gather_grid_geos, scatter_grid_grad
+    key, grid_np = synthetic.grid_params(C.scene, torch.device("cuda"))
+    key = key.contiguous()
+    grid = torch.from_numpy(grid_np).cuda().to(grid_dtype)
+    M = grid.numel()
+    r = BatchedRasterizer(cams, C.octpath, C.centers, C.lengths, max_level=C.scene.max_level, tile_size=8)
+    r.set_backward_pixels_per_thread(ppt)
+    r.fit_capacity(C.sh0, C.shs, 3)
+    r.prepare(C.sh0, C.shs, 3)
+    g = torch.Generator(device="cuda").manual_seed(31)
+    wC = torch.randn(3 * r.n_pixels, device="cuda", generator=g)
+    wT = torch.randn(r.n_pixels, device="cuda", generator=g)
+    P = C.centers.shape[0]
+    geos = torch.empty(P, 8, dtype=grid_dtype, device="cuda")
+    gather_grid_geos(key, grid, geos)
+    color_a, T_a = r.render(geos)
+    dgeo = torch.zeros(P, 8, device="cuda")
+    r.backward_render(geos, T_a, wC, wT, dgeo)
+    dgrid_a = torch.zeros(M, device="cuda")
+    scatter_grid_grad(key, dgeo, dgrid_a)
+    color_b, T_b = r.render_grid(key, grid)
+    dgrid_b = torch.zeros(M, device="cuda")
+    r.backward_render_grid(key, grid, T_b, wC, wT, dgrid_b)
+    torch.cuda.synchronize()
+    assert r.header()[1] == 0
+    assert torch.equal(color_a, color_b) and torch.equal(T_a, T_b)
+    err = rel_err(dgrid_b, dgrid_a)
+    print(f"fused grid ({views}, {grid_dtype}, {ppt} px/thread bwd): grid gradient rel {err:.2e}")
+    assert err < 1e-5
+    grads = {}
+    for fused in (False, True):
+        gp = grid.clone().requires_grad_(True)
+        s0 = C.sh0.clone().requires_grad_(True)
+        s1 = C.shs.clone().requires_grad_(True)
+        col, T = GridBatchedRender.apply(r, 3, key, gp, s0, s1, fused)
+        ((col * wC).sum() + (T * wT).sum()).backward()
+        grads[fused] = (col.detach(), gp.grad.float(), s0.grad, s1.grad)
+    assert torch.equal(grads[True][0], grads[False][0])
+    tol = 1e-5 if grid_dtype == torch.float32 else 1e-2  # bf16 gradients round differently per summation order
+    for a_, b_ in zip(grads[True][1:], grads[False][1:]):
+        assert rel_err(a_, b_) < tol
+
+
 def test_autotuner_runs_and_keeps_results(c1, tmp_path, monkeypatch):
     from sv_raster_b200.autotune import tune_batched
     monkeypatch.setenv("SVR_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
