@@ -97,7 +97,9 @@ struct StageSmem {
   float4 rgb[SB];         // rgb (xyz)
 };
 
-template <int SB>
+// MAYBE_GRID = false compiles the grid-point read out (kernels instantiated
+// apart for the per-voxel densities).
+template <int SB, bool MAYBE_GRID = true>
 __device__ __forceinline__ void stage_record(StageSmem<SB>& s, int slot, uint32_t val, const VoxelArrays& va,
                                              float ox, float oy, float oz) {
   const uint32_t vid = val_vox_id(val);
@@ -111,7 +113,7 @@ __device__ __forceinline__ void stage_record(StageSmem<SB>& s, int slot, uint32_
   s.slab_lo[slot] = make_float4(dx - rad, dy - rad, dz - rad, 1.f / len);
   s.slab_hi[slot] = make_float4(dx + rad, dy + rad, dz + rad, len);
   s.corner[slot] = make_float4(cx - 0.5f * len, cy - 0.5f * len, cz - 0.5f * len, __int_as_float((int)vid));
-  if (va.key) {
+  if (MAYBE_GRID && va.key) {
     const int64_t* k = va.key + 8 * (size_t)vid;
     float g[8];
 #pragma unroll

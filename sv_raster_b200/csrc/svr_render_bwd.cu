@@ -97,7 +97,7 @@ render_bwd_batch_kernel(const __grid_constant__ BwdBatchArgs a) {
 }
 
 // The same persistent form with two pixels per thread (svr_render_pair.cuh).
-template <class CFG, int NS, bool FAST>
+template <class CFG, int NS, bool FAST, bool GRID>
 __global__ void __launch_bounds__(CFG::NT, pair_min_blocks<CFG>())
 render_bwd_batch_pair_kernel(const __grid_constant__ BwdBatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -125,7 +125,7 @@ render_bwd_batch_pair_kernel(const __grid_constant__ BwdBatchArgs a) {
     in.dL_dT = a.in.dL_dT + pb;
     BwdTileOut o = a.out;
     o.dL_drgbs = a.out.dL_drgbs + (size_t)view * a.drgb_view_stride;
-    render_tile_bwd_pair<CFG, NS, FAST>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.tile_last[item], a.vals, va,
+    render_tile_bwd_pair<CFG, NS, FAST, GRID>(vp, sm.c2w, tile_x, tile_y, a.ranges[item], a.tile_last[item], a.vals, va,
                                         in, o, sm.s, sm.grad, sm.hit);
     __syncthreads();
   }
@@ -157,12 +157,19 @@ void launch_render_bwd(const ViewParams& vp, const uint2* ranges, const uint32_t
 template <class CFG>
 static void set_bwd_pair_attrs() {
   const int smem = (int)sizeof(BwdSmem<CFG>);
-  cudaFuncSetAttribute(render_bwd_batch_pair_kernel<CFG, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(render_bwd_batch_pair_kernel<CFG, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(render_bwd_batch_pair_kernel<CFG, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(render_bwd_batch_pair_kernel<CFG, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(render_bwd_batch_pair_kernel<CFG, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(render_bwd_batch_pair_kernel<CFG, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  auto set = [smem](const void* k) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); };
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 1, false, false>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 2, false, false>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 3, false, false>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 1, true, false>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 2, true, false>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 3, true, false>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 1, false, true>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 2, false, true>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 3, false, true>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 1, true, true>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 2, true, true>);
+  set((const void*)render_bwd_batch_pair_kernel<CFG, 3, true, true>);
 }
 
 template <class CFG, int NS>
@@ -218,9 +225,10 @@ static void launch_bwd_pair_arith(const BwdBatchArgs& args, int ns, int ctas_per
     const int grid = persistent_grid((const void*)kfn, CFG::NT, smem, args.n_items, ctas_per_sm);
     kfn<<<grid, CFG::NT, smem, stream>>>(args);
   };
-  if (ns == 1) go(render_bwd_batch_pair_kernel<CFG, 1, FAST>);
-  else if (ns == 2) go(render_bwd_batch_pair_kernel<CFG, 2, FAST>);
-  else go(render_bwd_batch_pair_kernel<CFG, 3, FAST>);
+  const bool grid = args.va.key != nullptr;
+  if (ns == 1) grid ? go(render_bwd_batch_pair_kernel<CFG, 1, FAST, true>) : go(render_bwd_batch_pair_kernel<CFG, 1, FAST, false>);
+  else if (ns == 2) grid ? go(render_bwd_batch_pair_kernel<CFG, 2, FAST, true>) : go(render_bwd_batch_pair_kernel<CFG, 2, FAST, false>);
+  else grid ? go(render_bwd_batch_pair_kernel<CFG, 3, FAST, true>) : go(render_bwd_batch_pair_kernel<CFG, 3, FAST, false>);
 }
 
 template <class CFG>

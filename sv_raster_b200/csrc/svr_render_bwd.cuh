@@ -47,8 +47,9 @@ struct BwdTileOut {
 // Density part of one record's flush: its 8 corner gradients into the
 // voxel's dL_dgeos row (two 16-byte reductions where the rows are aligned),
 // or into the grid points its corners index.
+template <bool MAYBE_GRID = true>
 __device__ __forceinline__ void flush_density(const BwdTileOut& out, uint32_t vid, const float acc[12], bool vec4) {
-  if (out.key) {
+  if (MAYBE_GRID && out.key) {
     const int64_t* k = out.key + 8 * (size_t)vid;
 #pragma unroll
     for (int c = 0; c < 8; ++c) atomicAdd(out.grid_grad + k[c], acc[c]);

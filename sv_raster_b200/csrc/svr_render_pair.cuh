@@ -177,7 +177,9 @@ __device__ __forceinline__ void render_tile_fwd_pair(const ViewParams& vp, const
   }
 }
 
-template <class CFG, int NS, bool FAST>
+// GRID: densities as grid points (VoxelArrays::key / BwdTileOut::key set);
+// the per-voxel form is instantiated without the grid reads.
+template <class CFG, int NS, bool FAST, bool GRID = false>
 __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const float* __restrict__ c2w_s,
                                                      int tile_x, int tile_y, uint2 range_raw, uint32_t tile_last,
                                                      const uint32_t* __restrict__ vals, const VoxelArrays& va,
@@ -232,7 +234,7 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
     const int base = r * SB;
     const int n_here = min(SB, todo_total - base);
     for (int i = tid; i < n_here; i += CFG::NT)
-      stage_record(s, i, vals[range.y - base - i - 1], va, ray[0].ox, ray[0].oy, ray[0].oz);
+      stage_record<CFG::SB, GRID>(s, i, vals[range.y - base - i - 1], va, ray[0].ox, ray[0].oy, ray[0].oz);
     __syncthreads();
 
     for (int g = 0; g < CFG::GROUPS && g * 32 < n_here; ++g) {
@@ -335,7 +337,7 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
       for (int c = 0; c < 12; ++c) gsum += fabsf(acc[c]);
       if (gsum != 0.f) {
         const uint32_t vid = (uint32_t)__float_as_int(s.corner[t].w);
-        flush_density(out, vid, acc, true);
+        flush_density<GRID>(out, vid, acc, true);
         atomicAdd(reinterpret_cast<float4*>(out.dL_drgbs) + vid, make_float4(acc[8], acc[9], acc[10], acc[11]));
       }
     }
