@@ -16,6 +16,22 @@
 
 namespace svr {
 
+// 32x32 bit matrix held one row per lane (bit l of lane j's word = entry
+// (j, l)) to its transpose: lane l returns the column l as a word, bit j =
+// entry (j, l).  Five exchanges swapping off-diagonal blocks of 16, 8, 4, 2
+// and 1 columns.
+__device__ __forceinline__ uint32_t warp_transpose_bits(uint32_t v, uint32_t lane) {
+  const uint32_t keep[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const int d = 16 >> k;
+    const uint32_t x = __shfl_xor_sync(0xffffffffu, v, d);
+    const uint32_t m = keep[k];
+    v = (lane & (uint32_t)d) ? ((v & ~m) | ((x >> d) & m)) : ((v & m) | ((x & m) << d));
+  }
+  return v;
+}
+
 struct FwdTileOut {
   uint32_t* tile_last;   // [T] of this view (indexed by the callers)
   uint32_t* n_contrib;   // [H*W] of this view
@@ -71,22 +87,38 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
 
     const uint32_t quad_mask = __reduce_or_sync(0xffffffffu, done ? 0u : (1u << ray.quad));
     if (quad_mask == 0u) continue;  // whole warp finished
+    // Lane q holds the mask of lanes still compositing whose ray quadrant is q.
+    const uint32_t lane = tid & 31;
+    uint32_t qlanes = 0u;
+    for (uint32_t qm = quad_mask; qm; qm &= qm - 1) {
+      const uint32_t q = (uint32_t)(__ffs(qm) - 1);
+      const uint32_t b = __ballot_sync(0xffffffffu, !done && ray.quad == q);
+      if (lane == q) qlanes = b;
+    }
     for (int g = 0; g < CFG::GROUPS && g * 32 < n_here; ++g) {
-      const int slot = g * 32 + (tid & 31);
+      const int slot = g * 32 + (int)lane;
       const bool hit = slot < n_here && record_hits_warp(s, slot, wx0, wy0, quad_mask);
-      uint32_t m = __ballot_sync(0xffffffffu, hit);
-      // This pixel's records among those: each lane then walks its own list
-      // in order, so one warp iteration serves a different record per lane
-      // (a warp takes as many iterations as its busiest pixel has records,
-      // not one per record that touches it).
-      uint32_t mine = 0u;
-      if (!done) {
-        while (m) {
-          const int bit = __ffs(m) - 1;
-          m &= m - 1;
-          if (record_hits_pixel(s, g * 32 + bit, px, py, ray.quad)) mine |= 1u << bit;
-        }
+      // Lane j: the pixels of the warp's 8x4 block that staged record j
+      // covers with a matching ray quadrant (record_hits_pixel for all 32
+      // pixels at once: the bbox clipped to the block, as byte rows).
+      uint32_t covers = 0u;
+      uint32_t rec_quad = 0u;
+      if (hit) {
+        const uint4 b = s.box[slot];
+        const uint32_t cx0 = max(b.x, wx0) - wx0, cx1 = min(b.x + b.y, wx0 + 7u) - wx0;
+        const uint32_t h = b.w & 0xFFFFu;
+        const uint32_t ry0 = max(b.z, wy0) - wy0, ry1 = min(b.z + h, wy0 + 3u) - wy0;
+        const uint32_t cols = (0xFFu >> (7u - cx1)) & (0xFFu << cx0);
+        const uint32_t rows = (0x01010101u >> (8u * (3u - ry1))) & (0x01010101u << (8u * ry0));
+        covers = cols * rows;
+        rec_quad = b.w >> 16;
       }
+      covers &= __shfl_sync(0xffffffffu, qlanes, (int)rec_quad);
+      // This pixel's records among those (a transposition of the 32 masks):
+      // each lane then walks its own list in order, so one warp iteration
+      // serves a different record per lane (a warp takes as many iterations
+      // as its busiest pixel has records, not one per record that touches it).
+      uint32_t mine = warp_transpose_bits(covers, lane);
       while (mine) {
         const int j = g * 32 + __ffs(mine) - 1;
         mine &= mine - 1;
