@@ -118,7 +118,10 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
       // each lane then walks its own list in order, so one warp iteration
       // serves a different record per lane (a warp takes as many iterations
       // as its busiest pixel has records, not one per record that touches it).
+      // (qlanes was taken at the start of the round: a pixel that finished in
+      // an earlier group of this round takes no more records.)
       uint32_t mine = warp_transpose_bits(covers, lane);
+      if (done) mine = 0u;
       while (mine) {
         const int j = g * 32 + __ffs(mine) - 1;
         mine &= mine - 1;
