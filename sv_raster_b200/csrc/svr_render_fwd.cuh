@@ -32,6 +32,19 @@ __device__ __forceinline__ uint32_t warp_transpose_bits(uint32_t v, uint32_t lan
   return v;
 }
 
+// Pixels of the 8x4 block with corner (bx0, by0) that staged box b covers, as
+// a 32-bit lane mask (lane = row * 8 + column; byte r = row r): the
+// record_hits_pixel bbox test for 32 pixels at once.  0 when disjoint.
+__device__ __forceinline__ uint32_t block_cover_mask(const uint4& b, uint32_t bx0, uint32_t by0) {
+  const uint32_t x1 = b.x + b.y, y1 = b.z + (b.w & 0xFFFFu);
+  if (b.x > bx0 + 7u || x1 < bx0 || b.z > by0 + 3u || y1 < by0) return 0u;
+  const uint32_t cx0 = max(b.x, bx0) - bx0, cx1 = min(x1, bx0 + 7u) - bx0;
+  const uint32_t ry0 = max(b.z, by0) - by0, ry1 = min(y1, by0 + 3u) - by0;
+  const uint32_t cols = (0xFFu >> (7u - cx1)) & (0xFFu << cx0);
+  const uint32_t rows = (0x01010101u >> (8u * (3u - ry1))) & (0x01010101u << (8u * ry0));
+  return cols * rows;
+}
+
 struct FwdTileOut {
   uint32_t* tile_last;   // [T] of this view (indexed by the callers)
   uint32_t* n_contrib;   // [H*W] of this view
@@ -105,12 +118,7 @@ __device__ __forceinline__ void render_tile_fwd(const ViewParams& vp, const floa
       uint32_t rec_quad = 0u;
       if (hit) {
         const uint4 b = s.box[slot];
-        const uint32_t cx0 = max(b.x, wx0) - wx0, cx1 = min(b.x + b.y, wx0 + 7u) - wx0;
-        const uint32_t h = b.w & 0xFFFFu;
-        const uint32_t ry0 = max(b.z, wy0) - wy0, ry1 = min(b.z + h, wy0 + 3u) - wy0;
-        const uint32_t cols = (0xFFu >> (7u - cx1)) & (0xFFu << cx0);
-        const uint32_t rows = (0x01010101u >> (8u * (3u - ry1))) & (0x01010101u << (8u * ry0));
-        covers = cols * rows;
+        covers = block_cover_mask(b, wx0, wy0);
         rec_quad = b.w >> 16;
       }
       covers &= __shfl_sync(0xffffffffu, qlanes, (int)rec_quad);

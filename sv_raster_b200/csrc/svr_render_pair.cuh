@@ -227,6 +227,17 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
   const uint32_t warp_lc = __reduce_max_sync(0xffffffffu, max(last_contrib[0], last_contrib[1]));
   const uint32_t quad_mask = __reduce_or_sync(
       0xffffffffu, (inside[0] ? (1u << ray[0].quad) : 0u) | (inside[1] ? (1u << ray[1].quad) : 0u));
+  // Lane q holds, per pixel row k, the lanes whose pixel k is in the image
+  // with ray quadrant q.
+  uint32_t qlanes[2] = {0u, 0u};
+  for (uint32_t qm = quad_mask; qm; qm &= qm - 1) {
+    const uint32_t q = (uint32_t)(__ffs(qm) - 1);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const uint32_t bk = __ballot_sync(0xffffffffu, inside[k] && ray[k].quad == q);
+      if ((uint32_t)lane == q) qlanes[k] = bk;
+    }
+  }
 
   const int rounds = (todo_total + SB - 1) / SB;
   for (int r = 0; r < rounds; ++r) {
@@ -242,11 +253,33 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
       const uint32_t pos = (uint32_t)(todo_total - base - slot - 1);
       const bool hit = slot < n_here && pos < warp_lc && record_hits_block8(s, slot, wx0, wy0, quad_mask);
       uint32_t m = __ballot_sync(0xffffffffu, hit);
+      // Each lane's candidate records of this group per pixel: lane j turns
+      // record j's bbox into masks of the pixels it covers in the two 8x4
+      // halves, restricted to the lanes of its ray quadrant, and a bit
+      // transposition hands every lane its records; a record reaches pixel k
+      // only while its position is below the pixel's contributor count.
+      uint32_t cov[2] = {0u, 0u};
+      uint32_t rec_quad = 0u;
+      if (hit) {
+        const uint4 b = s.box[slot];
+        cov[0] = block_cover_mask(b, wx0, wy0);
+        cov[1] = block_cover_mask(b, wx0, wy0 + 4u);
+        rec_quad = b.w >> 16;
+      }
+      uint32_t mine[2];
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        mine[k] = warp_transpose_bits(cov[k] & __shfl_sync(0xffffffffu, qlanes[k], (int)rec_quad), (uint32_t)lane);
+        // slot j is in reach while todo_total - base - j - 1 < last_contrib[k]
+        const int first = todo_total - base - (int)last_contrib[k] - g * 32;
+        mine[k] &= first <= 0 ? 0xffffffffu : (first >= 32 ? 0u : ~((1u << first) - 1u));
+      }
+      m &= __reduce_or_sync(0xffffffffu, mine[0] | mine[1]);  // records no pixel of the warp takes
       uint32_t wrote = 0u;
       while (m) {
-        const int j = g * 32 + __ffs(m) - 1;
+        const int bit = __ffs(m) - 1;
+        const int j = g * 32 + bit;
         m &= m - 1;
-        const uint32_t jpos = (uint32_t)(todo_total - base - j - 1);
         float gp[12];
 #pragma unroll
         for (int c = 0; c < 12; ++c) gp[c] = 0.f;
@@ -254,7 +287,7 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
         const float4 slo = s.slab_lo[j], shi = s.slab_hi[j];
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-          if (!(inside[k] && jpos < last_contrib[k]) || !record_hits_pixel(s, j, px, py[k], ray[k].quad)) continue;
+          if (!((mine[k] >> bit) & 1u)) continue;
           const float2 ab = staged_ray_box(slo, shi, ray[k]);
           const float a = ab.x, b = ab.y;
           if (a > b) continue;
