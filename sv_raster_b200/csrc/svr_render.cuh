@@ -155,6 +155,35 @@ __device__ __forceinline__ bool record_hits_warp(const StageSmem<SB>& s, int slo
          ((quad_mask >> (b.w >> 16)) & 1u);
 }
 
+// 32x32 bit matrix held one row per lane (bit l of lane j's word = entry
+// (j, l)) to its transpose: lane l returns the column l as a word, bit j =
+// entry (j, l).  Five exchanges swapping off-diagonal blocks of 16, 8, 4, 2
+// and 1 columns.
+__device__ __forceinline__ uint32_t warp_transpose_bits(uint32_t v, uint32_t lane) {
+  const uint32_t keep[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const int d = 16 >> k;
+    const uint32_t x = __shfl_xor_sync(0xffffffffu, v, d);
+    const uint32_t m = keep[k];
+    v = (lane & (uint32_t)d) ? ((v & ~m) | ((x >> d) & m)) : ((v & m) | ((x & m) << d));
+  }
+  return v;
+}
+
+// Pixels of the 8x4 block with corner (bx0, by0) that staged box b covers, as
+// a 32-bit lane mask (lane = row * 8 + column; byte r = row r): the
+// record_hits_pixel bbox test for 32 pixels at once.  0 when disjoint.
+__device__ __forceinline__ uint32_t block_cover_mask(const uint4& b, uint32_t bx0, uint32_t by0) {
+  const uint32_t x1 = b.x + b.y, y1 = b.z + (b.w & 0xFFFFu);
+  if (b.x > bx0 + 7u || x1 < bx0 || b.z > by0 + 3u || y1 < by0) return 0u;
+  const uint32_t cx0 = max(b.x, bx0) - bx0, cx1 = min(x1, bx0 + 7u) - bx0;
+  const uint32_t ry0 = max(b.z, by0) - by0, ry1 = min(y1, by0 + 3u) - by0;
+  const uint32_t cols = (0xFFu >> (7u - cx1)) & (0xFFu << cx0);
+  const uint32_t rows = (0x01010101u >> (8u * (3u - ry1))) & (0x01010101u << (8u * ry0));
+  return cols * rows;
+}
+
 // The reference's per-pixel test: pixel inside the packed bbox and ray
 // quadrant equal to the instance's (forward.cu:186), as two unsigned range
 // checks on the staged (min, extent) form.

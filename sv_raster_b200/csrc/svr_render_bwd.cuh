@@ -506,6 +506,13 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
   // Largest contributor count of this warp: records at or beyond it are skipped by every lane.
   const uint32_t warp_lc = __reduce_max_sync(0xffffffffu, last_contrib);
   const uint32_t quad_mask = __reduce_or_sync(0xffffffffu, inside ? (1u << ray.quad) : 0u);
+  // Lane q holds the lanes whose pixel is in the image with ray quadrant q.
+  uint32_t qlanes = 0u;
+  for (uint32_t qm = quad_mask; qm; qm &= qm - 1) {
+    const uint32_t q = (uint32_t)(__ffs(qm) - 1);
+    const uint32_t bq = __ballot_sync(0xffffffffu, inside && ray.quad == q);
+    if ((uint32_t)lane == q) qlanes = bq;
+  }
 
   const int rounds = (todo_total + SB - 1) / SB;
   for (int r = 0; r < rounds; ++r) {
@@ -522,17 +529,30 @@ __device__ __forceinline__ void render_tile_bwd(const ViewParams& vp, const floa
       const uint32_t pos = (uint32_t)(todo_total - base - slot - 1);
       const bool hit = slot < n_here && pos < warp_lc && record_hits_warp(s, slot, wx0, wy0, quad_mask);
       uint32_t m = __ballot_sync(0xffffffffu, hit);
+      // This lane's candidate records of the group (pixel in the record's
+      // bbox, matching quadrant, record within the contributor count): lane
+      // j's block mask of record j, transposed across the warp.
+      uint32_t covers = 0u, rec_quad = 0u;
+      if (hit) {
+        const uint4 b = s.box[slot];
+        covers = block_cover_mask(b, wx0, wy0);
+        rec_quad = b.w >> 16;
+      }
+      uint32_t mine = warp_transpose_bits(covers & __shfl_sync(0xffffffffu, qlanes, (int)rec_quad), (uint32_t)lane);
+      {
+        // slot j is in reach while todo_total - base - j - 1 < last_contrib
+        const int first = todo_total - base - (int)last_contrib - g * 32;
+        mine &= first <= 0 ? 0xffffffffu : (first >= 32 ? 0u : ~((1u << first) - 1u));
+      }
+      m &= __reduce_or_sync(0xffffffffu, mine);  // records no pixel of the warp takes
       uint32_t wrote = 0u;
       while (m) {
-        const int j = g * 32 + __ffs(m) - 1;
+        const int bit = __ffs(m) - 1;
+        const int j = g * 32 + bit;
         m &= m - 1;
-        const uint32_t jpos = (uint32_t)(todo_total - base - j - 1);
         bool contrib = false;
         float gp[12];
-        if (inside && jpos < last_contrib) {
-          if (record_hits_pixel(s, j, px, py, ray.quad))
-            contrib = bwd_pixel_record<SB, NS, DEPTH, DIST, NORMAL, FAST>(s, j, ray, in, st, gp);
-        }
+        if ((mine >> bit) & 1u) contrib = bwd_pixel_record<SB, NS, DEPTH, DIST, NORMAL, FAST>(s, j, ray, in, st, gp);
         // Warp reduction of this record's gradients into its accumulator.
         const uint32_t act_mask = __ballot_sync(0xffffffffu, contrib);
         if (act_mask == 0u) continue;
