@@ -88,8 +88,7 @@ project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* _
   for (int v = 0; v < views.n; ++v) {
     const size_t o = (size_t)v * P + i;
     const float* m = s_m[v];
-    Projection pr = tight ? project_voxel_fast(views.v[v], m, m + 12, cx, cy, cz, len)
-                          : project_voxel(views.v[v], m, m + 12, cx, cy, cz, len);
+    Projection pr = project_voxel(views.v[v], m, m + 12, cx, cy, cz, len);
     if (tight) tighten_bbox(views.v[v], pr);
     ndup[o] = pr.n;
     bboxes[o] = pr.bbox;

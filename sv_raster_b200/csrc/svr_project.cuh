@@ -66,71 +66,6 @@ __device__ __forceinline__ Projection project_voxel(const ViewParams& vp, const 
   return pr;
 }
 
-// project_voxel with cheaper arithmetic, for the tight-bbox path only: the
-// 8 corners' camera coordinates built from the centre's plus the scaled
-// rotation columns (additions instead of a matrix product per corner), an
-// approximate reciprocal of the depth, and the quadrant bits per axis.  The
-// corner coordinates differ from project_voxel's in the last bits (the
-// quadrant bits do not), so the rounded bbox can differ where a side lands on
-// a half pixel; tighten_bbox
-// keeps only pixel centres within kTightMargin of the extent, far beyond
-// that error, so the instance lists it produces stay exact in what they
-// drop (every pixel left out has a ray that misses the cube).
-__device__ __forceinline__ Projection project_voxel_fast(const ViewParams& vp, const float* w2c, const float* c2w,
-                                                         float vcx, float vcy, float vcz, float len) {
-  Projection pr{0u, make_uint2(0u, 0u), 0u, 0.f, 0.f, 0.f, 0.f, false};
-  const float vr = 0.5f * len;
-  const float rox = c2w[3], roy = c2w[7], roz = c2w[11];
-  const float near = vp.near_plane;
-  const float rx = vcx - rox, ry = vcy - roy, rz = vcz - roz;
-  if (rx * rx + ry * ry + rz * rz < near * near) return pr;
-  const float ccx = w2c[0] * vcx + w2c[1] * vcy + w2c[2] * vcz + w2c[3];
-  const float ccy = w2c[4] * vcx + w2c[5] * vcy + w2c[6] * vcz + w2c[7];
-  const float ccz = w2c[8] * vcx + w2c[9] * vcy + w2c[10] * vcz + w2c[11];
-  // half-edge offsets along the world axes, in camera coordinates
-  const float ax = vr * w2c[0], ay = vr * w2c[4], az = vr * w2c[8];
-  const float bx = vr * w2c[1], by = vr * w2c[5], bz = vr * w2c[9];
-  const float gx = vr * w2c[2], gy = vr * w2c[6], gz = vr * w2c[10];
-  // quadrant bit of each axis for the - and + corner (the world corner
-  // coordinates compared with the camera centre, as project_voxel does)
-  const uint32_t qx0 = (vcx + vr * -1.f) < rox, qx1 = (vcx + vr * 1.f) < rox;
-  const uint32_t qy0 = (vcy + vr * -1.f) < roy, qy1 = (vcy + vr * 1.f) < roy;
-  const uint32_t qz0 = (vcz + vr * -1.f) < roz, qz1 = (vcz + vr * 1.f) < roz;
-  float umin = 1e9f, vmin = 1e9f, umax = -1e9f, vmax = -1e9f;
-  uint32_t qbits = 0;
-  int n_front = 0;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const float sx = (i & 4) ? 1.f : -1.f, sy = (i & 2) ? 1.f : -1.f, sz = (i & 1) ? 1.f : -1.f;
-    const float camx = ccx + sx * ax + sy * bx + sz * gx;
-    const float camy = ccy + sx * ay + sy * by + sz * gy;
-    const float camz = ccz + sx * az + sy * bz + sz * gz;
-    if (camz < near) continue;
-    const float inv_z = __fdividef(1.0f, camz);
-    const float u = camx * inv_z, v = camy * inv_z;
-    const uint32_t q = (((i & 4) ? qx1 : qx0) << 2) | (((i & 2) ? qy1 : qy0) << 1) | ((i & 1) ? qz1 : qz0);
-    umin = fminf(umin, u); vmin = fminf(vmin, v);
-    umax = fmaxf(umax, u); vmax = fmaxf(vmax, v);
-    qbits |= (1u << q);
-    ++n_front;
-  }
-  const float cxh = vp.cx - 0.5f, cyh = vp.cy - 0.5f;
-  const float bx0 = fmaxf(vp.focal_x * umin + cxh, 0.0f);
-  const float by0 = fmaxf(vp.focal_y * vmin + cyh, 0.0f);
-  const float bx1 = fminf(vp.focal_x * umax + cxh, (float)vp.W);
-  const float by1 = fminf(vp.focal_y * vmax + cyh, (float)vp.H);
-  if (bx0 > bx1 || by0 > by1) return pr;
-  pr.bbox.x = (((uint32_t)lrintf(bx0)) << 16) | ((uint32_t)lrintf(by0));
-  pr.bbox.y = (((uint32_t)lrintf(bx1)) << 16) | ((uint32_t)lrintf(by1));
-  int tx0, ty0, tx1, ty1;
-  bbox_tile_rect(pr.bbox, vp.grid_x, vp.grid_y, vp.tile_shift, tx0, ty0, tx1, ty1);
-  pr.n = (uint32_t)((1 + ty1 - ty0) * (1 + tx1 - tx0)) * (uint32_t)__popc(qbits);
-  pr.quads = qbits;
-  pr.bx0 = bx0; pr.by0 = by0; pr.bx1 = bx1; pr.by1 = by1;
-  pr.front = n_front == 8;
-  return pr;
-}
-
 // The pixels of the rounded bbox whose centre ray can meet the cube.  The ray
 // of pixel (px, py) has the projected coordinates (px, py) themselves (the
 // ray direction of make_pixel_ray, (p + 0.5 - c) / focal, maps to
