@@ -65,6 +65,7 @@ project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* _
                   const int64_t* __restrict__ octpaths, int level_low_bits, int tight, uint32_t* __restrict__ ndup,
                   uint2* __restrict__ bboxes, uint32_t* __restrict__ quads, float* __restrict__ rgbs,
                   uint32_t* __restrict__ err) {
+  constexpr int NB = (DEG + 1) * (DEG + 1) - 1;  // rest coefficients per channel
   __shared__ float s_m[kMaxViews][24];           // w2c (12) and c2w (12) of every view
   for (int t = threadIdx.x; t < views.n * 24; t += blockDim.x) {
     const int v = t / 24, k = t % 24;
@@ -154,44 +155,6 @@ __device__ __forceinline__ int nth_set_bit(uint32_t m, int k) {
 // positions, so the final lists do not depend on it.
 constexpr int kDupWrite = 0, kDupCount = 1, kDupScatter = 2;
 
-// Instance p of a warp's run: its owning lane (sl), quadrant, tile (local to
-// the view) and whether it is written (inside the run and the capacity).
-// Every lane of the warp must call it (it shuffles).
-struct DupInst {
-  bool active;
-  int sl;
-  uint32_t q, local;
-};
-
-__device__ __forceinline__ DupInst dup_decode(uint32_t p, uint32_t total, uint32_t run0, uint32_t cap, uint32_t off,
-                                              uint32_t tiles, uint32_t w, int tx0, int ty0, uint32_t qb,
-                                              int grid_x) {
-  DupInst d;
-  // owning lane: the largest s with off_s <= p (offsets are non-decreasing)
-  int sl = 0;
-#pragma unroll
-  for (int step = 16; step > 0; step >>= 1) {
-    const uint32_t t = __shfl_sync(0xffffffffu, off, sl + step);
-    if (t <= p) sl += step;
-  }
-  const uint32_t k = p - __shfl_sync(0xffffffffu, off, sl);
-  const uint32_t s_tiles = __shfl_sync(0xffffffffu, tiles, sl);
-  const uint32_t s_w = __shfl_sync(0xffffffffu, w, sl);
-  const int s_tx0 = __shfl_sync(0xffffffffu, tx0, sl), s_ty0 = __shfl_sync(0xffffffffu, ty0, sl);
-  const uint32_t s_qb = __shfl_sync(0xffffffffu, qb, sl);
-  d.active = p < total && run0 + p < cap;
-  d.sl = sl;
-  d.q = 0u;
-  d.local = 0u;
-  if (d.active) {
-    const uint32_t qi = k / s_tiles, rem = k - qi * s_tiles;
-    const uint32_t ty = (uint32_t)s_ty0 + rem / s_w, tx = (uint32_t)s_tx0 + rem % s_w;
-    d.q = (uint32_t)nth_set_bit(s_qb, (int)qi);
-    d.local = ty * (uint32_t)grid_x + tx;
-  }
-  return d;
-}
-
 template <int MODE>
 __global__ void __launch_bounds__(256)
 duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const uint32_t* __restrict__ rank_pos,
@@ -229,74 +192,51 @@ duplicate_batch_kernel(const __grid_constant__ ViewTable views, int P, const uin
   const uint32_t run0 = __shfl_sync(0xffffffffu, end - n, 0) + 0u;  // lane 0's start (valid even if n == 0)
   const uint32_t w = (uint32_t)(tx1 - tx0 + 1);
   const uint32_t tiles = w * (uint32_t)(ty1 - ty0 + 1);
-  if constexpr (MODE == kDupScatter) {
-    // Two chunks of 32 instances per iteration: their rank-position loads
-    // and their returning tile-cursor atomics are in flight together.
-    for (uint32_t cb = 0; cb < total; cb += 64) {
-      DupInst d[2];
-      uint32_t rp[2], peers[2], base[2];
-      int leader[2];
+  for (uint32_t cb = 0; cb < total; cb += 32) {
+    const uint32_t p = cb + lane;
+    // owning lane: the largest s with off_s <= p (offsets are non-decreasing)
+    int sl = 0;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        d[h] = dup_decode(cb + 32u * h + (uint32_t)lane, total, run0, cap, off, tiles, w, tx0, ty0, qb, vp.grid_x);
-        rp[h] = d[h].active ? rank_pos[8 * (size_t)(blockIdx.x * blockDim.x + (threadIdx.x & ~31) + d[h].sl) + d[h].q]
-                            : 0u;
-      }
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const uint32_t gtile = d[h].active ? vp.tile_base + d[h].local : 0xffffffffu;
-        peers[h] = __match_any_sync(0xffffffffu, gtile);
-        leader[h] = __ffs(peers[h]) - 1;
-        base[h] = 0u;
-        if (d[h].active && lane == leader[h]) base[h] = atomicAdd(&ranges[gtile].y, (uint32_t)__popc(peers[h]));
-      }
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const uint32_t b = __shfl_sync(0xffffffffu, base[h], leader[h]);
-        if (d[h].active) {
-          const uint32_t pos = b + (uint32_t)__popc(peers[h] & ((1u << lane) - 1u));
-          const uint32_t vid = (uint32_t)(blockIdx.x * blockDim.x + (threadIdx.x & ~31) + d[h].sl);
-          keys[pos] = ((uint64_t)(vp.sort_tile_off + d[h].local) << kPosShift) | rp[h];
-          vals[pos] = make_sort_val(vid, d[h].q);
-        }
-      }
+    for (int step = 16; step > 0; step >>= 1) {
+      const uint32_t t = __shfl_sync(0xffffffffu, off, sl + step);
+      if (t <= p) sl += step;
     }
-  } else {
-    for (uint32_t cb = 0; cb < total; cb += 32) {
-      const uint32_t p = cb + lane;
-      // owning lane: the largest s with off_s <= p (offsets are non-decreasing)
-      int sl = 0;
-  #pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
-        const uint32_t t = __shfl_sync(0xffffffffu, off, sl + step);
-        if (t <= p) sl += step;
-      }
-      const uint32_t k = p - __shfl_sync(0xffffffffu, off, sl);
-      const uint32_t s_tiles = __shfl_sync(0xffffffffu, tiles, sl);
-      const uint32_t s_w = __shfl_sync(0xffffffffu, w, sl);
-      const int s_tx0 = __shfl_sync(0xffffffffu, tx0, sl), s_ty0 = __shfl_sync(0xffffffffu, ty0, sl);
-      const uint32_t s_qb = __shfl_sync(0xffffffffu, qb, sl);
-      const uint32_t slot = run0 + p;
-      const bool active = p < total && slot < cap;
-      uint32_t q = 0, vid = 0, local = 0;
+    const uint32_t k = p - __shfl_sync(0xffffffffu, off, sl);
+    const uint32_t s_tiles = __shfl_sync(0xffffffffu, tiles, sl);
+    const uint32_t s_w = __shfl_sync(0xffffffffu, w, sl);
+    const int s_tx0 = __shfl_sync(0xffffffffu, tx0, sl), s_ty0 = __shfl_sync(0xffffffffu, ty0, sl);
+    const uint32_t s_qb = __shfl_sync(0xffffffffu, qb, sl);
+    const uint32_t slot = run0 + p;
+    const bool active = p < total && slot < cap;
+    uint32_t q = 0, vid = 0, local = 0;
+    if (active) {
+      const uint32_t qi = k / s_tiles, rem = k - qi * s_tiles;
+      const uint32_t ty = (uint32_t)s_ty0 + rem / s_w, tx = (uint32_t)s_tx0 + rem % s_w;
+      q = (uint32_t)nth_set_bit(s_qb, (int)qi);
+      vid = (uint32_t)(blockIdx.x * blockDim.x + (threadIdx.x & ~31) + sl);
+      local = ty * (uint32_t)vp.grid_x + tx;
+    }
+    if (MODE == kDupWrite) {
       if (active) {
-        const uint32_t qi = k / s_tiles, rem = k - qi * s_tiles;
-        const uint32_t ty = (uint32_t)s_ty0 + rem / s_w, tx = (uint32_t)s_tx0 + rem % s_w;
-        q = (uint32_t)nth_set_bit(s_qb, (int)qi);
-        vid = (uint32_t)(blockIdx.x * blockDim.x + (threadIdx.x & ~31) + sl);
-        local = ty * (uint32_t)vp.grid_x + tx;
+        keys[slot] = ((uint64_t)(vp.sort_tile_off + local) << kPosShift) | rank_pos[8 * (size_t)vid + q];
+        vals[slot] = make_sort_val(vid, q);
       }
-      if (MODE == kDupWrite) {
-        if (active) {
-          keys[slot] = ((uint64_t)(vp.sort_tile_off + local) << kPosShift) | rank_pos[8 * (size_t)vid + q];
-          vals[slot] = make_sort_val(vid, q);
-        }
+    } else {
+      // global tile of the instance; inactive lanes share a value no tile has
+      const uint32_t gtile = active ? vp.tile_base + local : 0xffffffffu;
+      const uint32_t peers = __match_any_sync(0xffffffffu, gtile);
+      const int leader = __ffs(peers) - 1;
+      if (MODE == kDupCount) {
+        if (active && lane == leader) atomicAdd(counts + gtile, (uint32_t)__popc(peers));
       } else {
-        // global tile of the instance; inactive lanes share a value no tile has
-        const uint32_t gtile = active ? vp.tile_base + local : 0xffffffffu;
-        const uint32_t peers = __match_any_sync(0xffffffffu, gtile);
-        const int leader = __ffs(peers) - 1;
-        if (active && lane == leader) atomicAdd(counts + gtile, (uint32_t)__popc(peers));  // kDupCount
+        uint32_t base = 0;
+        if (active && lane == leader) base = atomicAdd(&ranges[gtile].y, (uint32_t)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (active) {
+          const uint32_t pos = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+          keys[pos] = ((uint64_t)(vp.sort_tile_off + local) << kPosShift) | rank_pos[8 * (size_t)vid + q];
+          vals[pos] = make_sort_val(vid, q);
+        }
       }
     }
   }
