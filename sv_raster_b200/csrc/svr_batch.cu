@@ -65,7 +65,6 @@ project_sh_kernel(const __grid_constant__ ViewTable views, int P, const float* _
                   const int64_t* __restrict__ octpaths, int level_low_bits, int tight, uint32_t* __restrict__ ndup,
                   uint2* __restrict__ bboxes, uint32_t* __restrict__ quads, float* __restrict__ rgbs,
                   uint32_t* __restrict__ err) {
-  constexpr int NB = (DEG + 1) * (DEG + 1) - 1;  // rest coefficients per channel
   __shared__ float s_m[kMaxViews][24];           // w2c (12) and c2w (12) of every view
   for (int t = threadIdx.x; t < views.n * 24; t += blockDim.x) {
     const int v = t / 24, k = t % 24;
