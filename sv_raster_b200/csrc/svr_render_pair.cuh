@@ -285,21 +285,22 @@ __device__ __forceinline__ void render_tile_bwd_pair(const ViewParams& vp, const
         for (int c = 0; c < 12; ++c) gp[c] = 0.f;
         bool contrib = false;
         const float4 slo = s.slab_lo[j], shi = s.slab_hi[j];
+        // the record's densities and corner, read once for both pixels
+        float geo[8];
+        load_geo(s, j, geo);
+        const float4 cr = s.corner[j];
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
           if (!((mine[k] >> bit) & 1u)) continue;
           const float2 ab = staged_ray_box(slo, shi, ray[k]);
           const float a = ab.x, b = ab.y;
           if (a > b) continue;
-          float geo[8];
-          load_geo(s, j, geo);
           float vol_int = 0.f;
           float dI_dgeo[8];
 #pragma unroll
           for (int c = 0; c < 8; ++c) dI_dgeo[c] = 0.f;
           float w[8];
           const float vox_l_inv = slo.w;
-          const float4 cr = s.corner[j];
           const float step_sz = (b - a) * (1.f / NS);
           const float stx = step_sz * ray[k].dx, sty = step_sz * ray[k].dy, stz = step_sz * ray[k].dz;
           const float t0 = a + 0.5f * step_sz;
